@@ -1,0 +1,154 @@
+/*
+ * shtns.h -- public C API of shtns_b200, a drop-in replacement for the
+ * SHTns 3.5.2 transform API whose transforms run on an NVIDIA B200 (sm_100a).
+ *
+ * Every declaration below keeps the name, signature, argument meaning and
+ * return value of the SHTns 3.5.2 function it replaces (the reference
+ * shtns.h line is given beside each), so code written against SHTns compiles
+ * and links against libshtns_b200.so unchanged.  Host-pointer transforms
+ * (SH_to_spat, ...) copy their arrays to the GPU, transform there and copy
+ * back; the cu_* functions of shtns_cuda.h take device pointers.
+ *
+ * Functions of the SHTns API that are not on the transform path (rotations,
+ * point and latitude evaluation, complex-field transforms, regular grids) are
+ * not provided.
+ */
+#ifndef SHTNS_B200_SHTNS_H
+#define SHTNS_B200_SHTNS_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+	#include <complex>
+	typedef std::complex<double> cplx;
+	typedef std::complex<float> cplx_f;
+#else
+	#include <complex.h>
+	typedef complex double cplx;
+	typedef complex float cplx_f;
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* interface version: same encoding as the reference (shtns.h:39) */
+#define SHTNS_INTERFACE 0x30500
+
+/* plan handle (shtns.h:42) */
+typedef struct shtns_info* shtns_cfg;
+
+/* normalisations (shtns.h:48-55) */
+enum shtns_norm {
+	sht_orthonormal,
+	sht_fourpi,
+	sht_schmidt,
+	sht_for_rotations
+};
+#define SHT_NO_CS_PHASE (256*4)
+#define SHT_REAL_NORM (256*8)
+
+/* grid types and layout flags (shtns.h:58-75).  Only Gauss grids are
+ * provided: sht_gauss, sht_auto, sht_quick_init and sht_gauss_fly. */
+enum shtns_type {
+	sht_gauss,
+	sht_auto,
+	sht_reg_fast,
+	sht_reg_dct,
+	sht_quick_init,
+	sht_reg_poles,
+	sht_gauss_fly
+};
+#define SHT_NATIVE_LAYOUT 0
+#define SHT_THETA_CONTIGUOUS 256
+#define SHT_PHI_CONTIGUOUS (256*2)
+#define SHT_SOUTH_POLE_FIRST (256*32)
+#define SHT_SCALAR_ONLY (256*16)
+#define SHT_LOAD_SAVE_CFG (256*64)
+#define SHT_ALLOW_GPU (256*128)
+#define SHT_ALLOW_PADDING (256*256)
+
+#ifndef SHTNS_B200_PRIVATE
+/* read-only public part of the plan, layout-compatible with shtns.h:79-94 */
+struct shtns_info {
+	const unsigned int nlm;
+	const unsigned short lmax;
+	const unsigned short mmax;
+	const unsigned short mres;
+	const unsigned short nlat_2;
+	const unsigned int nlat;
+	const unsigned int nphi;
+	const unsigned int nspat;
+	const unsigned short *const li;
+	const unsigned short *const mi;
+	const double *const ct;
+	const double *const st;
+	const unsigned int nlat_padded;
+	const unsigned int nlm_cplx;
+};
+#endif
+
+/* index macros (shtns.h:104-106) */
+#define LiM(shtns, l,im) ( (((im)*(2*shtns->lmax + 2 - ((im)+1)*shtns->mres))>>1) + (l) )
+#define LM(shtns, l,m) ( (((((unsigned short)(m))/shtns->mres)*(2*shtns->lmax + 2 - ((m)+shtns->mres)))>>1) + (l) )
+#define LM_LOOP( shtns, action ) { int lm=0; do { action } while(++lm < shtns->nlm); }
+#define LM_L_LOOP( shtns, action ) { int lm=0; do { int l=shtns->li[lm]; action } while(++lm < shtns->nlm); }
+#define NSPAT_ALLOC(shtns) (shtns->nspat)
+#define PHI_DEG(shtns, ip) (360./(shtns->nphi*shtns->mres))*(ip)
+#define PHI_RAD(shtns, ip) (2.*M_PI/(shtns->nphi*shtns->mres))*(ip)
+
+long nlm_calc(long lmax, long mmax, long mres);                 /* shtns.h:133 */
+long nlm_cplx_calc(long lmax, long mmax, long mres);            /* shtns.h:136 */
+void shtns_verbose(int);                                        /* shtns.h:138 */
+void shtns_print_version(void);                                 /* shtns.h:139 */
+const char* shtns_get_build_info(void);                         /* shtns.h:140 */
+void shtns_print_cfg(shtns_cfg);                                /* shtns.h:144 */
+
+shtns_cfg shtns_init(enum shtns_type flags, int lmax, int mmax, int mres, int nlat, int nphi);   /* shtns.h:149 */
+shtns_cfg shtns_create(int lmax, int mmax, int mres, enum shtns_norm norm);                     /* shtns.h:151 */
+int shtns_set_grid(shtns_cfg, enum shtns_type flags, double eps, int nlat, int nphi);           /* shtns.h:153 */
+int shtns_set_grid_auto(shtns_cfg, enum shtns_type flags, double eps, int nl_order, int *nlat, int *nphi); /* shtns.h:155 */
+shtns_cfg shtns_create_with_grid(shtns_cfg, int mmax, int nofft);                                /* shtns.h:157 */
+int shtns_use_threads(int num_threads);                         /* shtns.h:159 */
+int shtns_use_gpu(int device_id);                               /* shtns.h:161 */
+void shtns_reset(void);                                         /* shtns.h:163 */
+void shtns_destroy(shtns_cfg);                                  /* shtns.h:164 */
+void shtns_unset_grid(shtns_cfg);                               /* shtns.h:165 */
+void shtns_robert_form(shtns_cfg, int robert);                  /* shtns.h:168 */
+void* shtns_malloc(size_t bytes);                               /* shtns.h:170 */
+void shtns_free(void* p);                                       /* shtns.h:171 */
+
+double sh00_1(shtns_cfg);                                       /* shtns.h:178 */
+double sh10_ct(shtns_cfg);                                      /* shtns.h:179 */
+double sh11_st(shtns_cfg);                                      /* shtns.h:180 */
+double shlm_e1(shtns_cfg, int l, int m);                        /* shtns.h:181 */
+int shtns_gauss_wts(shtns_cfg, double *wts);                    /* shtns.h:183 */
+
+/* scalar transforms (shtns.h:262-267); spat_to_SH leaves Vr unchanged */
+void spat_to_SH(shtns_cfg shtns, double *Vr, cplx *Qlm);
+void SH_to_spat(shtns_cfg shtns, cplx *Qlm, double *Vr);
+/* 2-D vector transforms (shtns.h:282-288) */
+void spat_to_SHsphtor(shtns_cfg, double *Vt, double *Vp, cplx *Slm, cplx *Tlm);
+void SHsphtor_to_spat(shtns_cfg, cplx *Slm, cplx *Tlm, double *Vt, double *Vp);
+void SHsph_to_spat(shtns_cfg, cplx *Slm, double *Vt, double *Vp);
+void SHtor_to_spat(shtns_cfg, cplx *Tlm, double *Vt, double *Vp);
+#define SH_to_grad_spat(shtns, S,Gt,Gp) SHsph_to_spat(shtns, S, Gt, Gp)
+/* 3-D vector transforms (shtns.h:303-306) */
+void spat_to_SHqst(shtns_cfg, double *Vr, double *Vt, double *Vp, cplx *Qlm, cplx *Slm, cplx *Tlm);
+void SHqst_to_spat(shtns_cfg, cplx *Qlm, cplx *Slm, cplx *Tlm, double *Vr, double *Vt, double *Vp);
+/* truncated transforms (shtns.h:315-324) */
+void spat_to_SH_l(shtns_cfg, double *Vr, cplx *Qlm, int ltr);
+void SH_to_spat_l(shtns_cfg, cplx *Qlm, double *Vr, int ltr);
+void SHsphtor_to_spat_l(shtns_cfg, cplx *Slm, cplx *Tlm, double *Vt, double *Vp, int ltr);
+void SHsph_to_spat_l(shtns_cfg, cplx *Slm, double *Vt, double *Vp, int ltr);
+void SHtor_to_spat_l(shtns_cfg, cplx *Tlm, double *Vt, double *Vp, int ltr);
+void spat_to_SHsphtor_l(shtns_cfg, double *Vt, double *Vp, cplx *Slm, cplx *Tlm, int ltr);
+void spat_to_SHqst_l(shtns_cfg, double *Vr, double *Vt, double *Vp, cplx *Qlm, cplx *Slm, cplx *Tlm, int ltr);
+void SHqst_to_spat_l(shtns_cfg, cplx *Qlm, cplx *Slm, cplx *Tlm, double *Vr, double *Vt, double *Vp, int ltr);
+#define SH_to_grad_spat_l(shtns, S,Gt,Gp,ltr) SHsph_to_spat_l(shtns, S, Gt, Gp, ltr)
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHTNS_B200_SHTNS_H */

@@ -1,0 +1,49 @@
+/*
+ * shtns_b200.h -- entry points of shtns_b200 that have no counterpart in
+ * SHTns 3.5.2.  They sit beside the drop-in API of shtns.h / shtns_cuda.h.
+ */
+#ifndef SHTNS_B200_EXT_H
+#define SHTNS_B200_EXT_H
+
+#include <stddef.h>
+#include "shtns.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Batched transforms.  After shtns_set_batch(cfg, howmany, spec_dist,
+ * spat_dist) every transform of this plan (host and cu_* forms) processes
+ * `howmany` independent fields: field i of each spectral array starts at
+ * element i*spec_dist (complex elements, >= nlm) and field i of each spatial
+ * array at element i*spat_dist (doubles, >= nspat).  howmany = 1 restores the
+ * single-field behaviour.  Returns 0, or -1 for invalid arguments.
+ * No counterpart in SHTns 3.5.2 (its transforms take one field per call). */
+int shtns_set_batch(shtns_cfg, int howmany, long spec_dist, long spat_dist);
+
+/* Error handling.  By default, like SHTns 3.5.2 (sht_init.c:67-72), an invalid
+ * plan request prints a message and exits the process.  With
+ * shtns_b200_error_mode(1) the failing call instead returns NULL / -1 and the
+ * message is kept for shtns_b200_last_error().  Transform errors (invalid
+ * sizes, CUDA launch failures) never exit: they are recorded here and the
+ * transform returns without writing its outputs. */
+void shtns_b200_error_mode(int return_errors);
+const char* shtns_b200_last_error(void);
+/* 0 if no transform error happened since the last call, else a nonzero code
+ * (1 = invalid argument, 2 = CUDA error, 3 = allocation failure);
+ * the status is cleared by this call. */
+int shtns_b200_status(void);
+
+/* Device used by a plan and bytes of GPU memory it holds (tables + work). */
+int shtns_b200_device(shtns_cfg);
+size_t shtns_b200_device_bytes(shtns_cfg);
+
+/* Number of kernel launches issued by this library since process start (all
+ * plans).  Used to count the launches inside a timed region. */
+long shtns_b200_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHTNS_B200_EXT_H */

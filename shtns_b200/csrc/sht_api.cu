@@ -1,0 +1,298 @@
+// Transform entry points of shtns_b200.
+//
+// Device-pointer transforms (cu_*, reference sht_gpu.cu:495-577) enqueue three
+// kernels per direction on the plan's compute stream and return:
+//   synthesis: coefficient prologue -> Legendre contraction -> phi FFT
+//   analysis:  phi FFT -> Legendre contraction -> coefficient epilogue
+// Host-pointer transforms (SH_to_spat, ..., reference sht_com.c:26-126 with the
+// GPU offload of sht_gpu.cu:584-1489) copy their inputs to plan-owned device
+// staging, run the same pipeline and copy the outputs back before returning.
+#include "sht_internal.h"
+
+#include <cstring>
+#include <algorithm>
+
+namespace {
+
+bool ensure(void** p, size_t* cap, size_t bytes, const char* what)
+{
+	if (*cap >= bytes && *p) return true;
+	if (*p) cudaFree(*p);
+	*p = nullptr; *cap = 0;
+	if (cudaMalloc(p, bytes) != cudaSuccess) {
+		cudaGetLastError();
+		shtb_set_error(3, std::string("out of device memory for ") + what);
+		return false;
+	}
+	*cap = bytes;
+	return true;
+}
+
+struct Job {
+	int ncomp;
+	int type[3];      // 0 scalar, 1 V (theta / spheroidal), 2 W (phi / toroidal)
+	int nf, nfc, ncol, llim, mlim, vec_extra;
+};
+
+bool setup_job(shtns_cfg s, Job& j, int ncomp, const int* types, int ltr)
+{
+	if (!s || !s->grid_set) { shtb_set_error(1, "transform on a plan without grid"); return false; }
+	if (ltr < 0) { shtb_set_error(1, "negative truncation degree"); return false; }
+	j.ncomp = ncomp;
+	for (int c = 0; c < 3; c++) j.type[c] = (c < ncomp) ? types[c] : 0;
+	j.nf = s->batch;
+	j.nfc = j.nf * ncomp;
+	j.ncol = 16 * ((j.nfc + 3) / 4);
+	j.llim = std::min<int>(ltr, s->lmax);
+	j.mlim = std::min<int>(s->mmax, j.llim / s->mres);
+	j.vec_extra = 0;
+	for (int c = 0; c < ncomp; c++) if (types[c]) j.vec_extra = 1;
+	// work buffers
+	size_t qq_bytes = sizeof(double) * (size_t) s->ktot * j.ncol;
+	size_t F_bytes = sizeof(double2) * (size_t) j.nfc * (s->mmax + 1) * s->nlat;
+	size_t cq = s->qq_cap * sizeof(double), cf = s->F_cap * sizeof(double2);
+	if (!ensure((void**) &s->d_qq, &cq, qq_bytes, "coefficient buffer")) { s->qq_cap = 0; return false; }
+	s->qq_cap = cq / sizeof(double);
+	if (!ensure((void**) &s->d_F, &cf, F_bytes, "Fourier buffer")) { s->F_cap = 0; return false; }
+	s->F_cap = cf / sizeof(double2);
+	return true;
+}
+
+LegParams leg_params(shtns_cfg s, const Job& j)
+{
+	LegParams p;
+	memset(&p, 0, sizeof(p));
+	p.nlat = s->nlat; p.nlat_2 = s->nlat_2; p.llim = j.llim; p.mlim = j.mlim; p.mres = s->mres;
+	p.vec_extra = j.vec_extra; p.ncol = j.ncol; p.nfc = j.nfc;
+	p.south_first = s->south_first; p.robert = s->robert;
+	p.mpos_inv = 1.0 / s->mpos_renorm;
+	p.x = s->d_x; p.x2 = s->d_x2; p.sinv = s->d_sinv; p.w = s->d_w; p.c = s->d_c;
+	p.ck = s->d_ck; p.mt = s->mt;
+	p.nf = j.nf;
+	for (int c = 0; c < 3; c++) p.ctype[c] = j.type[c];
+	p.qq = s->d_qq; p.F = s->d_F;
+	p.fstride = (long)(s->mmax + 1) * s->nlat;
+	return p;
+}
+
+PrepParams prep_params(shtns_cfg s, const Job& j)
+{
+	PrepParams p;
+	memset(&p, 0, sizeof(p));
+	p.lmax = s->lmax; p.llim = j.llim; p.mlim = j.mlim; p.mres = s->mres;
+	p.nf = j.nf; p.ncomp = j.ncomp; p.ncol = j.ncol;
+	for (int c = 0; c < 3; c++) p.comp_type[c] = j.type[c];
+	p.spec_dist = s->spec_dist;
+	p.xs = s->d_xs; p.xa = s->d_xa;
+	p.stdt_lo = s->d_stdt_lo; p.stdt_hi = s->d_stdt_hi; p.van_lo = s->d_van_lo; p.van_hi = s->d_van_hi;
+	p.l2 = s->d_l2; p.mt = s->mt; p.qq = s->d_qq;
+	return p;
+}
+
+FftParams fft_params(shtns_cfg s, const Job& j)
+{
+	FftParams p;
+	memset(&p, 0, sizeof(p));
+	p.N = s->nphi; p.nlat = s->nlat; p.mlim = j.mlim;
+	p.nradix = (int) s->fft_radix.size();
+	p.rcode = 0;
+	int rmin = 8;
+	for (int i = 0; i < p.nradix; i++) {
+		p.rcode |= (unsigned long long) s->fft_radix[i] << (4 * i);
+		rmin = std::min(rmin, s->fft_radix[i]);
+	}
+	(void) rmin;
+	// latitude pairs per CTA: up to 4 (8 latitudes) with two buffers of S*nphi
+	// complex in shared memory (at most 98 KB so two CTAs fit on an SM)
+	int S = std::max(1, std::min(4, 3072 / (int) s->nphi));
+	while (S > 1 && 2 * S > (int) s->nlat) S--;
+	p.S = S;
+	p.tw = s->d_tw; p.F = s->d_F;
+	p.fstride = (long)(s->mmax + 1) * s->nlat;
+	p.nf = j.nf; p.spat_dist = s->spat_dist;
+	p.phi_contiguous = s->phi_contiguous;
+	return p;
+}
+
+bool check_launch(const char* what)
+{
+	return shtb_cuda_ok(cudaGetLastError(), what);
+}
+
+// ---- device pipelines ----
+void run_synth(shtns_cfg s, int ncomp, const int* types, const cplx* Q, const cplx* S, const cplx* T,
+               double* o0, double* o1, double* o2, int ltr)
+{
+	Job j;
+	if (!setup_job(s, j, ncomp, types, ltr)) return;
+	PrepParams pp = prep_params(s, j);
+	pp.Q = reinterpret_cast<const double2*>(Q);
+	pp.S = reinterpret_cast<const double2*>(S);
+	pp.T = reinterpret_cast<const double2*>(T);
+	launch_prep_synth(pp, s->comp_stream);
+	LegParams lp = leg_params(s, j);
+	launch_leg_synth(lp, s->comp_stream);
+	FftParams fp = fft_params(s, j);
+	fp.spat[0] = o0; fp.spat[1] = o1; fp.spat[2] = o2;
+	launch_fft_synth(fp, j.nfc, s->comp_stream);
+	check_launch("synthesis launch");
+}
+
+void run_analys(shtns_cfg s, int ncomp, const int* types, const double* i0, const double* i1, const double* i2,
+                cplx* Qo, cplx* So, cplx* To, int ltr)
+{
+	Job j;
+	if (!setup_job(s, j, ncomp, types, ltr)) return;
+	FftParams fp = fft_params(s, j);
+	fp.spat_in[0] = i0; fp.spat_in[1] = i1; fp.spat_in[2] = i2;
+	launch_fft_analys(fp, j.nfc, s->comp_stream);
+	LegParams lp = leg_params(s, j);
+	int kmax_all = 0;
+	for (int im = 0; im <= j.mlim; im++) kmax_all = std::max(kmax_all, (j.llim + j.vec_extra - im * s->mres) / 2 + 1);
+	launch_leg_analys(lp, kmax_all, s->comp_stream);
+	PrepParams pp = prep_params(s, j);
+	pp.Qo = reinterpret_cast<double2*>(Qo);
+	pp.So = reinterpret_cast<double2*>(So);
+	pp.To = reinterpret_cast<double2*>(To);
+	launch_post_analys_m(pp, s->mmax, s->comp_stream);
+	check_launch("analysis launch");
+}
+
+const int T_SCAL[1] = {0};
+const int T_VEC[2] = {1, 2};
+const int T_QST[3] = {0, 1, 2};
+
+// ---- host-pointer forms: stage through device memory ----
+struct Stage {
+	double2* spec[3];
+	double* spat[3];
+};
+
+bool stage_alloc(shtns_cfg s, int nspec, int nspatial, Stage& st)
+{
+	const size_t spec_elems = (size_t)(s->batch - 1) * s->spec_dist + s->nlm;
+	const size_t spat_elems = (size_t)(s->batch - 1) * s->spat_dist + s->nspat;
+	const size_t spec_b = (sizeof(double2) * spec_elems + 255) & ~(size_t) 255;
+	const size_t spat_b = (sizeof(double) * spat_elems + 255) & ~(size_t) 255;
+	const size_t total = nspec * spec_b + nspatial * spat_b;
+	if (!ensure(&s->d_stage, &s->stage_cap, total, "staging buffers")) return false;
+	char* base = (char*) s->d_stage;
+	for (int i = 0; i < 3; i++) { st.spec[i] = nullptr; st.spat[i] = nullptr; }
+	for (int i = 0; i < nspec; i++) { st.spec[i] = (double2*) base; base += spec_b; }
+	for (int i = 0; i < nspatial; i++) { st.spat[i] = (double*) base; base += spat_b; }
+	return true;
+}
+
+size_t spec_bytes(shtns_cfg s) { return sizeof(double2) * ((size_t)(s->batch - 1) * s->spec_dist + s->nlm); }
+size_t spat_bytes(shtns_cfg s) { return sizeof(double) * ((size_t)(s->batch - 1) * s->spat_dist + s->nspat); }
+
+void h_synth(shtns_cfg s, int ncomp, const int* types, const cplx* Q, const cplx* S, const cplx* T,
+             double* o0, double* o1, double* o2, int ltr)
+{
+	if (!s || !s->grid_set) { shtb_set_error(1, "transform on a plan without grid"); return; }
+	const int nin = (Q ? 1 : 0) + (S ? 1 : 0) + (T ? 1 : 0);
+	Stage st;
+	if (!stage_alloc(s, nin, ncomp, st)) return;
+	int k = 0;
+	const double2* dQ = nullptr; const double2* dS = nullptr; const double2* dT = nullptr;
+	cudaStream_t cs = s->comp_stream;
+	if (Q) { cudaMemcpyAsync(st.spec[k], Q, spec_bytes(s), cudaMemcpyHostToDevice, cs); dQ = st.spec[k++]; }
+	if (S) { cudaMemcpyAsync(st.spec[k], S, spec_bytes(s), cudaMemcpyHostToDevice, cs); dS = st.spec[k++]; }
+	if (T) { cudaMemcpyAsync(st.spec[k], T, spec_bytes(s), cudaMemcpyHostToDevice, cs); dT = st.spec[k++]; }
+	run_synth(s, ncomp, types, (const cplx*) dQ, (const cplx*) dS, (const cplx*) dT, st.spat[0], st.spat[1], st.spat[2], ltr);
+	double* outs[3] = {o0, o1, o2};
+	for (int c = 0; c < ncomp; c++) cudaMemcpyAsync(outs[c], st.spat[c], spat_bytes(s), cudaMemcpyDeviceToHost, cs);
+	shtb_cuda_ok(cudaStreamSynchronize(cs), "synthesis");
+}
+
+void h_analys(shtns_cfg s, int ncomp, const int* types, const double* i0, const double* i1, const double* i2,
+              cplx* Qo, cplx* So, cplx* To, int ltr)
+{
+	if (!s || !s->grid_set) { shtb_set_error(1, "transform on a plan without grid"); return; }
+	Stage st;
+	if (!stage_alloc(s, ncomp, ncomp, st)) return;
+	cudaStream_t cs = s->comp_stream;
+	const double* ins[3] = {i0, i1, i2};
+	for (int c = 0; c < ncomp; c++) cudaMemcpyAsync(st.spat[c], ins[c], spat_bytes(s), cudaMemcpyHostToDevice, cs);
+	double2* outs_d[3] = {nullptr, nullptr, nullptr};
+	cplx* outs_h[3] = {nullptr, nullptr, nullptr};
+	int k = 0;
+	if (Qo) { outs_d[0] = st.spec[k++]; outs_h[0] = Qo; }
+	if (So) { outs_d[1] = st.spec[k++]; outs_h[1] = So; }
+	if (To) { outs_d[2] = st.spec[k++]; outs_h[2] = To; }
+	run_analys(s, ncomp, types, st.spat[0], st.spat[1], st.spat[2],
+	           (cplx*) outs_d[0], (cplx*) outs_d[1], (cplx*) outs_d[2], ltr);
+	for (int c = 0; c < 3; c++)
+		if (outs_h[c]) cudaMemcpyAsync(outs_h[c], outs_d[c], spec_bytes(s), cudaMemcpyDeviceToHost, cs);
+	shtb_cuda_ok(cudaStreamSynchronize(cs), "analysis");
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" int shtns_set_batch(shtns_cfg s, int howmany, long spec_dist, long spat_dist)
+{
+	if (!s || howmany < 1) { shtb_set_error(1, "shtns_set_batch: invalid arguments"); return -1; }
+	if (spec_dist < (long) s->nlm) spec_dist = s->nlm;
+	if (spat_dist < (long) s->nspat) spat_dist = s->nspat;
+	s->batch = howmany; s->spec_dist = spec_dist; s->spat_dist = spat_dist;
+	return 0;
+}
+
+// ---- device-pointer API (shtns_cuda.h) ----
+extern "C" void cu_SH_to_spat(shtns_cfg s, cplx* Qlm, double* Vr, int ltr)
+{ run_synth(s, 1, T_SCAL, Qlm, nullptr, nullptr, Vr, nullptr, nullptr, ltr); }
+
+extern "C" void cu_spat_to_SH(shtns_cfg s, double* Vr, cplx* Qlm, int ltr)
+{ run_analys(s, 1, T_SCAL, Vr, nullptr, nullptr, Qlm, nullptr, nullptr, ltr); }
+
+extern "C" void cu_SHsphtor_to_spat(shtns_cfg s, cplx* Slm, cplx* Tlm, double* Vt, double* Vp, int ltr)
+{ run_synth(s, 2, T_VEC, nullptr, Slm, Tlm, Vt, Vp, nullptr, ltr); }
+
+extern "C" void cu_spat_to_SHsphtor(shtns_cfg s, double* Vt, double* Vp, cplx* Slm, cplx* Tlm, int ltr)
+{ run_analys(s, 2, T_VEC, Vt, Vp, nullptr, nullptr, Slm, Tlm, ltr); }
+
+extern "C" void cu_SHqst_to_spat(shtns_cfg s, cplx* Qlm, cplx* Slm, cplx* Tlm, double* Vr, double* Vt, double* Vp, int ltr)
+{ run_synth(s, 3, T_QST, Qlm, Slm, Tlm, Vr, Vt, Vp, ltr); }
+
+extern "C" void cu_spat_to_SHqst(shtns_cfg s, double* Vr, double* Vt, double* Vp, cplx* Qlm, cplx* Slm, cplx* Tlm, int ltr)
+{ run_analys(s, 3, T_QST, Vr, Vt, Vp, Qlm, Slm, Tlm, ltr); }
+
+// Single-precision device transforms (shtns_cuda.h:410,414) are not provided:
+// the FP64 path is the product; these report an error instead of computing.
+extern "C" void cu_SH_to_spat_float(shtns_cfg, cplx_f*, float*, int)
+{ shtb_set_error(1, "cu_SH_to_spat_float is not provided by shtns_b200"); }
+extern "C" void cu_spat_to_SH_float(shtns_cfg, float*, cplx_f*, int)
+{ shtb_set_error(1, "cu_spat_to_SH_float is not provided by shtns_b200"); }
+
+// ---- host-pointer API (shtns.h) ----
+extern "C" void SH_to_spat(shtns_cfg s, cplx* Qlm, double* Vr) { h_synth(s, 1, T_SCAL, Qlm, nullptr, nullptr, Vr, nullptr, nullptr, s ? s->lmax : 0); }
+extern "C" void SH_to_spat_l(shtns_cfg s, cplx* Qlm, double* Vr, int ltr) { h_synth(s, 1, T_SCAL, Qlm, nullptr, nullptr, Vr, nullptr, nullptr, ltr); }
+extern "C" void spat_to_SH(shtns_cfg s, double* Vr, cplx* Qlm) { h_analys(s, 1, T_SCAL, Vr, nullptr, nullptr, Qlm, nullptr, nullptr, s ? s->lmax : 0); }
+extern "C" void spat_to_SH_l(shtns_cfg s, double* Vr, cplx* Qlm, int ltr) { h_analys(s, 1, T_SCAL, Vr, nullptr, nullptr, Qlm, nullptr, nullptr, ltr); }
+
+extern "C" void SHsphtor_to_spat(shtns_cfg s, cplx* Slm, cplx* Tlm, double* Vt, double* Vp)
+{ h_synth(s, 2, T_VEC, nullptr, Slm, Tlm, Vt, Vp, nullptr, s ? s->lmax : 0); }
+extern "C" void SHsphtor_to_spat_l(shtns_cfg s, cplx* Slm, cplx* Tlm, double* Vt, double* Vp, int ltr)
+{ h_synth(s, 2, T_VEC, nullptr, Slm, Tlm, Vt, Vp, nullptr, ltr); }
+extern "C" void SHsph_to_spat(shtns_cfg s, cplx* Slm, double* Vt, double* Vp)
+{ h_synth(s, 2, T_VEC, nullptr, Slm, nullptr, Vt, Vp, nullptr, s ? s->lmax : 0); }
+extern "C" void SHsph_to_spat_l(shtns_cfg s, cplx* Slm, double* Vt, double* Vp, int ltr)
+{ h_synth(s, 2, T_VEC, nullptr, Slm, nullptr, Vt, Vp, nullptr, ltr); }
+extern "C" void SHtor_to_spat(shtns_cfg s, cplx* Tlm, double* Vt, double* Vp)
+{ h_synth(s, 2, T_VEC, nullptr, nullptr, Tlm, Vt, Vp, nullptr, s ? s->lmax : 0); }
+extern "C" void SHtor_to_spat_l(shtns_cfg s, cplx* Tlm, double* Vt, double* Vp, int ltr)
+{ h_synth(s, 2, T_VEC, nullptr, nullptr, Tlm, Vt, Vp, nullptr, ltr); }
+extern "C" void spat_to_SHsphtor(shtns_cfg s, double* Vt, double* Vp, cplx* Slm, cplx* Tlm)
+{ h_analys(s, 2, T_VEC, Vt, Vp, nullptr, nullptr, Slm, Tlm, s ? s->lmax : 0); }
+extern "C" void spat_to_SHsphtor_l(shtns_cfg s, double* Vt, double* Vp, cplx* Slm, cplx* Tlm, int ltr)
+{ h_analys(s, 2, T_VEC, Vt, Vp, nullptr, nullptr, Slm, Tlm, ltr); }
+
+extern "C" void SHqst_to_spat(shtns_cfg s, cplx* Qlm, cplx* Slm, cplx* Tlm, double* Vr, double* Vt, double* Vp)
+{ h_synth(s, 3, T_QST, Qlm, Slm, Tlm, Vr, Vt, Vp, s ? s->lmax : 0); }
+extern "C" void SHqst_to_spat_l(shtns_cfg s, cplx* Qlm, cplx* Slm, cplx* Tlm, double* Vr, double* Vt, double* Vp, int ltr)
+{ h_synth(s, 3, T_QST, Qlm, Slm, Tlm, Vr, Vt, Vp, ltr); }
+extern "C" void spat_to_SHqst(shtns_cfg s, double* Vr, double* Vt, double* Vp, cplx* Qlm, cplx* Slm, cplx* Tlm)
+{ h_analys(s, 3, T_QST, Vr, Vt, Vp, Qlm, Slm, Tlm, s ? s->lmax : 0); }
+extern "C" void spat_to_SHqst_l(shtns_cfg s, double* Vr, double* Vt, double* Vp, cplx* Qlm, cplx* Slm, cplx* Tlm, int ltr)
+{ h_analys(s, 3, T_QST, Vr, Vt, Vp, Qlm, Slm, Tlm, ltr); }

@@ -1,0 +1,309 @@
+// Longitude (phi) FFT stage on sm_100a.
+//
+// Replaces the reference's FFTW / cuFFT step (sht_init.c:353-518,
+// sht_gpu.cu:372-446).  As in the reference, two real latitudes a, b are
+// packed into one complex sequence z = v_a + i v_b, so one complex DFT of
+// length nphi transforms a latitude pair; the spectra are separated with
+// Hermitian symmetry.  Each CTA owns one field-component and 2*S consecutive
+// latitudes, holds the S complex sequences in shared memory and runs an
+// mixed-radix (8, 4, 2, 3, 5, 7) self-sorting Stockham transform between two
+// shared-memory buffers.
+//
+// Synthesis input is F[fc][m][theta] (m <= mlim, exact Fourier coefficients of
+// each latitude); output is v(phi_j) = sum_m (2 - delta_m0) Re(F_m e^{i m phi_j}).
+// Analysis computes F_m = (1/nphi) sum_j v(phi_j) e^{-i m phi_j}.
+// The spatial arrays are theta-contiguous (v[j*nlat + theta]) or
+// phi-contiguous (v[theta*nphi + j]).
+#include "sht_internal.h"
+
+namespace {
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+	return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// multiply by sign*i
+__device__ __forceinline__ double2 mul_si(double2 a, int sign) { return sign > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x); }
+
+template <int R> struct Dft;
+
+template <> struct Dft<2> {
+	static __device__ __forceinline__ void run(double2* u, int) {
+		double2 a = u[0], b = u[1];
+		u[0] = cadd(a, b); u[1] = csub(a, b);
+	}
+};
+template <> struct Dft<4> {
+	static __device__ __forceinline__ void run(double2* u, int s) {
+		double2 t0 = cadd(u[0], u[2]), t1 = csub(u[0], u[2]);
+		double2 t2 = cadd(u[1], u[3]), t3 = mul_si(csub(u[1], u[3]), s);
+		u[0] = cadd(t0, t2); u[2] = csub(t0, t2);
+		u[1] = cadd(t1, t3); u[3] = csub(t1, t3);
+	}
+};
+template <> struct Dft<8> {
+	static __device__ __forceinline__ void run(double2* u, int s) {
+		const double h = 0.70710678118654752440084436210485;
+		// radix-2 split into even / odd halves, each a 4-point DFT
+		double2 e[4] = {u[0], u[2], u[4], u[6]};
+		double2 o[4] = {u[1], u[3], u[5], u[7]};
+		Dft<4>::run(e, s);
+		Dft<4>::run(o, s);
+		// twiddles w8^q = exp(s*i*pi*q/4)
+		double2 o1 = make_double2(h * (o[1].x - s * o[1].y), h * (o[1].y + s * o[1].x));
+		double2 o2 = mul_si(o[2], s);
+		double2 o3 = make_double2(h * (-o[3].x - s * o[3].y), h * (-o[3].y + s * o[3].x));
+		u[0] = cadd(e[0], o[0]); u[4] = csub(e[0], o[0]);
+		u[1] = cadd(e[1], o1);   u[5] = csub(e[1], o1);
+		u[2] = cadd(e[2], o2);   u[6] = csub(e[2], o2);
+		u[3] = cadd(e[3], o3);   u[7] = csub(e[3], o3);
+	}
+};
+template <> struct Dft<3> {
+	static __device__ __forceinline__ void run(double2* u, int s) {
+		const double c1 = -0.5, s1 = s * 0.86602540378443864676372317075294;
+		double2 t = cadd(u[1], u[2]), d = csub(u[1], u[2]);
+		double2 mm = make_double2(fma(c1, t.x, u[0].x), fma(c1, t.y, u[0].y));
+		u[0] = cadd(u[0], t);
+		u[1] = make_double2(mm.x - s1 * d.y, mm.y + s1 * d.x);
+		u[2] = make_double2(mm.x + s1 * d.y, mm.y - s1 * d.x);
+	}
+};
+template <> struct Dft<5> {
+	static __device__ __forceinline__ void run(double2* u, int s) {
+		const double c1 = 0.30901699437494742410229341718282;   // cos(2pi/5)
+		const double c2 = -0.80901699437494742410229341718282;  // cos(4pi/5)
+		const double s1 = s * 0.95105651629515357211643933337938;  // sin(2pi/5)
+		const double s2 = s * 0.58778525229247312916870595463907;  // sin(4pi/5)
+		double2 a1 = cadd(u[1], u[4]), b1 = csub(u[1], u[4]);
+		double2 a2 = cadd(u[2], u[3]), b2 = csub(u[2], u[3]);
+		double2 x0 = u[0];
+		u[0] = cadd(x0, cadd(a1, a2));
+		double2 r1 = make_double2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+		double2 r2 = make_double2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+		// i*(s1 b1 + s2 b2) and i*(s2 b1 - s1 b2)
+		double2 i1 = make_double2(-(s1 * b1.y + s2 * b2.y), s1 * b1.x + s2 * b2.x);
+		double2 i2 = make_double2(-(s2 * b1.y - s1 * b2.y), s2 * b1.x - s1 * b2.x);
+		u[1] = cadd(r1, i1); u[4] = csub(r1, i1);
+		u[2] = cadd(r2, i2); u[3] = csub(r2, i2);
+	}
+};
+// 7-point DFT as a direct sum with the roots of unity as literals
+// (cos, sin of 2 pi k / 7, symmetric pairs folded).
+template <> struct Dft<7> {
+	static __device__ __forceinline__ void run(double2* u, int s) {
+		const double c[4] = {1.0, 0.62348980185873353053, -0.22252093395631440429, -0.90096886790241912624};
+		const double sn[4] = {0.0, 0.78183148246802980871, 0.97492791218182360702, 0.43388373911755812048};
+		double2 a[4], b[4];
+		#pragma unroll
+		for (int q = 1; q < 4; q++) { a[q] = cadd(u[q], u[7 - q]); b[q] = csub(u[q], u[7 - q]); }
+		const double2 x0 = u[0];
+		u[0] = cadd(x0, cadd(a[1], cadd(a[2], a[3])));
+		#pragma unroll
+		for (int k = 1; k < 4; k++) {
+			double2 r = x0, im = make_double2(0.0, 0.0);
+			#pragma unroll
+			for (int q = 1; q < 4; q++) {
+				const int j = (q * k) % 7;
+				const double cq = (j < 4) ? c[j] : c[7 - j];
+				const double sq = (j < 4) ? sn[j] : -sn[7 - j];
+				r.x = fma(cq, a[q].x, r.x);  r.y = fma(cq, a[q].y, r.y);
+				im.x = fma(sq, b[q].x, im.x); im.y = fma(sq, b[q].y, im.y);
+			}
+			// y_k = r + i s im,  y_{7-k} = r - i s im
+			const double2 t = make_double2(-s * im.y, s * im.x);
+			u[k] = cadd(r, t);
+			u[7 - k] = csub(r, t);
+		}
+	}
+};
+
+// One Stockham pass of radix R over S sequences of length N, from X to Y.
+// Butterfly b of a sequence reads X[b + q*N/R] (q < R), applies twiddles
+// w^{q*k*N/(p*R)} with k = b mod p, runs the R-point DFT and writes
+// Y[(b - k)*R + k + q*p].
+template <int R>
+__device__ __forceinline__ void fft_pass(const double2* __restrict__ X, double2* __restrict__ Y, int N, int S, int p,
+                                         const double2* __restrict__ tw, int sign)
+{
+	const int nbf = N / R;
+	const int total = S * nbf;
+	const int tstep = N / (p * R);
+	for (int g = threadIdx.x; g < total; g += blockDim.x) {
+		const int sq = g / nbf, b = g - sq * nbf;
+		const int k = b % p;
+		const double2* x = X + sq * N;
+		double2 u[R];
+		#pragma unroll
+		for (int q = 0; q < R; q++) u[q] = x[b + q * nbf];
+		if (k) {
+			#pragma unroll
+			for (int q = 1; q < R; q++) {
+				double2 w = __ldg(tw + q * k * tstep);
+				if (sign < 0) w.y = -w.y;
+				u[q] = cmul(u[q], w);
+			}
+		}
+		Dft<R>::run(u, sign);
+		double2* y = Y + sq * N + (b - k) * R + k;
+		#pragma unroll
+		for (int q = 0; q < R; q++) y[q * p] = u[q];
+	}
+	__syncthreads();
+}
+
+// Runs all passes; the result ends in X or Y, returned.
+__device__ __forceinline__ double2* fft_run(double2* X, double2* Y, int N, int S, unsigned long long rcode, int nradix,
+                                            const double2* __restrict__ tw, int sign)
+{
+	int pp = 1;
+	for (int r = 0; r < nradix; r++) {
+		const int R = (int)((rcode >> (4 * r)) & 15);
+		switch (R) {
+			case 8: fft_pass<8>(X, Y, N, S, pp, tw, sign); break;
+			case 4: fft_pass<4>(X, Y, N, S, pp, tw, sign); break;
+			case 2: fft_pass<2>(X, Y, N, S, pp, tw, sign); break;
+			case 3: fft_pass<3>(X, Y, N, S, pp, tw, sign); break;
+			case 5: fft_pass<5>(X, Y, N, S, pp, tw, sign); break;
+			default: fft_pass<7>(X, Y, N, S, pp, tw, sign); break;
+		}
+		pp *= R;
+		double2* t = X; X = Y; Y = t;
+	}
+	return X;
+}
+
+__device__ __forceinline__ double* spat_ptr(double* const* base, int fc, int nf, long dist)
+{
+	const int c = fc / nf;
+	return base[c] + (long)(fc - c * nf) * dist;
+}
+
+__global__ void fft_synth_kernel(FftParams p)
+{
+	extern __shared__ double2 smem[];
+	double2* X = smem;
+	const int fc = blockIdx.y;
+	const int lat0 = blockIdx.x * 2 * p.S;
+	const int N = p.N, S = p.S, T = blockDim.x;
+	double2* Y = smem + S * N;
+	const double2* Ff = p.F + (long)fc * p.fstride;
+	for (int e = threadIdx.x; e < S * N; e += T) X[e] = make_double2(0.0, 0.0);
+	__syncthreads();
+	// Z_k = A_k + i B_k,  Z_{N-k} = conj(A_k) + i conj(B_k)
+	for (int e = threadIdx.x; e < (p.mlim + 1) * S; e += T) {
+		const int k = e / S, sq = e - k * S;
+		const int ra = lat0 + 2 * sq;
+		double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+		if (ra < p.nlat) a = Ff[(long)k * p.nlat + ra];
+		if (ra + 1 < p.nlat) b = Ff[(long)k * p.nlat + ra + 1];
+		if (k == 0) { a.y = 0.0; b.y = 0.0; }
+		X[sq * N + k] = make_double2(a.x - b.y, a.y + b.x);
+		if (k > 0) X[sq * N + N - k] = make_double2(a.x + b.y, b.x - a.y);
+	}
+	__syncthreads();
+	X = fft_run(X, Y, N, S, p.rcode, p.nradix, p.tw, +1);
+	double* out = spat_ptr(p.spat, fc, p.nf, p.spat_dist);
+	const int nl = 2 * S;
+	if (!p.phi_contiguous) {
+		for (int e = threadIdx.x; e < N * nl; e += T) {
+			const int j = e / nl, l = e - j * nl;
+			const int row = lat0 + l;
+			if (row < p.nlat) {
+				const double2 z = X[(l >> 1) * N + j];
+				out[(long)j * p.nlat + row] = (l & 1) ? z.y : z.x;
+			}
+		}
+	} else {
+		for (int e = threadIdx.x; e < N * nl; e += T) {
+			const int l = e / N, j = e - l * N;
+			const int row = lat0 + l;
+			if (row < p.nlat) {
+				const double2 z = X[(l >> 1) * N + j];
+				out[(long)row * N + j] = (l & 1) ? z.y : z.x;
+			}
+		}
+	}
+}
+
+__global__ void fft_analys_kernel(FftParams p)
+{
+	extern __shared__ double2 smem[];
+	double2* X = smem;
+	const int fc = blockIdx.y;
+	const int lat0 = blockIdx.x * 2 * p.S;
+	const int N = p.N, S = p.S, T = blockDim.x;
+	double2* Y = smem + S * N;
+	const int c = fc / p.nf;
+	const double* in = p.spat_in[c] + (long)(fc - c * p.nf) * p.spat_dist;
+	const int nl = 2 * S;
+	double* Xd = reinterpret_cast<double*>(X);
+	if (!p.phi_contiguous) {
+		for (int e = threadIdx.x; e < N * nl; e += T) {
+			const int j = e / nl, l = e - j * nl;
+			const int row = lat0 + l;
+			const double v = (row < p.nlat) ? in[(long)j * p.nlat + row] : 0.0;
+			Xd[2 * ((l >> 1) * N + j) + (l & 1)] = v;
+		}
+	} else {
+		for (int e = threadIdx.x; e < N * nl; e += T) {
+			const int l = e / N, j = e - l * N;
+			const int row = lat0 + l;
+			const double v = (row < p.nlat) ? in[(long)row * N + j] : 0.0;
+			Xd[2 * ((l >> 1) * N + j) + (l & 1)] = v;
+		}
+	}
+	__syncthreads();
+	X = fft_run(X, Y, N, S, p.rcode, p.nradix, p.tw, -1);
+	double2* Ff = p.F + (long)fc * p.fstride;
+	const double sc = 0.5 / N;
+	for (int e = threadIdx.x; e < (p.mlim + 1) * S; e += T) {
+		const int k = e / S, sq = e - k * S;
+		const int ra = lat0 + 2 * sq;
+		const double2 z = X[sq * N + k];
+		const double2 w = X[sq * N + (k ? N - k : 0)];
+		// A = (Z_k + conj Z_{N-k})/2,  B = (Z_k - conj Z_{N-k})/(2i)
+		const double2 a = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
+		const double2 b = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
+		if (ra < p.nlat) Ff[(long)k * p.nlat + ra] = a;
+		if (ra + 1 < p.nlat) Ff[(long)k * p.nlat + ra + 1] = b;
+	}
+}
+
+} // namespace
+
+int fft_threads(int N, int S, unsigned long long rcode, int nradix)
+{
+	(void) rcode; (void) nradix;
+	// about two radix-8 butterflies per thread
+	const int need = S * N / 16;
+	int T = 128;
+	while (T < need && T < 512) T *= 2;
+	return T;
+}
+
+void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st)
+{
+	const int T = fft_threads(p.N, p.S, p.rcode, p.nradix);
+	const size_t smem = 2 * sizeof(double2) * p.S * p.N;
+	dim3 grid((p.nlat + 2 * p.S - 1) / (2 * p.S), nfc);
+	fft_synth_kernel<<<grid, T, smem, st>>>(p);
+	shtb_count_launch();
+}
+
+void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st)
+{
+	const int T = fft_threads(p.N, p.S, p.rcode, p.nradix);
+	const size_t smem = 2 * sizeof(double2) * p.S * p.N;
+	dim3 grid((p.nlat + 2 * p.S - 1) / (2 * p.S), nfc);
+	fft_analys_kernel<<<grid, T, smem, st>>>(p);
+	shtb_count_launch();
+}
+
+void fft_set_smem_limits()
+{
+	cudaFuncSetAttribute(fft_synth_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+	cudaFuncSetAttribute(fft_analys_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}

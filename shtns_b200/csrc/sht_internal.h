@@ -1,0 +1,150 @@
+// Private definitions of shtns_b200: the plan structure, the per-order (m)
+// table layout in GPU memory and the kernel launch interfaces.
+#pragma once
+
+#define SHTNS_B200_PRIVATE
+#include "../../include/shtns.h"
+#include "../../include/shtns_cuda.h"
+#include "../../include/shtns_b200.h"
+
+#include <cuda_runtime.h>
+#include <vector>
+#include <string>
+#include <cstdint>
+
+// Tile sizes of the Legendre contraction kernels (see sht_legendre.cu).
+#define LG_BM 64      // synthesis: theta rows per CTA;  analysis: k rows per CTA
+#define LG_BN 64      // real columns per CTA (16 field-components x {E,O} x {re,im})
+#define LG_BK 32      // synthesis: k per chunk;  analysis: theta rows per chunk
+#define LG_SEG 32     // recurrence checkpoint spacing in k (== LG_BK)
+#define LG_THREADS 256
+
+#define FFT_MAX_FACTORS 16
+#define FFT_NB 2      // butterflies held in registers per thread and pass
+
+// Per-order metadata, one entry per im = 0..mmax (int arrays on the device).
+struct MTables {
+	int* koff;    // first row of order im in the k-major coefficient buffer
+	int* coff;    // offset into the Ishioka recurrence coefficients (2 per k)
+	int* xoff;    // offset into the Ishioka basis-change coefficients (3 per k)
+	int* voff;    // offset into per-degree vector coefficients (degrees m..lmax+1)
+	int* ckoff;   // first checkpoint segment of order im
+	int* tm;      // first theta row (north index) kept by the polar threshold
+};
+
+// Public prefix must stay identical to shtns.h:struct shtns_info.
+struct shtns_info {
+	unsigned int nlm;
+	unsigned short lmax;
+	unsigned short mmax;
+	unsigned short mres;
+	unsigned short nlat_2;
+	unsigned int nlat;
+	unsigned int nphi;
+	unsigned int nspat;
+	unsigned short *li;
+	unsigned short *mi;
+	double *ct, *st;
+	unsigned int nlat_padded;
+	unsigned int nlm_cplx;
+	// ---------------- private ----------------
+	int norm_flags;          // shtns_norm | SHT_NO_CS_PHASE | SHT_REAL_NORM
+	int base_norm;           // shtns_norm without flags
+	int cs_phase;            // 1 with Condon-Shortley phase
+	double mpos_renorm;      // 1.0 (complex convention) or 0.5 (SHT_REAL_NORM)
+	int layout;              // layout bits given to shtns_set_grid
+	int phi_contiguous;
+	int south_first;
+	int robert;
+	int grid_set;
+	double eps;
+	int batch;               // fields per transform
+	long spec_dist, spat_dist;
+	// host tables
+	std::vector<unsigned short> li_v, mi_v;
+	std::vector<double> ct_v, st_v;      // full grid (public ct/st point here)
+	std::vector<double> wq;              // Gauss weights of the north rows (sum over both hemispheres = 2)
+	std::vector<double> alm;             // classic recurrence: per m pairs, reference layout (sht_legendre.c:630-657)
+	std::vector<long> alm_off;           // offset of order im in alm
+	std::vector<double> ish_c;           // Ishioka recurrence coefficients (2 per k)
+	std::vector<double> ish_xs, ish_xa;  // Ishioka basis change for synthesis / analysis (3 per k)
+	std::vector<double> stdt_lo, stdt_hi, van_lo, van_hi;   // per degree l = m..lmax+1
+	std::vector<double> l_2;             // 1/(l(l+1)), l_2[0] = 0
+	std::vector<int> koff_h, coff_h, xoff_h, voff_h, ckoff_h, tm_h, kmax_h;
+	long ktot, ctot, xtot, vtot, segtot;
+	std::vector<int> fft_radix;          // factorisation of nphi
+	double Y00_1, Y10_ct, Y11_st;
+	// device tables
+	int dev;
+	double *d_x, *d_x2, *d_s, *d_sinv, *d_w;   // north rows: |cos|, cos^2, sin, 1/sin, analysis weights
+	double *d_c, *d_xs, *d_xa;
+	double *d_stdt_lo, *d_stdt_hi, *d_van_lo, *d_van_hi, *d_l2;
+	double2 *d_ck;                      // checkpoints (Y_k, Y_k+1), [segment][north row]
+	double2 *d_tw;                       // exp(+2 pi i j / nphi), j < nphi
+	MTables mt;
+	int *d_mint;                         // backing store of mt
+	size_t table_bytes;
+	// work buffers (grow on demand)
+	double *d_qq; size_t qq_cap;         // k-major coefficient buffer [row][col]
+	double2 *d_F; size_t F_cap;          // Fourier coefficients [fc][im][theta]
+	void *d_stage; size_t stage_cap;     // device staging for host-pointer transforms
+	cudaStream_t comp_stream, xfer_stream;
+	int own_xfer;
+	int is_clone;
+	shtns_cfg base;                      // plan whose tables a clone shares (NULL for originals)
+	int nclones;
+};
+
+// ---- kernel parameter blocks ----
+struct LegParams {
+	int nlat, nlat_2, llim, mlim, mres, vec_extra;
+	int ncol, nfc;
+	int south_first, robert;
+	double mpos_inv;                     // analysis factor for m>0 (1/mpos_renorm)
+	const double *x, *x2, *sinv, *w, *c;
+	const double2 *ck;
+	MTables mt;
+	int nf;                              // fields per component (fc = component * nf + field)
+	int ctype[3];                        // per component: 0 scalar, 1 V, 2 W
+	double *qq;                          // coefficient buffer
+	double2 *F;                          // Fourier buffer
+	long fstride;                        // complex elements between field-components in F
+};
+
+struct PrepParams {
+	int lmax, llim, mlim, mres, nf, ncomp, ncol, comp_type[3];   // comp_type: 0 scalar Q, 1 V (from S,T), 2 W (from S,T)
+	const double2 *Q, *S, *T;            // spectral inputs (may be null: zeros)
+	double2 *Qo, *So, *To;               // spectral outputs (analysis)
+	long spec_dist;
+	const double *xs, *xa, *stdt_lo, *stdt_hi, *van_lo, *van_hi, *l2;
+	MTables mt;
+	double *qq;
+};
+
+struct FftParams {
+	int N, S, nlat, mlim, nradix;
+	unsigned long long rcode;            // radices of nphi, 4 bits each, first pass in the low bits
+	const double2 *tw;
+	double2 *F;
+	long fstride;                        // complex elements between field-components in F
+	double *spat[3];                     // per component base pointer
+	const double *spat_in[3];
+	int nf;                              // fields per component
+	long spat_dist;
+	int phi_contiguous;
+};
+
+// ---- launchers (sht_legendre.cu / sht_fft.cu) ----
+void launch_checkpoints(shtns_cfg s, cudaStream_t st);
+void launch_prep_synth(const PrepParams& p, cudaStream_t st);
+void launch_post_analys_m(const PrepParams& p, int mmax, cudaStream_t st);
+void launch_leg_synth(const LegParams& p, cudaStream_t st);
+void launch_leg_analys(const LegParams& p, int kmax_all, cudaStream_t st);
+int fft_threads(int N, int S, unsigned long long rcode, int nradix);
+void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st);
+void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st);
+
+// ---- error reporting (sht_plan.cu) ----
+void shtb_set_error(int code, const std::string& msg);
+void shtb_count_launch(int n = 1);
+bool shtb_cuda_ok(cudaError_t e, const char* where);

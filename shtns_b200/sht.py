@@ -1,0 +1,304 @@
+"""Python surface of shtns_b200, mirroring the reference's `shtns.sht` class
+(shtns_numpy.i:150-460): same constructor, set_grid, idx, spec_array,
+spat_array, synth and analys semantics.
+
+Arrays may be NumPy arrays (transformed through the host-pointer C API with
+copies to and from the GPU) or torch CUDA tensors (transformed in place on the
+device through the cu_* C API, on torch's current stream).  Leading dimensions
+are batch dimensions: a spectral array of shape (..., nlm) or a spatial array
+of shape (..., *spat_shape) transforms every field in one call.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .capi import (sht_orthonormal, sht_fourpi, sht_schmidt, SHT_NO_CS_PHASE, SHT_REAL_NORM,  # noqa: F401
+                   sht_gauss, sht_auto, sht_quick_init, sht_gauss_fly, sht_reg_fast, sht_reg_dct, sht_reg_poles,
+                   SHT_NATIVE_LAYOUT, SHT_THETA_CONTIGUOUS, SHT_PHI_CONTIGUOUS, SHT_SOUTH_POLE_FIRST,
+                   SHT_SCALAR_ONLY, SHT_LOAD_SAVE_CFG, SHT_ALLOW_GPU, SHT_ALLOW_PADDING, SHTError)
+
+try:
+    import torch
+except ImportError:  # torch is optional for the NumPy path
+    torch = None
+
+
+def _is_torch(x):
+    return torch is not None and isinstance(x, torch.Tensor)
+
+
+class sht:
+    """Spherical harmonic transform plan on the GPU.
+
+    sht(lmax, mmax=-1, mres=1, norm=sht_orthonormal, nthreads=0) as in the
+    reference (shtns_numpy.i:173-190); nthreads is accepted and ignored."""
+
+    def __init__(self, lmax, mmax=-1, mres=1, norm=sht_orthonormal, nthreads=0):
+        self._lib = capi.load()
+        if lmax < 2:
+            raise ValueError("lmax < 2 not allowed")
+        if mres <= 0:
+            raise ValueError("mres <= 0 invalid")
+        if mmax < 0:
+            mmax = lmax // mres
+        if mmax * mres > lmax:
+            raise ValueError("lmax < mmax*mres invalid")
+        self._cfg = self._lib.shtns_create(int(lmax), int(mmax), int(mres), int(norm))
+        if not self._cfg:
+            raise SHTError(self._lib.shtns_b200_last_error().decode())
+        s = self._cfg.contents
+        self.lmax, self.mmax, self.mres, self.nlm = s.lmax, s.mmax, s.mres, s.nlm
+        self.norm = norm
+        self.nlat = 0
+        self.nphi = 0
+        self.l = np.zeros(self.nlm, dtype=np.int32)
+        self.m = np.zeros(self.nlm, dtype=np.int32)
+        for mm in range(0, self.mmax * self.mres + 1, self.mres):
+            for ll in range(mm, self.lmax + 1):
+                ii = self.idx(ll, mm)
+                self.l[ii] = ll
+                self.m[ii] = mm
+        self.l.flags.writeable = False
+        self.m.flags.writeable = False
+
+    # ---------------- set-up ----------------
+    def set_grid(self, nlat=0, nphi=0, flags=sht_quick_init, polar_opt=1.0e-10, nl_order=1):
+        """Gauss grid set-up (shtns_numpy.i:204-222): default layout is
+        phi-contiguous unless SHT_THETA_CONTIGUOUS is given."""
+        if nlat != 0 and nlat <= self.lmax:
+            raise ValueError("nlat <= lmax")
+        if nphi != 0 and nphi <= self.mmax * 2:
+            raise ValueError("nphi <= 2*mmax")
+        if not (flags & SHT_THETA_CONTIGUOUS):
+            flags |= SHT_PHI_CONTIGUOUS
+        grd = flags & 255
+        if grd in (sht_auto, sht_gauss_fly, sht_gauss):
+            grd = sht_quick_init
+        flags = (flags & ~255) | grd
+        nl = C.c_int(int(nlat))
+        np_ = C.c_int(int(nphi))
+        r = self._lib.shtns_set_grid_auto(self._cfg, int(flags), float(polar_opt), int(nl_order),
+                                          C.byref(nl), C.byref(np_))
+        if r < 0:
+            raise SHTError(self._lib.shtns_b200_last_error().decode())
+        s = self._cfg.contents
+        self.nlat, self.nphi, self.nspat = s.nlat, s.nphi, s.nspat
+        self.flags = flags
+        self.layout = flags & ~255
+        self.cos_theta = np.ctypeslib.as_array(s.ct, shape=(self.nlat,)).copy()
+        self.cos_theta.flags.writeable = False
+        if self.layout & SHT_PHI_CONTIGUOUS:
+            self.spat_shape = (self.nlat, self.nphi)
+        else:
+            self.spat_shape = (self.nphi, self.nlat)
+        return self.nlat, self.nphi
+
+    def robert_form(self, v=1):
+        self._lib.shtns_robert_form(self._cfg, int(v))
+
+    def print_info(self):
+        self._lib.shtns_print_cfg(self._cfg)
+
+    def sh00_1(self):
+        return self._lib.sh00_1(self._cfg)
+
+    def sh10_ct(self):
+        return self._lib.sh10_ct(self._cfg)
+
+    def sh11_st(self):
+        return self._lib.sh11_st(self._cfg)
+
+    def shlm_e1(self, l, m):
+        return self._lib.shlm_e1(self._cfg, int(l), int(m))
+
+    def gauss_wts(self):
+        w = np.zeros(self.nlat // 2)
+        n = self._lib.shtns_gauss_wts(self._cfg, w.ctypes.data_as(C.c_void_p))
+        return w[:n]
+
+    def idx(self, l, m):
+        if l > self.lmax:
+            raise ValueError("l invalid")
+        if m > l or m > self.mmax * self.mres or m % self.mres != 0:
+            raise ValueError("m invalid")
+        im = m // self.mres
+        return (im * (2 * self.lmax + 2 - (im + 1) * self.mres)) // 2 + l
+
+    def spec_array(self, im=-1):
+        if im < 0:
+            return np.zeros(self.nlm, dtype=complex)
+        return np.zeros(self.lmax + 1 - im * self.mres, dtype=complex)
+
+    def spat_array(self):
+        if self.nlat == 0:
+            raise RuntimeError("Grid not set. Call .set_grid() method.")
+        return np.zeros(self.spat_shape)
+
+    def clone(self, stream=0):
+        """cushtns_clone: a plan sharing this plan's tables, for another stream."""
+        c = object.__new__(sht)
+        c.__dict__.update(self.__dict__)
+        c._cfg = self._lib.cushtns_clone(self._cfg, C.c_void_p(stream), None)
+        if not c._cfg:
+            raise SHTError(self._lib.shtns_b200_last_error().decode())
+        c._clone_of = self
+        return c
+
+    def device_bytes(self):
+        return self._lib.shtns_b200_device_bytes(self._cfg)
+
+    def __del__(self):
+        try:
+            if getattr(self, "_cfg", None):
+                self._lib.shtns_destroy(self._cfg)
+                self._cfg = None
+        except Exception:
+            pass
+
+    # ---------------- helpers ----------------
+    def _need_grid(self):
+        if self.nlat == 0:
+            raise RuntimeError("Grid not set. Call .set_grid() method.")
+
+    def _batch(self, nf):
+        if self._lib.shtns_set_batch(self._cfg, int(nf), int(self.nlm), int(self.nspat)) != 0:
+            capi.check(self._lib)
+
+    def _stream(self):
+        s = torch.cuda.current_stream().cuda_stream
+        self._lib.cushtns_set_streams(self._cfg, C.c_void_p(s), None)
+
+    # ---------------- transforms ----------------
+    def synth(self, *arg, ltr=None):
+        """v = synth(qlm); vt, vp = synth(slm, tlm); vr, vt, vp = synth(qlm, slm, tlm)
+        (shtns_numpy.i:396-425).  With ltr, the truncated _l transform."""
+        self._need_grid()
+        n = len(arg)
+        if n < 1 or n > 3:
+            raise RuntimeError("1,2 or 3 arguments required.")
+        ltr = self.lmax if ltr is None else int(ltr)
+        if _is_torch(arg[0]):
+            return self._synth_torch(arg, ltr)
+        q = []
+        for a in arg:
+            a = np.asarray(a)
+            if a.shape[-1] != self.nlm:
+                raise RuntimeError("spectral array has wrong size.")
+            if a.dtype != np.complex128:
+                raise RuntimeError("spectral array should be dtype=complex.")
+            q.append(np.ascontiguousarray(a))
+        lead = q[0].shape[:-1]
+        nf = int(np.prod(lead)) if lead else 1
+        outs = [np.empty(lead + self.spat_shape) for _ in range(n)]
+        self._batch(nf)
+        P = [x.ctypes.data_as(C.c_void_p) for x in q]
+        O = [x.ctypes.data_as(C.c_void_p) for x in outs]
+        L = self._lib
+        if n == 1:
+            L.SH_to_spat_l(self._cfg, P[0], O[0], ltr)
+        elif n == 2:
+            L.SHsphtor_to_spat_l(self._cfg, P[0], P[1], O[0], O[1], ltr)
+        else:
+            L.SHqst_to_spat_l(self._cfg, P[0], P[1], P[2], O[0], O[1], O[2], ltr)
+        capi.check(L)
+        return outs[0] if n == 1 else tuple(outs)
+
+    def analys(self, *arg, ltr=None):
+        """qlm = analys(v); slm, tlm = analys(vt, vp); qlm, slm, tlm = analys(vr, vt, vp)
+        (shtns_numpy.i:427-456).  Inputs are left unchanged."""
+        self._need_grid()
+        n = len(arg)
+        if n < 1 or n > 3:
+            raise RuntimeError("1,2 or 3 arguments required.")
+        ltr = self.lmax if ltr is None else int(ltr)
+        if _is_torch(arg[0]):
+            return self._analys_torch(arg, ltr)
+        v = []
+        for a in arg:
+            a = np.asarray(a)
+            if a.shape[-2:] != self.spat_shape:
+                raise RuntimeError("spatial array has wrong shape.")
+            if a.dtype != np.float64:
+                raise RuntimeError("spatial array should be dtype=float64.")
+            v.append(np.ascontiguousarray(a))
+        lead = v[0].shape[:-2]
+        nf = int(np.prod(lead)) if lead else 1
+        outs = [np.empty(lead + (self.nlm,), dtype=np.complex128) for _ in range(n)]
+        self._batch(nf)
+        P = [x.ctypes.data_as(C.c_void_p) for x in v]
+        O = [x.ctypes.data_as(C.c_void_p) for x in outs]
+        L = self._lib
+        if n == 1:
+            L.spat_to_SH_l(self._cfg, P[0], O[0], ltr)
+        elif n == 2:
+            L.spat_to_SHsphtor_l(self._cfg, P[0], P[1], O[0], O[1], ltr)
+        else:
+            L.spat_to_SHqst_l(self._cfg, P[0], P[1], P[2], O[0], O[1], O[2], ltr)
+        capi.check(L)
+        return outs[0] if n == 1 else tuple(outs)
+
+    def synth_grad(self, slm):
+        """(vtheta, vphi) = gradient of slm (SHsph_to_spat)."""
+        self._need_grid()
+        z = np.zeros_like(slm)
+        return self.synth(slm, z)
+
+    # ---------------- torch (device) path ----------------
+    def _synth_torch(self, arg, ltr):
+        q = []
+        for a in arg:
+            if not a.is_cuda or a.dtype != torch.complex128 or a.shape[-1] != self.nlm:
+                raise RuntimeError("spectral tensors must be CUDA complex128 with last dimension nlm")
+            q.append(a.contiguous())
+        lead = tuple(q[0].shape[:-1])
+        nf = int(np.prod(lead)) if lead else 1
+        outs = [torch.empty(lead + self.spat_shape, dtype=torch.float64, device=q[0].device) for _ in q]
+        self.synth_into(q, outs, ltr)
+        return outs[0] if len(outs) == 1 else tuple(outs)
+
+    def _analys_torch(self, arg, ltr):
+        v = []
+        for a in arg:
+            if not a.is_cuda or a.dtype != torch.float64 or tuple(a.shape[-2:]) != self.spat_shape:
+                raise RuntimeError("spatial tensors must be CUDA float64 with trailing shape spat_shape")
+            v.append(a.contiguous())
+        lead = tuple(v[0].shape[:-2])
+        outs = [torch.empty(lead + (self.nlm,), dtype=torch.complex128, device=v[0].device) for _ in v]
+        self.analys_into(v, outs, ltr)
+        return outs[0] if len(outs) == 1 else tuple(outs)
+
+    def synth_into(self, q, outs, ltr=None):
+        """Device synthesis into preallocated tensors (no allocation by torch):
+        q: list of 1-3 complex128 CUDA tensors (..., nlm); outs: float64 (..., *spat_shape)."""
+        ltr = self.lmax if ltr is None else int(ltr)
+        nf = q[0].numel() // self.nlm
+        self._batch(nf)
+        self._stream()
+        P = [C.c_void_p(x.data_ptr()) for x in q]
+        O = [C.c_void_p(x.data_ptr()) for x in outs]
+        L = self._lib
+        if len(q) == 1:
+            L.cu_SH_to_spat(self._cfg, P[0], O[0], ltr)
+        elif len(q) == 2:
+            L.cu_SHsphtor_to_spat(self._cfg, P[0], P[1], O[0], O[1], ltr)
+        else:
+            L.cu_SHqst_to_spat(self._cfg, P[0], P[1], P[2], O[0], O[1], O[2], ltr)
+        capi.check(L)
+
+    def analys_into(self, v, outs, ltr=None):
+        """Device analysis into preallocated tensors (see synth_into)."""
+        ltr = self.lmax if ltr is None else int(ltr)
+        nf = v[0].numel() // self.nspat
+        self._batch(nf)
+        self._stream()
+        P = [C.c_void_p(x.data_ptr()) for x in v]
+        O = [C.c_void_p(x.data_ptr()) for x in outs]
+        L = self._lib
+        if len(v) == 1:
+            L.cu_spat_to_SH(self._cfg, P[0], O[0], ltr)
+        elif len(v) == 2:
+            L.cu_spat_to_SHsphtor(self._cfg, P[0], P[1], O[0], O[1], ltr)
+        else:
+            L.cu_spat_to_SHqst(self._cfg, P[0], P[1], P[2], O[0], O[1], O[2], ltr)
+        capi.check(L)

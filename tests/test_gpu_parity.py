@@ -1,0 +1,223 @@
+"""Parity of the CUDA transforms with the reference SHTns 3.5.2 CPU transforms.
+
+Bar (north star): max relative error <= 1e-12 in FP64 (normwise:
+max|gpu - ref| / max|ref|), with the reference's kernel choice pinned
+(sht_quick_init) and polar threshold 0 unless a test says otherwise.  Inputs
+follow the benchmark recipes (tests/common.py).  The references are the
+committed golden fixtures (generated from the reference library) and, where
+built, the reference library itself in oracle/_ref.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tests.common import rand_spec, relerr
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 1e-12
+
+
+def _ref():
+    from oracle import shtns_ref as R
+    if not R.available():
+        pytest.skip("reference library not built")
+    return R
+
+
+def _golden():
+    with open(os.path.join(GOLDEN, "index.json")) as f:
+        return json.load(f)
+
+
+def _plan(meta_or_cfg, eps=0.0):
+    import shtns_b200
+    lmax, mmax, mres, nlat, nphi, norm, layout = meta_or_cfg
+    s = shtns_b200.sht(lmax, mmax, mres, norm)
+    flags = shtns_b200.sht_quick_init | layout
+    if not (layout & shtns_b200.SHT_PHI_CONTIGUOUS):
+        flags |= shtns_b200.SHT_THETA_CONTIGUOUS
+    s.set_grid(nlat, nphi, flags=flags, polar_opt=eps)
+    return s
+
+
+def _inputs(meta):
+    q = rand_spec(meta["lmax"], meta["mmax"], meta["mres"], meta["seed"], power=1.0)
+    s = rand_spec(meta["lmax"], meta["mmax"], meta["mres"], meta["seed"] + 1, power=1.5, zero_l0=True)
+    t = rand_spec(meta["lmax"], meta["mmax"], meta["mres"], meta["seed"] + 2, power=1.5, zero_l0=True)
+    return q, s, t
+
+
+def _meta_cfg(meta):
+    return (meta["lmax"], meta["mmax"], meta["mres"], meta["nlat"], meta["nphi"], meta["norm"], meta["layout"])
+
+
+@pytest.mark.parametrize("name", sorted(_golden()))
+def test_golden_host_api(name):
+    """Host-pointer API (SH_to_spat, ... through the Python class)."""
+    meta = _golden()[name]
+    g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    sh = _plan(_meta_cfg(meta))
+    assert np.abs(sh.cos_theta - g["ct"]).max() < 4e-16
+    q, s, t = _inputs(meta)
+    ltr = meta["ltr"]
+    if meta["kind"] == "scalar":
+        assert relerr(g["synth_v"], sh.synth(q, ltr=ltr)) < TOL
+        assert relerr(g["analys_q"], sh.analys(g["synth_v"], ltr=ltr)) < TOL
+    elif meta["kind"] == "sphtor":
+        vt, vp = sh.synth(s, t, ltr=ltr)
+        assert relerr(g["synth_vt"], vt) < TOL and relerr(g["synth_vp"], vp) < TOL
+        S, T = sh.analys(g["synth_vt"], g["synth_vp"], ltr=ltr)
+        assert relerr(g["analys_s"], S) < TOL and relerr(g["analys_t"], T) < TOL
+    else:
+        vr, vt, vp = sh.synth(q, s, t, ltr=ltr)
+        for k, v in (("synth_vr", vr), ("synth_vt", vt), ("synth_vp", vp)):
+            assert relerr(g[k], v) < TOL, k
+        Q, S, T = sh.analys(g["synth_vr"], g["synth_vt"], g["synth_vp"], ltr=ltr)
+        for k, v in (("analys_q", Q), ("analys_s", S), ("analys_t", T)):
+            assert relerr(g[k], v) < TOL, k
+
+
+@pytest.mark.parametrize("name", ["cfg1_scalar", "small_qst", "phi_schmidt_mres2"])
+def test_golden_device_api(name):
+    """Device-pointer API (cu_* on torch CUDA tensors)."""
+    meta = _golden()[name]
+    g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    sh = _plan(_meta_cfg(meta))
+    q, s, t = _inputs(meta)
+    dev = torch.device("cuda:0")
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    ltr = meta["ltr"]
+    if meta["kind"] == "scalar":
+        v = sh.synth(T(q), ltr=ltr)
+        assert relerr(g["synth_v"], v.cpu().numpy()) < TOL
+        qa = sh.analys(T(g["synth_v"]), ltr=ltr)
+        assert relerr(g["analys_q"], qa.cpu().numpy()) < TOL
+    else:
+        vr, vt, vp = sh.synth(T(q), T(s), T(t), ltr=ltr)
+        for k, v in (("synth_vr", vr), ("synth_vt", vt), ("synth_vp", vp)):
+            assert relerr(g[k], v.cpu().numpy()) < TOL, k
+        Q, S, Tt = sh.analys(T(g["synth_vr"]), T(g["synth_vt"]), T(g["synth_vp"]), ltr=ltr)
+        for k, v in (("analys_q", Q), ("analys_s", S), ("analys_t", Tt)):
+            assert relerr(g[k], v.cpu().numpy()) < TOL, k
+
+
+def test_known_answer_on_gpu():
+    """examples/test_suite.c:96-152 through the GPU path (ftol 1e-14)."""
+    from tests.test_oracle import spat_func_test, kat_expected
+    import shtns_b200
+    sh = shtns_b200.sht(7, 3, 1)
+    sh.set_grid(64, 8, flags=shtns_b200.sht_quick_init | shtns_b200.SHT_THETA_CONTIGUOUS, polar_opt=1e-10)
+    theta = np.arccos(sh.cos_theta)
+    phi = 2 * np.pi * np.arange(8) / 8
+    Tg, Pg = np.meshgrid(theta, phi)
+    d = spat_func_test(Tg, Pg)
+    q = sh.analys(d)
+    assert np.abs(q - kat_expected(sh.idx, sh.nlm)).max() < 1e-14
+    assert np.abs(sh.synth(q) - d).max() < 1e-14
+
+
+@pytest.mark.parametrize("kind", ["scalar", "sphtor", "qst"])
+def test_batch_equals_single_fields(kind):
+    cfg = (63, 63, 1, 96, 192, 0, 256)
+    sh = _plan(cfg)
+    nf = 5
+    q = rand_spec(63, 63, 1, 11, nfields=nf)
+    s = rand_spec(63, 63, 1, 12, power=1.5, zero_l0=True, nfields=nf)
+    t = rand_spec(63, 63, 1, 13, power=1.5, zero_l0=True, nfields=nf)
+    args = {"scalar": (q,), "sphtor": (s, t), "qst": (q, s, t)}[kind]
+    out = sh.synth(*args)
+    out = out if isinstance(out, tuple) else (out,)
+    for f in range(nf):
+        one = sh.synth(*(a[f] for a in args))
+        one = one if isinstance(one, tuple) else (one,)
+        for a, b in zip(out, one):
+            assert np.array_equal(a[f], b)
+    back = sh.analys(*out)
+    back = back if isinstance(back, tuple) else (back,)
+    for a, b in zip(args, back):
+        assert relerr(a, b) < TOL
+
+
+@pytest.mark.parametrize("cfg", [
+    (127, 127, 1, 192, 384, 0, 256),
+    (255, 255, 1, 384, 768, 0, 256),
+    (100, 70, 1, 160, 150, 0, 512),            # nphi = 2*3*5*5, phi-contiguous
+    (60, 20, 3, 90, 140, 0, 256),              # mres = 3, nphi with radix 7
+])
+def test_against_reference_library(cfg):
+    R = _ref()
+    lmax, mmax, mres, nlat, nphi, norm, layout = cfg
+    ref = R.RefSHT(lmax, mmax, mres, norm, nlat, nphi, flags=R.sht_quick_init | layout, eps=0.0, nthreads=8)
+    sh = _plan(cfg)
+    q = rand_spec(lmax, mmax, mres, 21)
+    s = rand_spec(lmax, mmax, mres, 22, power=1.5, zero_l0=True)
+    t = rand_spec(lmax, mmax, mres, 23, power=1.5, zero_l0=True)
+    vr, vt, vp = ref.qst_synth(q, s, t)
+    gr, gt, gp = sh.synth(q, s, t)
+    assert relerr(vr, gr) < TOL and relerr(vt, gt) < TOL and relerr(vp, gp) < TOL
+    Q, S, T = ref.qst_analys(vr, vt, vp)
+    gQ, gS, gT = sh.analys(vr, vt, vp)
+    assert relerr(Q, gQ) < TOL and relerr(S, gS) < TOL and relerr(T, gT) < TOL
+    # truncated forms
+    ltr = lmax // 2
+    assert relerr(ref.synth(q, ltr), sh.synth(q, ltr=ltr)) < TOL
+    assert relerr(ref.analys(vr, ltr), sh.analys(vr, ltr=ltr)) < TOL
+    a = ref.sphtor_analys(vt, vp, ltr)
+    b = sh.analys(vt, vp, ltr=ltr)
+    assert relerr(a[0], b[0]) < TOL and relerr(a[1], b[1]) < TOL
+    ref.close()
+
+
+def test_polar_threshold_matches_reference_within_eps():
+    """With the polar threshold on (eps=1e-10, the reference default), both
+    sides drop rows whose Legendre values stay below eps; the reference rounds
+    the start row down to its SIMD width, so they agree to O(eps)."""
+    R = _ref()
+    cfg = (255, 255, 1, 384, 768, 0, 256)
+    ref = R.RefSHT(255, 255, 1, 0, 384, 768, flags=R.sht_quick_init | 256, eps=1e-10, nthreads=8)
+    sh = _plan(cfg, eps=1e-10)
+    q = rand_spec(255, 255, 1, 31)
+    v = ref.synth(q)
+    assert relerr(v, sh.synth(q)) < 1e-9
+    assert relerr(ref.analys(v), sh.analys(v)) < 1e-9
+    ref.close()
+
+
+def test_lmax511_vector_batch_against_reference():
+    """Configuration-2 sizes (lmax=511, 768 x 1536) on a small batch."""
+    R = _ref()
+    ref = R.RefSHT(511, 511, 1, 0, 768, 1536, flags=R.sht_quick_init | 256, eps=0.0, nthreads=16)
+    sh = _plan((511, 511, 1, 768, 1536, 0, 256))
+    nf = 2
+    q = rand_spec(511, 511, 1, 41, nfields=nf)
+    s = rand_spec(511, 511, 1, 42, power=1.5, zero_l0=True, nfields=nf)
+    t = rand_spec(511, 511, 1, 43, power=1.5, zero_l0=True, nfields=nf)
+    gr, gt, gp = sh.synth(q, s, t)
+    gQ, gS, gT = sh.analys(gr, gt, gp)
+    for f in range(nf):
+        vr, vt, vp = ref.qst_synth(q[f], s[f], t[f])
+        assert relerr(vr, gr[f]) < TOL and relerr(vt, gt[f]) < TOL and relerr(vp, gp[f]) < TOL
+        Q, S, T = ref.qst_analys(vr, vt, vp)
+        assert relerr(Q, gQ[f]) < TOL and relerr(S, gS[f]) < TOL and relerr(T, gT[f]) < TOL
+    ref.close()
+
+
+def test_lmax511_64_fields_round_trip():
+    """Full configuration-2 batch: 64 qst fields; analysis(synthesis(x)) = x."""
+    import shtns_b200
+    sh = _plan((511, 511, 1, 768, 1536, 0, 256))
+    dev = torch.device("cuda:0")
+    nf = 64
+    q = torch.from_numpy(rand_spec(511, 511, 1, 51, nfields=nf)).to(dev)
+    s = torch.from_numpy(rand_spec(511, 511, 1, 52, power=1.5, zero_l0=True, nfields=nf)).to(dev)
+    t = torch.from_numpy(rand_spec(511, 511, 1, 53, power=1.5, zero_l0=True, nfields=nf)).to(dev)
+    vr, vt, vp = sh.synth(q, s, t)
+    Q, S, T = sh.analys(vr, vt, vp)
+    for a, b in ((q, Q), (s, S), (t, T)):
+        assert relerr(a.cpu().numpy(), b.cpu().numpy()) < TOL
+    assert shtns_b200.capi.load().shtns_b200_status() == 0
