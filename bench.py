@@ -1,0 +1,401 @@
+"""Benchmark: SH_to_spat + spat_to_SH pairs per second at lmax=511.
+
+Workload (the configuration the headline metric is quoted on): lmax=mmax=511,
+mres=1, orthonormal + Condon-Shortley, Gauss grid nlat=768 x nphi=1536,
+theta-contiguous, a batch of 64 independent fields (a stack of radial
+shells), 3-D vector transforms: one step = SHqst_to_spat then spat_to_SHqst
+of all 64 fields.  Coefficients are seeded N(0,1)(l+1)^-p (p = 1 radial,
+1.5 spheroidal/toroidal, l=0 zeroed), polar threshold 1e-10 (the SHTns
+default) on both arms.  The unit is field-pairs per second (one field-pair =
+one 3-component synthesis + analysis of one field).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU (torchrun): fields are independent, every rank transforms its own 64
+fields with no collective on the data path (weak scaling); time = max over
+ranks of the device-timed region.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LMAX, NLAT, NPHI, NFIELDS, EPS = 511, 768, 1536, 64, 1e-10
+METRIC = "SH_to_spat+spat_to_SH pairs/s vs lmax; FP64 plain vs batched/split-prec at 1e-11"
+UNIT = "field-pairs/s (SHqst_to_spat+spat_to_SHqst, lmax=511, 768x1536)"
+WORKLOAD = "lmax511_qst_64fields"
+
+
+def spectral_inputs(nf, seed):
+    from tests.common import rand_spec
+    q = rand_spec(LMAX, LMAX, 1, seed, power=1.0, nfields=nf)
+    s = rand_spec(LMAX, LMAX, 1, seed + 1, power=1.5, zero_l0=True, nfields=nf)
+    t = rand_spec(LMAX, LMAX, 1, seed + 2, power=1.5, zero_l0=True, nfields=nf)
+    return q, s, t
+
+
+def legendre_flops(tm, nfields, kind="qst"):
+    """Multiply-adds of the even/odd-folded Legendre contraction, x2 flops.
+    Per order m, latitude row kept by the polar threshold, field-component and
+    Ishioka step k: 4 real FMAs (even/odd x re/im).  Scalar components run
+    k < (lmax-m)/2+1, vector components (V, W) k < (lmax+1-m)/2+1."""
+    n2 = NLAT // 2
+    tot = 0
+    for m in range(LMAX + 1):
+        rows = n2 - tm[m]
+        ks = (LMAX - m) // 2 + 1
+        kv = (LMAX + 1 - m) // 2 + 1
+        tot += rows * (ks + 2 * kv)          # Q + V + W components
+    return 8.0 * tot * nfields
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock, power and throttle reasons while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev_index):
+        self.dev = dev_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.dev)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU side
+class quiet_stdout:
+    """Route the C library's stdout to /dev/null (the reference's plan set-up
+    prints Newton-iteration diagnostics) so that bench.py prints one JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+
+    def __exit__(self, *exc):
+        try:
+            import ctypes
+            ctypes.CDLL(None).fflush(None)
+        except OSError:
+            pass
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
+def reference_cpu_rate(target_s=10.0, fields_per_step=None, steps=None, warmup=1, nthreads=None):
+    """Field-pairs/s of the reference SHTns CPU library (oracle/_ref: the
+    reference's own sources, OpenMP on all host threads, autotuned sht_gauss
+    plan) on the same lmax=511 qst workload, one field at a time.  Either runs
+    for about target_s seconds or for `steps` steps of `fields_per_step` fields."""
+    from oracle import shtns_ref as R
+    nthreads = nthreads or os.cpu_count()
+    L = R.lib()
+    with quiet_stdout():
+        ref = R.RefSHT(LMAX, LMAX, 1, R.sht_orthonormal, NLAT, NPHI, flags=R.sht_gauss | R.SHT_THETA_CONTIGUOUS,
+                       eps=EPS, nthreads=nthreads)
+    q, s, t = spectral_inputs(2, 100)
+    sp = [np.zeros((NPHI, NLAT)) for _ in range(3)]
+    sq = [np.zeros(ref.nlm, dtype=np.complex128) for _ in range(3)]
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+
+    def pair(f):
+        L.SHqst_to_spat(ref.cfg, P(q[f]), P(s[f]), P(t[f]), P(sp[0]), P(sp[1]), P(sp[2]))
+        L.spat_to_SHqst(ref.cfg, P(sp[0]), P(sp[1]), P(sp[2]), P(sq[0]), P(sq[1]), P(sq[2]))
+
+    for i in range(max(1, warmup)):
+        pair(i % 2)
+    n = 0
+    t0 = time.perf_counter()
+    if steps is None:
+        while time.perf_counter() - t0 < target_s or n < 3:
+            pair(n % 2)
+            n += 1
+    else:
+        for _ in range(steps):
+            for _ in range(fields_per_step):
+                pair(n % 2)
+                n += 1
+    dt = time.perf_counter() - t0
+    ref.close()
+    return n / dt, n, dt, nthreads
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation of the path on the
+    host cores (rank 0 only under torchrun)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    fps = 2
+    rate, n, dt, nth = reference_cpu_rate(steps=args.steps, fields_per_step=fps, warmup=args.warmup)
+    sample = f"{args.steps} steps x {fps} field-pairs of the lmax=511 qst workload ({n} pairs, {dt:.1f} s)"
+    line = {
+        "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "lmax": LMAX, "nlat": NLAT, "nphi": NPHI, "fields_per_step": fps,
+                   "polar_eps": EPS, "layout": "theta-contiguous"},
+        "impl": "reference",
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": nth, "kind": "reference", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def fp64_gemm_peak(torch, dev):
+    """Measured FP64 tensor-core throughput of this GPU: cuBLAS DGEMM 8192^3,
+    best of 3 (the FP64 counterpart of the bf16 GEMM figure of
+    MEASURED_PEAKS.json, which holds no FP64 number)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    import shtns_b200
+    from shtns_b200 import capi
+    lib = capi.load()
+    nf = args.fields
+    sh = shtns_b200.sht(LMAX, LMAX, 1)
+    sh.set_grid(NLAT, NPHI, flags=shtns_b200.sht_quick_init | shtns_b200.SHT_THETA_CONTIGUOUS, polar_opt=EPS)
+    qn, sn, tn = spectral_inputs(nf, 100 + 7 * rank)
+    spec = [torch.from_numpy(a).to(dev) for a in (qn, sn, tn)]
+    spat = [torch.empty((nf, NPHI, NLAT), dtype=torch.float64, device=dev) for _ in range(3)]
+    back = [torch.empty((nf, sh.nlm), dtype=torch.complex128, device=dev) for _ in range(3)]
+
+    def step():
+        sh.synth_into(spec, spat)
+        sh.analys_into(spat, back)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    lib.shtns_b200_set_timing(sh._cfg, 1)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    n0 = lib.shtns_b200_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    e1.synchronize()
+    launches = lib.shtns_b200_launch_count() - n0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms_total = e0.elapsed_time(e1)
+    ms_stage = np.zeros(6)
+    calls = np.zeros(6, dtype=np.int64)
+    lib.shtns_b200_stage_times(sh._cfg, ms_stage.ctypes.data_as(C.c_void_p), calls.ctypes.data_as(C.c_void_p))
+    lib.shtns_b200_set_timing(sh._cfg, 0)
+    if world > 1:
+        t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    # correctness of what was timed
+    rt_err = max(float((a - b).abs().max() / a.abs().max()) for a, b in zip(spec, back))
+
+    # end to end through the public API: pinned host spectra in, spectra out
+    host_in = [torch.from_numpy(a).pin_memory() for a in (qn, sn, tn)]
+    host_out = [torch.empty((nf, sh.nlm), dtype=torch.complex128).pin_memory() for _ in range(3)]
+    e2e_steps = max(3, min(args.steps, 20))
+
+    def e2e_step():
+        for d, h in zip(spec, host_in):
+            d.copy_(h, non_blocking=True)
+        sh.synth_into(spec, spat)
+        sh.analys_into(spat, back)
+        for h, d in zip(host_out, back):
+            h.copy_(d, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(e2e_steps):
+        e2e_step()
+    f1.record()
+    f1.synchronize()
+    ms_e2e = f0.elapsed_time(f1) / e2e_steps
+    if world > 1:
+        t = torch.tensor([ms_e2e], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    bytes_io = 3 * nf * sh.nlm * 16
+
+    if rank == 0:
+        ms_step = ms_total / args.steps
+        value = world * nf / (ms_step * 1e-3)
+        tm = np.zeros(LMAX + 1, dtype=np.int32)
+        lib.shtns_b200_polar_rows(sh._cfg, tm.ctypes.data_as(C.c_void_p))
+        flops = legendre_flops(tm, nf)
+        peak_fp64 = fp64_gemm_peak(torch, dev)
+        per_launch = ms_stage / np.maximum(calls, 1)
+        share = ms_stage / max(ms_stage.sum(), 1e-30)
+        names = ["prologue", "legendre_synthesis", "fft_synthesis", "fft_analysis", "legendre_analysis", "epilogue"]
+        dom = int(np.argmax(ms_stage))
+        peaks = measured_peaks()
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        fft_bytes = 3 * nf * (NLAT * (LMAX + 1) * 16 + NLAT * NPHI * 8)
+        stages = {}
+        for i, nm in enumerate(names):
+            d = {"ms_per_launch": per_launch[i], "share": share[i]}
+            if i in (1, 4):
+                d["tflops"] = flops / (per_launch[i] * 1e-3) / 1e12
+                d["frac_of_fp64_peak"] = d["tflops"] / peak_fp64
+            if i in (2, 3):
+                d["gbs"] = fft_bytes / (per_launch[i] * 1e-3) / 1e9
+                d["frac_of_hbm"] = d["gbs"] / hbm
+            stages[nm] = d
+        if dom in (1, 4):
+            ach = flops / (per_launch[dom] * 1e-3) / 1e12
+            roof = {"kernel": names[dom], "bound": "tensor", "achieved": ach, "peak": peak_fp64,
+                    "unit": "TFLOP/s", "frac": ach / peak_fp64, "traffic": None,
+                    "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 on the FP64 tensor cores",
+                    "work_per_launch": f"{flops:.4e} flop (8 per theta-row x field-component x Ishioka step)"}
+        else:
+            ach = fft_bytes / (per_launch[dom] * 1e-3) / 1e9
+            roof = {"kernel": names[dom], "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                    "frac": ach / hbm, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1)(l+1)^-p coefficients)",
+            "config": {"workload": WORKLOAD, "lmax": LMAX, "nlat": NLAT, "nphi": NPHI, "fields_per_gpu": nf,
+                       "transform": "SHqst_to_spat + spat_to_SHqst", "polar_eps": EPS,
+                       "layout": "theta-contiguous", "parallelism": f"fields sharded over {world} GPU(s)",
+                       "l2": "no flush: per-step working set %.1f GB > 126 MB L2" %
+                             ((3 * nf * sh.nlm * 16 * 2 + 3 * nf * NLAT * NPHI * 8) / 1e9)},
+            "roofline": roof,
+            "stages": stages,
+            "roundtrip_relerr": rt_err,
+            "gpu_launches": int(launches),
+            "e2e": {"value": world * nf / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
+                    "d2h_bytes_per_step": bytes_io},
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu:
+            try:
+                rate, n, dt, nth = reference_cpu_rate(target_s=args.cpu_seconds)
+                line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": nth, "kind": "reference",
+                                        "sample": f"{n} field-pairs of the same workload, one field at a time, "
+                                                  f"{dt:.1f} s, reference SHTns 3.5.2 sources (OpenMP, autotuned)"}
+            except Exception as e:     # reference library not built on this machine
+                line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(),
+                                        "kind": "reference", "sample": f"unavailable: {e}"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="shtns_b200", choices=["shtns_b200", "reference"])
+    ap.add_argument("--fields", type=int, default=NFIELDS)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -42,6 +42,21 @@ size_t shtns_b200_device_bytes(shtns_cfg);
  * plans).  Used to count the launches inside a timed region. */
 long shtns_b200_launch_count(void);
 
+/* Per-stage GPU timing.  With shtns_b200_set_timing(cfg, 1) every transform
+ * records CUDA events around its kernels on the plan's compute stream (one
+ * event pair per stage, no host synchronisation).  shtns_b200_stage_times()
+ * waits for the recorded events, writes the accumulated milliseconds and call
+ * counts of the 6 stages (0 coefficient prologue, 1 Legendre synthesis,
+ * 2 FFT synthesis, 3 FFT analysis, 4 Legendre analysis, 5 coefficient
+ * epilogue) into ms[6] and calls[6] (either may be NULL), and resets them. */
+void shtns_b200_set_timing(shtns_cfg, int on);
+int shtns_b200_stage_times(shtns_cfg, double* ms, long* calls);
+
+/* First north-hemisphere latitude row kept by the polar threshold for each
+ * order im = 0..mmax (rows closer to the pole are treated as zero, as the
+ * reference's PolarOptimize does).  Writes mmax+1 ints; returns mmax+1. */
+int shtns_b200_polar_rows(shtns_cfg, int* tm);
+
 #ifdef __cplusplus
 }
 #endif

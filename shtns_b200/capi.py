@@ -105,6 +105,9 @@ PROTOTYPES = {
     "shtns_b200_device": (I, [CFG]),
     "shtns_b200_device_bytes": (C.c_size_t, [CFG]),
     "shtns_b200_launch_count": (C.c_long, []),
+    "shtns_b200_set_timing": (None, [CFG, I]),
+    "shtns_b200_stage_times": (I, [CFG, P, P]),
+    "shtns_b200_polar_rows": (I, [CFG, P]),
 }
 
 _lib = None

@@ -129,12 +129,18 @@ void run_synth(shtns_cfg s, int ncomp, const int* types, const cplx* Q, const cp
 	pp.Q = reinterpret_cast<const double2*>(Q);
 	pp.S = reinterpret_cast<const double2*>(S);
 	pp.T = reinterpret_cast<const double2*>(T);
+	shtb_stage_begin(s, 0);
 	launch_prep_synth(pp, s->comp_stream);
+	shtb_stage_end(s);
 	LegParams lp = leg_params(s, j);
+	shtb_stage_begin(s, 1);
 	launch_leg_synth(lp, s->comp_stream);
+	shtb_stage_end(s);
 	FftParams fp = fft_params(s, j);
 	fp.spat[0] = o0; fp.spat[1] = o1; fp.spat[2] = o2;
+	shtb_stage_begin(s, 2);
 	launch_fft_synth(fp, j.nfc, s->comp_stream);
+	shtb_stage_end(s);
 	check_launch("synthesis launch");
 }
 
@@ -145,16 +151,22 @@ void run_analys(shtns_cfg s, int ncomp, const int* types, const double* i0, cons
 	if (!setup_job(s, j, ncomp, types, ltr)) return;
 	FftParams fp = fft_params(s, j);
 	fp.spat_in[0] = i0; fp.spat_in[1] = i1; fp.spat_in[2] = i2;
+	shtb_stage_begin(s, 3);
 	launch_fft_analys(fp, j.nfc, s->comp_stream);
+	shtb_stage_end(s);
 	LegParams lp = leg_params(s, j);
 	int kmax_all = 0;
 	for (int im = 0; im <= j.mlim; im++) kmax_all = std::max(kmax_all, (j.llim + j.vec_extra - im * s->mres) / 2 + 1);
+	shtb_stage_begin(s, 4);
 	launch_leg_analys(lp, kmax_all, s->comp_stream);
+	shtb_stage_end(s);
 	PrepParams pp = prep_params(s, j);
 	pp.Qo = reinterpret_cast<double2*>(Qo);
 	pp.So = reinterpret_cast<double2*>(So);
 	pp.To = reinterpret_cast<double2*>(To);
+	shtb_stage_begin(s, 5);
 	launch_post_analys_m(pp, s->mmax, s->comp_stream);
+	shtb_stage_end(s);
 	check_launch("analysis launch");
 }
 

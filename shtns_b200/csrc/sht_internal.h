@@ -19,6 +19,9 @@
 #define LG_SEG 32     // recurrence checkpoint spacing in k (== LG_BK)
 #define LG_THREADS 256
 
+// pipeline stages (for shtns_b200_stage_times)
+#define SHTB_NSTAGES 6   // 0 prologue, 1 Legendre synthesis, 2 FFT synthesis, 3 FFT analysis, 4 Legendre analysis, 5 epilogue
+
 #define FFT_MAX_FACTORS 16
 #define FFT_NB 2      // butterflies held in registers per thread and pass
 
@@ -93,6 +96,13 @@ struct shtns_info {
 	int is_clone;
 	shtns_cfg base;                      // plan whose tables a clone shares (NULL for originals)
 	int nclones;
+	// optional per-stage timing with CUDA events on the compute stream
+	int timing;
+	std::vector<cudaEvent_t> ev;         // pool: pairs (start, stop)
+	std::vector<int> ev_stage;           // stage of each used pair
+	int ev_used;
+	double stage_ms[SHTB_NSTAGES];
+	long stage_calls[SHTB_NSTAGES];
 };
 
 // ---- kernel parameter blocks ----
@@ -148,3 +158,6 @@ void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st);
 void shtb_set_error(int code, const std::string& msg);
 void shtb_count_launch(int n = 1);
 bool shtb_cuda_ok(cudaError_t e, const char* where);
+void shtb_stage_begin(shtns_cfg s, int stage);
+void shtb_stage_end(shtns_cfg s);
+void shtb_timing_release(shtns_cfg s);

@@ -360,13 +360,17 @@ leg_analys_kernel(LegParams p, int nkb)
 			double* a = &As[sgi * LG_SEG][tt];
 			a[0] = y0;
 			a[AA_LD] = y1;
-			const double* cc = cm + 2 * ks;
-			#pragma unroll 6
-			for (int j = 2; j < LG_SEG; j++) {
-				const double aa = fma(cc[2 * j - 1], x2, cc[2 * j - 2]);
-				const double y2 = fma(aa, y1, y0);
-				a[j * AA_LD] = y2;
-				y0 = y1; y1 = y2;
+			if (ks < nk) {
+				const double* cc = cm + 2 * ks;
+				#pragma unroll 6
+				for (int j = 2; j < LG_SEG; j++) {
+					const double aa = fma(cc[2 * j - 1], x2, cc[2 * j - 2]);
+					const double y2 = fma(aa, y1, y0);
+					a[j * AA_LD] = y2;
+					y0 = y1; y1 = y2;
+				}
+			} else {
+				for (int j = 2; j < LG_SEG; j++) a[j * AA_LD] = 0.0;
 			}
 		}
 		for (int e = tid; e < LG_BK * (LG_BN / 4); e += LG_THREADS) {

@@ -347,6 +347,7 @@ static void free_device(shtns_cfg s)
 }
 
 void fft_set_smem_limits();
+void shtb_timing_release(shtns_cfg s);
 
 // Upload tables and build the checkpoints.  Returns 0 on success.
 static int init_device(shtns_cfg s)
@@ -550,6 +551,7 @@ extern "C" shtns_cfg shtns_init(enum shtns_type flags, int lmax, int mmax, int m
 
 static void destroy_plan(shtns_cfg s)
 {
+	shtb_timing_release(s);
 	if (s->is_clone) {
 		free_device(s);
 		if (s->base) s->base->nclones--;
@@ -647,6 +649,7 @@ extern "C" shtns_cfg cushtns_clone(shtns_cfg b, cudaStream_t compute_stream, cud
 	s->d_qq = nullptr; s->qq_cap = 0; s->d_F = nullptr; s->F_cap = 0;
 	s->d_stage = nullptr; s->stage_cap = 0;
 	s->xfer_stream = nullptr; s->own_xfer = 0;
+	s->ev.clear(); s->ev_stage.clear(); s->ev_used = 0; s->timing = 0;
 	cushtns_set_streams(s, compute_stream, transfer_stream);
 	std::lock_guard<std::mutex> lk(g_plans_mu);
 	g_plans.push_back(s);
@@ -670,4 +673,76 @@ extern "C" void cushtns_set_streams(shtns_cfg s, cudaStream_t compute_stream, cu
 	} else if (!s->xfer_stream) {
 		if (cudaStreamCreateWithFlags(&s->xfer_stream, cudaStreamNonBlocking) == cudaSuccess) s->own_xfer = 1;
 	}
+}
+
+// ---------------------------------------------------------------------------
+// Per-stage timing: a pool of event pairs recorded on the compute stream,
+// read back only when the caller asks (or when the pool is full).
+static void timing_collect(shtns_cfg s)
+{
+	for (int i = 0; i < s->ev_used; i++) {
+		float ms = 0.f;
+		cudaEventSynchronize(s->ev[2 * i + 1]);
+		if (cudaEventElapsedTime(&ms, s->ev[2 * i], s->ev[2 * i + 1]) == cudaSuccess) {
+			s->stage_ms[s->ev_stage[i]] += ms;
+			s->stage_calls[s->ev_stage[i]]++;
+		}
+	}
+	s->ev_used = 0;
+}
+
+void shtb_timing_release(shtns_cfg s)
+{
+	for (cudaEvent_t e : s->ev) cudaEventDestroy(e);
+	s->ev.clear(); s->ev_stage.clear(); s->ev_used = 0;
+}
+
+void shtb_stage_begin(shtns_cfg s, int stage)
+{
+	if (!s->timing) return;
+	const int pool = 256;
+	if (s->ev.empty()) {
+		s->ev.resize(2 * pool);
+		s->ev_stage.assign(pool, 0);
+		for (auto& e : s->ev) cudaEventCreate(&e);
+	}
+	if (s->ev_used >= pool) timing_collect(s);
+	s->ev_stage[s->ev_used] = stage;
+	cudaEventRecord(s->ev[2 * s->ev_used], s->comp_stream);
+}
+
+void shtb_stage_end(shtns_cfg s)
+{
+	if (!s->timing) return;
+	cudaEventRecord(s->ev[2 * s->ev_used + 1], s->comp_stream);
+	s->ev_used++;
+}
+
+extern "C" void shtns_b200_set_timing(shtns_cfg s, int on)
+{
+	if (!s) return;
+	if (!on && s->timing) { timing_collect(s); }
+	s->timing = on ? 1 : 0;
+	if (on) {
+		for (int i = 0; i < SHTB_NSTAGES; i++) { s->stage_ms[i] = 0.0; s->stage_calls[i] = 0; }
+	}
+}
+
+extern "C" int shtns_b200_stage_times(shtns_cfg s, double* ms, long* calls)
+{
+	if (!s) return -1;
+	timing_collect(s);
+	for (int i = 0; i < SHTB_NSTAGES; i++) {
+		if (ms) ms[i] = s->stage_ms[i];
+		if (calls) calls[i] = s->stage_calls[i];
+		s->stage_ms[i] = 0.0; s->stage_calls[i] = 0;
+	}
+	return SHTB_NSTAGES;
+}
+
+extern "C" int shtns_b200_polar_rows(shtns_cfg s, int* tm)
+{
+	if (!s || !s->grid_set) return 0;
+	for (int im = 0; im <= s->mmax; im++) tm[im] = s->tm_h[im];
+	return s->mmax + 1;
 }
