@@ -10,6 +10,8 @@
 #include "sht_internal.h"
 
 #include <cstring>
+#include <cstdint>
+#include <cstdlib>
 #include <algorithm>
 
 namespace {
@@ -102,9 +104,16 @@ FftParams fft_params(shtns_cfg s, const Job& j)
 		rmin = std::min(rmin, s->fft_radix[i]);
 	}
 	(void) rmin;
-	// latitude pairs per CTA: up to 4 (8 latitudes) with two buffers of S*nphi
-	// complex in shared memory (at most 98 KB so two CTAs fit on an SM)
-	int S = std::max(1, std::min(4, 3072 / (int) s->nphi));
+	// latitude pairs per CTA: the largest of 4, 2, 1 whose two shared-memory
+	// buffers fit in about 110 KB (two CTAs per SM); SHTNS_B200_FFT_PAIRS
+	// overrides (tuning knob, clamped to what fits in 227 KB).
+	int S = 4;
+	while (S > 1 && fft_smem_bytes(s->nphi, S) > 112 * 1024) S /= 2;
+	if (const char* e = getenv("SHTNS_B200_FFT_PAIRS")) {
+		int v = atoi(e);
+		if (v >= 1 && v <= 8) S = v;
+		while (S > 1 && fft_smem_bytes(s->nphi, S) > 227 * 1024) S--;
+	}
 	while (S > 1 && 2 * S > (int) s->nlat) S--;
 	p.S = S;
 	p.tw = s->d_tw; p.F = s->d_F;
@@ -112,6 +121,12 @@ FftParams fft_params(shtns_cfg s, const Job& j)
 	p.nf = j.nf; p.spat_dist = s->spat_dist;
 	p.phi_contiguous = s->phi_contiguous;
 	return p;
+}
+
+int aligned16(const void* a, const void* b, const void* c, long dist)
+{
+	auto ok = [](const void* x) { return ((uintptr_t) x & 15) == 0; };
+	return ok(a) && ok(b) && ok(c) && (dist % 2 == 0);
 }
 
 bool check_launch(const char* what)
@@ -138,6 +153,7 @@ void run_synth(shtns_cfg s, int ncomp, const int* types, const cplx* Q, const cp
 	shtb_stage_end(s);
 	FftParams fp = fft_params(s, j);
 	fp.spat[0] = o0; fp.spat[1] = o1; fp.spat[2] = o2;
+	fp.vec2 = aligned16(o0, o1, o2, s->spat_dist);
 	shtb_stage_begin(s, 2);
 	launch_fft_synth(fp, j.nfc, s->comp_stream);
 	shtb_stage_end(s);
@@ -151,6 +167,7 @@ void run_analys(shtns_cfg s, int ncomp, const int* types, const double* i0, cons
 	if (!setup_job(s, j, ncomp, types, ltr)) return;
 	FftParams fp = fft_params(s, j);
 	fp.spat_in[0] = i0; fp.spat_in[1] = i1; fp.spat_in[2] = i2;
+	fp.vec2 = aligned16(i0, i1, i2, s->spat_dist);
 	shtb_stage_begin(s, 3);
 	launch_fft_analys(fp, j.nfc, s->comp_stream);
 	shtb_stage_end(s);

@@ -120,13 +120,20 @@ template <> struct Dft<7> {
 	}
 };
 
+// Shared-memory layout: element i of sequence s lives at s*seq + i + i/8.
+// The pad of one slot per 8 elements spreads the stride-R writes of the first
+// Stockham pass over the banks, and seq = 2 mod 8 (in 16-byte units) spreads
+// the S sequences, so both the passes and the latitude-pair loads/stores are
+// free of bank conflicts.
+__device__ __forceinline__ int sidx(int s, int i, int seq) { return s * seq + i + (i >> 3); }
+
 // One Stockham pass of radix R over S sequences of length N, from X to Y.
-// Butterfly b of a sequence reads X[b + q*N/R] (q < R), applies twiddles
-// w^{q*k*N/(p*R)} with k = b mod p, runs the R-point DFT and writes
-// Y[(b - k)*R + k + q*p].
+// Butterfly b of a sequence reads element b + q*N/R (q < R), applies twiddles
+// w^{q*k*N/(p*R)} with k = b mod p, runs the R-point DFT and writes element
+// (b - k)*R + k + q*p.
 template <int R>
-__device__ __forceinline__ void fft_pass(const double2* __restrict__ X, double2* __restrict__ Y, int N, int S, int p,
-                                         const double2* __restrict__ tw, int sign)
+__device__ __forceinline__ void fft_pass(const double2* __restrict__ X, double2* __restrict__ Y, int N, int S, int seq,
+                                         int p, const double2* __restrict__ tw, int sign)
 {
 	const int nbf = N / R;
 	const int total = S * nbf;
@@ -134,10 +141,9 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ X, double2*
 	for (int g = threadIdx.x; g < total; g += blockDim.x) {
 		const int sq = g / nbf, b = g - sq * nbf;
 		const int k = b % p;
-		const double2* x = X + sq * N;
 		double2 u[R];
 		#pragma unroll
-		for (int q = 0; q < R; q++) u[q] = x[b + q * nbf];
+		for (int q = 0; q < R; q++) u[q] = X[sidx(sq, b + q * nbf, seq)];
 		if (k) {
 			#pragma unroll
 			for (int q = 1; q < R; q++) {
@@ -147,27 +153,27 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ X, double2*
 			}
 		}
 		Dft<R>::run(u, sign);
-		double2* y = Y + sq * N + (b - k) * R + k;
+		const int o = (b - k) * R + k;
 		#pragma unroll
-		for (int q = 0; q < R; q++) y[q * p] = u[q];
+		for (int q = 0; q < R; q++) Y[sidx(sq, o + q * p, seq)] = u[q];
 	}
 	__syncthreads();
 }
 
-// Runs all passes; the result ends in X or Y, returned.
-__device__ __forceinline__ double2* fft_run(double2* X, double2* Y, int N, int S, unsigned long long rcode, int nradix,
-                                            const double2* __restrict__ tw, int sign)
+// Runs all passes; returns the buffer (X or Y) that holds the result.
+__device__ __forceinline__ double2* fft_run(double2* X, double2* Y, int N, int S, int seq, unsigned long long rcode,
+                                            int nradix, const double2* __restrict__ tw, int sign)
 {
 	int pp = 1;
 	for (int r = 0; r < nradix; r++) {
 		const int R = (int)((rcode >> (4 * r)) & 15);
 		switch (R) {
-			case 8: fft_pass<8>(X, Y, N, S, pp, tw, sign); break;
-			case 4: fft_pass<4>(X, Y, N, S, pp, tw, sign); break;
-			case 2: fft_pass<2>(X, Y, N, S, pp, tw, sign); break;
-			case 3: fft_pass<3>(X, Y, N, S, pp, tw, sign); break;
-			case 5: fft_pass<5>(X, Y, N, S, pp, tw, sign); break;
-			default: fft_pass<7>(X, Y, N, S, pp, tw, sign); break;
+			case 8: fft_pass<8>(X, Y, N, S, seq, pp, tw, sign); break;
+			case 4: fft_pass<4>(X, Y, N, S, seq, pp, tw, sign); break;
+			case 2: fft_pass<2>(X, Y, N, S, seq, pp, tw, sign); break;
+			case 3: fft_pass<3>(X, Y, N, S, seq, pp, tw, sign); break;
+			case 5: fft_pass<5>(X, Y, N, S, seq, pp, tw, sign); break;
+			default: fft_pass<7>(X, Y, N, S, seq, pp, tw, sign); break;
 		}
 		pp *= R;
 		double2* t = X; X = Y; Y = t;
@@ -175,119 +181,141 @@ __device__ __forceinline__ double2* fft_run(double2* X, double2* Y, int N, int S
 	return X;
 }
 
-__device__ __forceinline__ double* spat_ptr(double* const* base, int fc, int nf, long dist)
+__device__ __forceinline__ int seq_len(int N)
 {
-	const int c = fc / nf;
-	return base[c] + (long)(fc - c * nf) * dist;
+	const int a = N + (N >> 3);
+	return a + ((2 - a) & 7);
 }
 
+// Synthesis: F[fc][m][theta] (m <= mlim) -> spatial field-component fc.
+// Sequence s of the CTA packs latitudes lat0+2s (real part) and lat0+2s+1
+// (imaginary part): Z_k = A_k + i B_k, Z_{N-k} = conj(A_k) + i conj(B_k).
 __global__ void fft_synth_kernel(FftParams p)
 {
 	extern __shared__ double2 smem[];
+	const int N = p.N, S = p.S, T = blockDim.x, seq = seq_len(N);
 	double2* X = smem;
+	double2* Y = smem + S * seq;
 	const int fc = blockIdx.y;
-	const int lat0 = blockIdx.x * 2 * p.S;
-	const int N = p.N, S = p.S, T = blockDim.x;
-	double2* Y = smem + S * N;
+	const int lat0 = blockIdx.x * 2 * S;
 	const double2* Ff = p.F + (long)fc * p.fstride;
-	for (int e = threadIdx.x; e < S * N; e += T) X[e] = make_double2(0.0, 0.0);
-	__syncthreads();
-	// Z_k = A_k + i B_k,  Z_{N-k} = conj(A_k) + i conj(B_k)
-	for (int e = threadIdx.x; e < (p.mlim + 1) * S; e += T) {
-		const int k = e / S, sq = e - k * S;
-		const int ra = lat0 + 2 * sq;
+	const int ml = p.mlim;
+	// zero the band between +mlim and -mlim
+	const int nz = N - 2 * ml - 1;
+	for (int e = threadIdx.x; e < S * nz; e += T) {
+		const int s = e / nz, i = ml + 1 + (e - s * nz);
+		X[sidx(s, i, seq)] = make_double2(0.0, 0.0);
+	}
+	for (int e = threadIdx.x; e < (ml + 1) * S; e += T) {
+		const int k = e / S, s = e - k * S;
+		const int ra = lat0 + 2 * s;
 		double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
-		if (ra < p.nlat) a = Ff[(long)k * p.nlat + ra];
-		if (ra + 1 < p.nlat) b = Ff[(long)k * p.nlat + ra + 1];
+		if (ra < p.nlat) {
+			a = Ff[(long)k * p.nlat + ra];
+			b = Ff[(long)k * p.nlat + ra + 1];
+		}
 		if (k == 0) { a.y = 0.0; b.y = 0.0; }
-		X[sq * N + k] = make_double2(a.x - b.y, a.y + b.x);
-		if (k > 0) X[sq * N + N - k] = make_double2(a.x + b.y, b.x - a.y);
+		X[sidx(s, k, seq)] = make_double2(a.x - b.y, a.y + b.x);
+		if (k > 0) X[sidx(s, N - k, seq)] = make_double2(a.x + b.y, b.x - a.y);
 	}
 	__syncthreads();
-	X = fft_run(X, Y, N, S, p.rcode, p.nradix, p.tw, +1);
-	double* out = spat_ptr(p.spat, fc, p.nf, p.spat_dist);
-	const int nl = 2 * S;
+	X = fft_run(X, Y, N, S, seq, p.rcode, p.nradix, p.tw, +1);
+	const int c = fc / p.nf;
+	double* out = p.spat[c] + (long)(fc - c * p.nf) * p.spat_dist;
 	if (!p.phi_contiguous) {
-		for (int e = threadIdx.x; e < N * nl; e += T) {
-			const int j = e / nl, l = e - j * nl;
-			const int row = lat0 + l;
+		for (int e = threadIdx.x; e < N * S; e += T) {
+			const int j = e / S, s = e - j * S;
+			const int row = lat0 + 2 * s;
 			if (row < p.nlat) {
-				const double2 z = X[(l >> 1) * N + j];
-				out[(long)j * p.nlat + row] = (l & 1) ? z.y : z.x;
+				const double2 z = X[sidx(s, j, seq)];
+				double* o = out + (long)j * p.nlat + row;
+				if (p.vec2) *reinterpret_cast<double2*>(o) = z;
+				else { o[0] = z.x; o[1] = z.y; }
 			}
 		}
 	} else {
-		for (int e = threadIdx.x; e < N * nl; e += T) {
-			const int l = e / N, j = e - l * N;
-			const int row = lat0 + l;
+		for (int e = threadIdx.x; e < N * S; e += T) {
+			const int s = e / N, j = e - s * N;
+			const int row = lat0 + 2 * s;
 			if (row < p.nlat) {
-				const double2 z = X[(l >> 1) * N + j];
-				out[(long)row * N + j] = (l & 1) ? z.y : z.x;
+				const double2 z = X[sidx(s, j, seq)];
+				out[(long)row * N + j] = z.x;
+				out[(long)(row + 1) * N + j] = z.y;
 			}
 		}
 	}
 }
 
+// Analysis: spatial field-component fc -> F[fc][m][theta] = A_m / N for m <= mlim,
+// with A_k = (Z_k + conj Z_{N-k})/2 and B_k = (Z_k - conj Z_{N-k})/(2i).
 __global__ void fft_analys_kernel(FftParams p)
 {
 	extern __shared__ double2 smem[];
+	const int N = p.N, S = p.S, T = blockDim.x, seq = seq_len(N);
 	double2* X = smem;
+	double2* Y = smem + S * seq;
 	const int fc = blockIdx.y;
-	const int lat0 = blockIdx.x * 2 * p.S;
-	const int N = p.N, S = p.S, T = blockDim.x;
-	double2* Y = smem + S * N;
+	const int lat0 = blockIdx.x * 2 * S;
 	const int c = fc / p.nf;
 	const double* in = p.spat_in[c] + (long)(fc - c * p.nf) * p.spat_dist;
-	const int nl = 2 * S;
-	double* Xd = reinterpret_cast<double*>(X);
 	if (!p.phi_contiguous) {
-		for (int e = threadIdx.x; e < N * nl; e += T) {
-			const int j = e / nl, l = e - j * nl;
-			const int row = lat0 + l;
-			const double v = (row < p.nlat) ? in[(long)j * p.nlat + row] : 0.0;
-			Xd[2 * ((l >> 1) * N + j) + (l & 1)] = v;
+		for (int e = threadIdx.x; e < N * S; e += T) {
+			const int j = e / S, s = e - j * S;
+			const int row = lat0 + 2 * s;
+			double2 v = make_double2(0.0, 0.0);
+			if (row < p.nlat) {
+				const double* i0 = in + (long)j * p.nlat + row;
+				v = p.vec2 ? *reinterpret_cast<const double2*>(i0) : make_double2(i0[0], i0[1]);
+			}
+			X[sidx(s, j, seq)] = v;
 		}
 	} else {
-		for (int e = threadIdx.x; e < N * nl; e += T) {
-			const int l = e / N, j = e - l * N;
-			const int row = lat0 + l;
-			const double v = (row < p.nlat) ? in[(long)row * N + j] : 0.0;
-			Xd[2 * ((l >> 1) * N + j) + (l & 1)] = v;
+		for (int e = threadIdx.x; e < N * S; e += T) {
+			const int s = e / N, j = e - s * N;
+			const int row = lat0 + 2 * s;
+			double2 v = make_double2(0.0, 0.0);
+			if (row < p.nlat) v = make_double2(in[(long)row * N + j], in[(long)(row + 1) * N + j]);
+			X[sidx(s, j, seq)] = v;
 		}
 	}
 	__syncthreads();
-	X = fft_run(X, Y, N, S, p.rcode, p.nradix, p.tw, -1);
+	X = fft_run(X, Y, N, S, seq, p.rcode, p.nradix, p.tw, -1);
 	double2* Ff = p.F + (long)fc * p.fstride;
 	const double sc = 0.5 / N;
 	for (int e = threadIdx.x; e < (p.mlim + 1) * S; e += T) {
-		const int k = e / S, sq = e - k * S;
-		const int ra = lat0 + 2 * sq;
-		const double2 z = X[sq * N + k];
-		const double2 w = X[sq * N + (k ? N - k : 0)];
-		// A = (Z_k + conj Z_{N-k})/2,  B = (Z_k - conj Z_{N-k})/(2i)
-		const double2 a = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
-		const double2 b = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
-		if (ra < p.nlat) Ff[(long)k * p.nlat + ra] = a;
-		if (ra + 1 < p.nlat) Ff[(long)k * p.nlat + ra + 1] = b;
+		const int k = e / S, s = e - k * S;
+		const int ra = lat0 + 2 * s;
+		const double2 z = X[sidx(s, k, seq)];
+		const double2 w = X[sidx(s, k ? N - k : 0, seq)];
+		if (ra < p.nlat) {
+			Ff[(long)k * p.nlat + ra] = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
+			Ff[(long)k * p.nlat + ra + 1] = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
+		}
 	}
 }
 
 } // namespace
 
+static int seq_len_host(int N)
+{
+	const int a = N + (N >> 3);
+	return a + ((2 - a) & 7);
+}
+
 int fft_threads(int N, int S, unsigned long long rcode, int nradix)
 {
 	(void) rcode; (void) nradix;
 	// about two radix-8 butterflies per thread
-	const int need = S * N / 16;
-	int T = 128;
-	while (T < need && T < 512) T *= 2;
-	return T;
+	int T = (S * N / 16 + 31) / 32 * 32;
+	return T < 64 ? 64 : (T > 512 ? 512 : T);
 }
+
+size_t fft_smem_bytes(int N, int S) { return 2 * sizeof(double2) * (size_t) S * seq_len_host(N); }
 
 void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st)
 {
 	const int T = fft_threads(p.N, p.S, p.rcode, p.nradix);
-	const size_t smem = 2 * sizeof(double2) * p.S * p.N;
+	const size_t smem = fft_smem_bytes(p.N, p.S);
 	dim3 grid((p.nlat + 2 * p.S - 1) / (2 * p.S), nfc);
 	fft_synth_kernel<<<grid, T, smem, st>>>(p);
 	shtb_count_launch();
@@ -296,7 +324,7 @@ void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st)
 void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st)
 {
 	const int T = fft_threads(p.N, p.S, p.rcode, p.nradix);
-	const size_t smem = 2 * sizeof(double2) * p.S * p.N;
+	const size_t smem = fft_smem_bytes(p.N, p.S);
 	dim3 grid((p.nlat + 2 * p.S - 1) / (2 * p.S), nfc);
 	fft_analys_kernel<<<grid, T, smem, st>>>(p);
 	shtb_count_launch();

@@ -142,6 +142,7 @@ struct FftParams {
 	int nf;                              // fields per component
 	long spat_dist;
 	int phi_contiguous;
+	int vec2;                            // spatial pointers 16-byte aligned: latitude pairs moved as double2
 };
 
 // ---- launchers (sht_legendre.cu / sht_fft.cu) ----
@@ -151,6 +152,7 @@ void launch_post_analys_m(const PrepParams& p, int mmax, cudaStream_t st);
 void launch_leg_synth(const LegParams& p, cudaStream_t st);
 void launch_leg_analys(const LegParams& p, int kmax_all, cudaStream_t st);
 int fft_threads(int N, int S, unsigned long long rcode, int nradix);
+size_t fft_smem_bytes(int N, int S);
 void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st);
 void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st);
 

@@ -70,70 +70,79 @@ __global__ void ck_kernel(int nlat_2, int mres, const double* __restrict__ x2g, 
 // for l = m..llim+1 (SH_vect_to_2scal, sht_private.h:534-584).
 // Column layout: field-component fc owns columns 16*(fc/4) + 2*(fc%4) + {0,1}
 // (even re, im) and the same +8 (odd re, im).
-__device__ __forceinline__ double2 ld_coef(const double2* base, long off, int j, int lrel_max, bool m0)
-{
-	if (base == nullptr || j < 0 || j > lrel_max) return make_double2(0.0, 0.0);
-	double2 v = base[off + j];
-	if (m0) v.y = 0.0;
-	return v;
-}
+//
+// CTA = (order im, 32 Ishioka rows k, 16 field-components): the degree window
+// [2k0-1, 2k0+66] of each input array is staged in shared memory with
+// coalesced loads, then every qq row segment is written contiguously.
+#define PT_K 32
+#define PT_F 16
+#define PT_W 69          // window length (68 needed), odd stride in 16-byte units
 
-__device__ __forceinline__ double2 vw_coef(const PrepParams& p, int type, long off, int f, int m, int voff,
-                                           int j, int lrel_max, bool m0)
+__global__ void __launch_bounds__(256) prep_synth_kernel(PrepParams p)
 {
-	// degree l = m + j, valid up to llim + 1 (lrel_max + 1)
-	if (j < 0 || j > lrel_max + 1) return make_double2(0.0, 0.0);
-	const double lo = (j > 0) ? p.stdt_lo[voff + j] : 0.0;
-	const double hi = p.stdt_hi[voff + j];
-	const long o = off + (long)f * p.spec_dist;
-	const double2 sm = ld_coef(p.S, o, j - 1, lrel_max, m0), sp = ld_coef(p.S, o, j + 1, lrel_max, m0);
-	const double2 tmm = ld_coef(p.T, o, j - 1, lrel_max, m0), tp = ld_coef(p.T, o, j + 1, lrel_max, m0);
-	const double2 s0 = ld_coef(p.S, o, j, lrel_max, m0), t0 = ld_coef(p.T, o, j, lrel_max, m0);
-	const double em = (double)m;
-	if (type == 1) {   // V = stdt S + i m T
-		return make_double2(lo * sm.x + hi * sp.x - em * t0.y, lo * sm.y + hi * sp.y + em * t0.x);
-	} else {           // W = -stdt T + i m S
-		return make_double2(-(lo * tmm.x + hi * tp.x) - em * s0.y, -(lo * tmm.y + hi * tp.y) + em * s0.x);
-	}
-}
-
-__global__ void prep_synth_kernel(PrepParams p)
-{
-	const int im = blockIdx.y;
+	__shared__ double2 win[2][PT_F][PT_W];
+	const int im = blockIdx.z;
 	if (im > p.mlim) return;
 	const int m = im * p.mres;
-	const int nfc = p.nf * p.ncomp;
 	const int kmax = (p.llim + 1 - m) / 2 + 1;
-	const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-	if (idx >= (long)kmax * nfc) return;
-	const int k = (int)(idx / nfc);
-	const int fc = (int)(idx - (long)k * nfc);
-	const int comp = fc / p.nf, f = fc - comp * p.nf;
-	const int type = p.comp_type[comp];
+	const int k0 = blockIdx.x * PT_K;
+	if (k0 >= kmax) return;
+	const int nfc = p.nf * p.ncomp;
+	const int fc0 = blockIdx.y * PT_F;
 	const bool m0 = (m == 0);
 	const int lrel_max = p.llim - m;
 	const long off = (long)im * (2 * p.lmax + 2 - (im + 1) * p.mres) / 2 + m;   // LM(m, m)
-	const double* X = p.xs + p.mt.xoff[im] + 3 * k;
-	double2 qa, qb, qc;   // relative degrees 2k, 2k+1, 2k+2
-	if (type == 0) {
-		const double2* Q = p.Q;
-		const long o = off + (long)f * p.spec_dist;
-		qa = ld_coef(Q, o, 2 * k, lrel_max, m0);
-		qb = ld_coef(Q, o, 2 * k + 1, lrel_max, m0);
-		qc = ld_coef(Q, o, 2 * k + 2, lrel_max, m0);
-	} else {
-		const int voff = p.mt.voff[im];
-		qa = vw_coef(p, type, off, f, m, voff, 2 * k, lrel_max, m0);
-		qb = vw_coef(p, type, off, f, m, voff, 2 * k + 1, lrel_max, m0);
-		qc = vw_coef(p, type, off, f, m, voff, 2 * k + 2, lrel_max, m0);
+	const int d0 = 2 * k0 - 1;
+	for (int e = threadIdx.x; e < 2 * PT_F * PT_W; e += blockDim.x) {
+		const int a = e / (PT_F * PT_W), r = e - a * PT_F * PT_W;
+		const int fl = r / PT_W, i = r - fl * PT_W;
+		const int fc = fc0 + fl, d = d0 + i;
+		double2 v = make_double2(0.0, 0.0);
+		if (fc < nfc && d >= 0 && d <= lrel_max) {
+			const int comp = fc / p.nf, f = fc - comp * p.nf;
+			const double2* base = (p.comp_type[comp] == 0) ? (a == 0 ? p.Q : nullptr) : (a == 0 ? p.S : p.T);
+			if (base) {
+				v = base[off + (long)f * p.spec_dist + d];
+				if (m0) v.y = 0.0;
+			}
+		}
+		win[a][fl][i] = v;
 	}
-	const double x0 = X[0], x1 = X[1], x2 = X[2];
-	const double2 qe = make_double2(fma(x0, qa.x, x1 * qc.x), fma(x0, qa.y, x1 * qc.y));
-	const double2 qo = make_double2(x2 * qb.x, x2 * qb.y);
-	double* row = p.qq + (long)(p.mt.koff[im] + k) * p.ncol;
-	const int ce = 16 * (fc >> 2) + 2 * (fc & 3);
-	*reinterpret_cast<double2*>(row + ce) = qe;
-	*reinterpret_cast<double2*>(row + ce + 8) = qo;
+	__syncthreads();
+	const int voff = p.mt.voff[im];
+	const double em = (double) m;
+	for (int e = threadIdx.x; e < PT_K * PT_F; e += blockDim.x) {
+		const int kl = e / PT_F, fl = e - kl * PT_F;
+		const int k = k0 + kl, fc = fc0 + fl;
+		if (k >= kmax || fc >= nfc) continue;
+		const int type = p.comp_type[fc / p.nf];
+		double2 q3[3];
+		#pragma unroll
+		for (int r = 0; r < 3; r++) {
+			const int d = 2 * k + r;               // relative degree
+			const int i = d - d0;                  // window index of degree d
+			if (type == 0) {
+				q3[r] = win[0][fl][i];
+			} else if (d > lrel_max + 1) {
+				q3[r] = make_double2(0.0, 0.0);
+			} else {
+				const double lo = (d > 0) ? p.stdt_lo[voff + d] : 0.0;
+				const double hi = p.stdt_hi[voff + d];
+				const double2 sm = win[0][fl][i - 1], sp = win[0][fl][i + 1], s0 = win[0][fl][i];
+				const double2 tmn = win[1][fl][i - 1], tp = win[1][fl][i + 1], t0 = win[1][fl][i];
+				if (type == 1)   // V = stdt S + i m T
+					q3[r] = make_double2(lo * sm.x + hi * sp.x - em * t0.y, lo * sm.y + hi * sp.y + em * t0.x);
+				else             // W = -stdt T + i m S
+					q3[r] = make_double2(-(lo * tmn.x + hi * tp.x) - em * s0.y, -(lo * tmn.y + hi * tp.y) + em * s0.x);
+			}
+		}
+		const double* X = p.xs + p.mt.xoff[im] + 3 * k;
+		const double x0 = X[0], x1 = X[1], x2 = X[2];
+		double* row = p.qq + (long)(p.mt.koff[im] + k) * p.ncol;
+		const int ce = 16 * (fc >> 2) + 2 * (fc & 3);
+		*reinterpret_cast<double2*>(row + ce) = make_double2(fma(x0, q3[0].x, x1 * q3[2].x), fma(x0, q3[0].y, x1 * q3[2].y));
+		*reinterpret_cast<double2*>(row + ce + 8) = make_double2(x2 * q3[1].x, x2 * q3[1].y);
+	}
 }
 
 // ---------------------------------------------------------------------------
@@ -143,80 +152,108 @@ __global__ void prep_synth_kernel(PrepParams p)
 //   S_l = -((MX V)_l + i m W_l) / (l(l+1)),  T_l = -(i m V_l - (MX W)_l) / (l(l+1))
 // with MX = 2 cos + sin d/dtheta (SH_2scal_to_vect, sht_private.h:296-337).
 // Degrees above llim and orders above mlim are written as zero (SHT_VAR_LTR).
-__device__ __forceinline__ double2 ish_inv(const PrepParams& p, const double* X, long row0, int col, int j)
+//
+// CTA = (order im, 64 degrees, 16 fields, output group): the k rows covering
+// the degree tile plus one row of halo on each side are staged in shared
+// memory for the (one or two) field-components of the group.
+#define PE_J 64
+#define PE_F 16
+#define PE_R 36          // staged k rows: j0/2-2 .. j0/2+33
+
+__device__ __forceinline__ double2 ish_inv_s(const double2 (*E)[PE_F][2], const double* X, int kb, int fl, int j)
 {
+	// E[row][field][0] = even pair (re, im), [1] = odd pair, row = k - kb
 	if (j < 0) return make_double2(0.0, 0.0);
 	const int k = j >> 1;
 	if ((j & 1) == 0) {
-		const double2 e = *reinterpret_cast<const double2*>(p.qq + (row0 + k) * p.ncol + col);
+		const double2 e = E[k - kb][fl][0];
 		double2 r = make_double2(X[3 * k] * e.x, X[3 * k] * e.y);
 		if (k > 0) {
-			const double2 e1 = *reinterpret_cast<const double2*>(p.qq + (row0 + k - 1) * p.ncol + col);
+			const double2 e1 = E[k - 1 - kb][fl][0];
 			r.x = fma(X[3 * (k - 1) + 1], e1.x, r.x);
 			r.y = fma(X[3 * (k - 1) + 1], e1.y, r.y);
 		}
 		return r;
-	} else {
-		const double2 o = *reinterpret_cast<const double2*>(p.qq + (row0 + k) * p.ncol + col + 8);
-		return make_double2(X[3 * k + 2] * o.x, X[3 * k + 2] * o.y);
 	}
+	const double2 o = E[k - kb][fl][1];
+	return make_double2(X[3 * k + 2] * o.x, X[3 * k + 2] * o.y);
 }
 
-__global__ void post_analys_kernel(PrepParams p)
+__global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 {
-	// one thread per (degree, field, output group); group 0 = scalar Q (if any),
-	// group g>0 = vector pair (S, T)
-	const int im = blockIdx.y;
+	__shared__ double2 sv[PE_R][PE_F][2];     // first component of the group (Q, or V)
+	__shared__ double2 sw[PE_R][PE_F][2];     // second component (W) for the vector group
+	const int im = blockIdx.z;
 	const int m = im * p.mres;
 	const int nl = p.lmax - m + 1;
-	const int ngroups = (p.comp_type[0] == 0) ? 1 + (p.ncomp > 1 ? 1 : 0) : 1;
-	const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-	if (idx >= (long)nl * p.nf * ngroups) return;
-	const int j = (int)(idx % nl);
-	const int rest = (int)(idx / nl);
-	const int f = rest % p.nf;
-	const int g = rest / p.nf;
+	const int j0 = blockIdx.x * PE_J;
+	if (j0 >= nl) return;
+	const bool has_q = (p.comp_type[0] == 0);
+	const int nft = (p.nf + PE_F - 1) / PE_F;
+	const int g = blockIdx.y / nft;                       // 0: first group, 1: second group
+	const int f0 = (blockIdx.y - g * nft) * PE_F;
+	const bool scalar_group = has_q && g == 0;
+	const bool zero_m = (im > p.mlim);
 	const long off = (long)im * (2 * p.lmax + 2 - (im + 1) * p.mres) / 2 + m;
-	const long o = off + (long)f * p.spec_dist + j;
-	const int l = m + j;
-	const bool scalar_group = (p.comp_type[0] == 0) && (g == 0);
-	const bool zero = (im > p.mlim) || (l > p.llim);
-	if (scalar_group) {
-		double2 q = make_double2(0.0, 0.0);
-		if (!zero) {
-			const int fc = f;   // scalar component is component 0
-			const int ce = 16 * (fc >> 2) + 2 * (fc & 3);
-			q = ish_inv(p, p.xa + p.mt.xoff[im], p.mt.koff[im], ce, j);
-			if (m == 0) q.y = 0.0;
-		}
-		p.Qo[o] = q;
-		return;
-	}
-	// vector pair: components V (type 1) and W (type 2)
-	const int cv = (p.comp_type[0] == 0) ? 1 : 0;
-	double2 s = make_double2(0.0, 0.0), t = make_double2(0.0, 0.0);
-	if (!zero) {
-		const int fcv = cv * p.nf + f, fcw = (cv + 1) * p.nf + f;
-		const int cev = 16 * (fcv >> 2) + 2 * (fcv & 3);
-		const int cew = 16 * (fcw >> 2) + 2 * (fcw & 3);
-		const double* X = p.xa + p.mt.xoff[im];
+	const int kb = j0 / 2 - 2;
+	const int nk = (p.llim + ((p.comp_type[0] | p.comp_type[1] | p.comp_type[2]) ? 1 : 0) - m) / 2 + 1;
+	if (!zero_m) {
+		const int cv = scalar_group ? 0 : (has_q ? 1 : 0);
 		const long r0 = p.mt.koff[im];
-		const double2 vm = ish_inv(p, X, r0, cev, j - 1), v0 = ish_inv(p, X, r0, cev, j), vp = ish_inv(p, X, r0, cev, j + 1);
-		const double2 wm = ish_inv(p, X, r0, cew, j - 1), w0 = ish_inv(p, X, r0, cew, j), wp = ish_inv(p, X, r0, cew, j + 1);
-		const int voff = p.mt.voff[im];
-		const double lo = (j > 0) ? p.van_lo[voff + j] : 0.0;
-		const double hi = p.van_hi[voff + j];
-		const double l2 = p.l2[l];
-		const double em = (double)m;
-		const double mxv_r = lo * vm.x + hi * vp.x, mxv_i = lo * vm.y + hi * vp.y;
-		const double mxw_r = lo * wm.x + hi * wp.x, mxw_i = lo * wm.y + hi * wp.y;
-		// i m W = (-m W.y, m W.x)
-		s = make_double2(-(mxv_r - em * w0.y) * l2, -(mxv_i + em * w0.x) * l2);
-		t = make_double2(-(-em * v0.y - mxw_r) * l2, -(em * v0.x - mxw_i) * l2);
-		if (m == 0) { s.y = 0.0; t.y = 0.0; }
+		for (int e = threadIdx.x; e < PE_R * PE_F * 2; e += blockDim.x) {
+			const int r = e / (PE_F * 2), rem = e - r * PE_F * 2;
+			const int fl = rem >> 1, eo = rem & 1;
+			const int k = kb + r, f = f0 + fl;
+			double2 v = make_double2(0.0, 0.0), w = make_double2(0.0, 0.0);
+			if (k >= 0 && k < nk && f < p.nf) {
+				const double* row = p.qq + (r0 + k) * p.ncol;
+				const int fcv = cv * p.nf + f;
+				v = *reinterpret_cast<const double2*>(row + 16 * (fcv >> 2) + 2 * (fcv & 3) + 8 * eo);
+				if (!scalar_group) {
+					const int fcw = (cv + 1) * p.nf + f;
+					w = *reinterpret_cast<const double2*>(row + 16 * (fcw >> 2) + 2 * (fcw & 3) + 8 * eo);
+				}
+			}
+			sv[r][fl][eo] = v;
+			sw[r][fl][eo] = w;
+		}
 	}
-	p.So[o] = s;
-	p.To[o] = t;
+	__syncthreads();
+	const double* X = p.xa + p.mt.xoff[im];
+	const int voff = p.mt.voff[im];
+	const double em = (double) m;
+	for (int e = threadIdx.x; e < PE_J * PE_F; e += blockDim.x) {
+		const int fl = e / PE_J, jl = e - fl * PE_J;
+		const int j = j0 + jl, f = f0 + fl;
+		if (j >= nl || f >= p.nf) continue;
+		const int l = m + j;
+		const long o = off + (long)f * p.spec_dist + j;
+		const bool zero = zero_m || (l > p.llim);
+		if (scalar_group) {
+			double2 q = make_double2(0.0, 0.0);
+			if (!zero) {
+				q = ish_inv_s(sv, X, kb, fl, j);
+				if (m == 0) q.y = 0.0;
+			}
+			p.Qo[o] = q;
+			continue;
+		}
+		double2 s = make_double2(0.0, 0.0), t = make_double2(0.0, 0.0);
+		if (!zero) {
+			const double2 vm = ish_inv_s(sv, X, kb, fl, j - 1), v0 = ish_inv_s(sv, X, kb, fl, j), vp = ish_inv_s(sv, X, kb, fl, j + 1);
+			const double2 wm = ish_inv_s(sw, X, kb, fl, j - 1), w0 = ish_inv_s(sw, X, kb, fl, j), wp = ish_inv_s(sw, X, kb, fl, j + 1);
+			const double lo = (j > 0) ? p.van_lo[voff + j] : 0.0;
+			const double hi = p.van_hi[voff + j];
+			const double l2 = p.l2[l];
+			const double mxv_r = lo * vm.x + hi * vp.x, mxv_i = lo * vm.y + hi * vp.y;
+			const double mxw_r = lo * wm.x + hi * wp.x, mxw_i = lo * wm.y + hi * wp.y;
+			s = make_double2(-(mxv_r - em * w0.y) * l2, -(mxv_i + em * w0.x) * l2);
+			t = make_double2(-(-em * v0.y - mxw_r) * l2, -(em * v0.x - mxw_i) * l2);
+			if (m == 0) { s.y = 0.0; t.y = 0.0; }
+		}
+		p.So[o] = s;
+		p.To[o] = t;
+	}
 }
 
 // ---------------------------------------------------------------------------
@@ -446,8 +483,8 @@ void launch_checkpoints(shtns_cfg s, cudaStream_t st)
 void launch_prep_synth(const PrepParams& p, cudaStream_t st)
 {
 	const int nfc = p.nf * p.ncomp;
-	const long rows = (long)((p.llim + 1) / 2 + 1) * nfc;
-	dim3 grid((unsigned)((rows + 255) / 256), p.mlim + 1);
+	const int kmax0 = (p.llim + 1) / 2 + 1;
+	dim3 grid((kmax0 + PT_K - 1) / PT_K, (nfc + PT_F - 1) / PT_F, p.mlim + 1);
 	prep_synth_kernel<<<grid, 256, 0, st>>>(p);
 	shtb_count_launch();
 }
@@ -473,8 +510,8 @@ void launch_leg_analys(const LegParams& p, int kmax_all, cudaStream_t st)
 void launch_post_analys_m(const PrepParams& p, int mmax, cudaStream_t st)
 {
 	const int ngroups = (p.comp_type[0] == 0) ? 1 + (p.ncomp > 1 ? 1 : 0) : 1;
-	const long n = (long)(p.lmax + 1) * p.nf * ngroups;
-	dim3 grid((unsigned)((n + 255) / 256), mmax + 1);
+	const int nft = (p.nf + PE_F - 1) / PE_F;
+	dim3 grid((p.lmax + 1 + PE_J - 1) / PE_J, nft * ngroups, mmax + 1);
 	post_analys_kernel<<<grid, 256, 0, st>>>(p);
 	shtb_count_launch();
 }

@@ -319,8 +319,8 @@ static int fft_factorize(int n, std::vector<int>& f)
 	int rmin = 8;
 	for (int r : f) rmin = r < rmin ? r : rmin;
 	(void) rmin;
-	// one CTA holds two buffers of a latitude pair (2 x nphi complex) in shared memory
-	return n == 1 && (int) f.size() <= FFT_MAX_FACTORS && n0 <= 7168;
+	// one CTA holds two padded buffers of a latitude pair in shared memory
+	return n == 1 && (int) f.size() <= FFT_MAX_FACTORS && fft_smem_bytes(n0, 1) <= 227 * 1024;
 }
 
 // ---------------------------------------------------------------------------
@@ -491,7 +491,7 @@ extern "C" int shtns_set_grid_auto(shtns_cfg s, enum shtns_type flags, double ep
 	if (np <= 2 * s->mmax) { plan_error("the sampling condition Nphi > 2*Mmax is not met."); return -1; }
 	if (nl > 65534 || np > 65534) { plan_error("Nlat or Nphi too large"); return -1; }
 	std::vector<int> rad;
-	if (!fft_factorize(np, rad)) { plan_error("Nphi must factor into 2, 3, 5 and 7 and not exceed 7168"); return -1; }
+	if (!fft_factorize(np, rad)) { plan_error("Nphi must factor into 2, 3, 5 and 7 and not exceed 6400"); return -1; }
 	if (layout & SHT_PHI_CONTIGUOUS && layout & SHT_THETA_CONTIGUOUS) { plan_error("conflicting layout flags"); return -1; }
 	shtns_unset_grid(s);
 	s->fft_radix = rad;
