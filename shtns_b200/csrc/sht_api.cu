@@ -69,7 +69,7 @@ LegParams leg_params(shtns_cfg s, const Job& j)
 	p.south_first = s->south_first; p.robert = s->robert;
 	p.mpos_inv = 1.0 / s->mpos_renorm;
 	p.x = s->d_x; p.x2 = s->d_x2; p.sinv = s->d_sinv; p.w = s->d_w; p.c = s->d_c;
-	p.ck = s->d_ck; p.mt = s->mt;
+	p.ck = s->d_ck; p.mt = s->mt; p.ckseg = s->ckseg;
 	p.nf = j.nf;
 	for (int c = 0; c < 3; c++) p.ctype[c] = j.type[c];
 	p.qq = s->d_qq; p.F = s->d_F;
@@ -111,10 +111,10 @@ FftParams fft_params(shtns_cfg s, const Job& j)
 	while (S > 1 && fft_smem_bytes(s->nphi, S) > 112 * 1024) S /= 2;
 	if (const char* e = getenv("SHTNS_B200_FFT_PAIRS")) {
 		int v = atoi(e);
-		if (v >= 1 && v <= 8) S = v;
-		while (S > 1 && fft_smem_bytes(s->nphi, S) > 227 * 1024) S--;
+		if (v == 1 || v == 2 || v == 4) S = v;
+		while (S > 1 && fft_smem_bytes(s->nphi, S) > 227 * 1024) S /= 2;
 	}
-	while (S > 1 && 2 * S > (int) s->nlat) S--;
+	while (S > 1 && 2 * S > (int) s->nlat) S /= 2;
 	p.S = S;
 	p.tw = s->d_tw; p.F = s->d_F;
 	p.fstride = (long)(s->mmax + 1) * s->nlat;

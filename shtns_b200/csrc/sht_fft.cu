@@ -127,6 +127,16 @@ template <> struct Dft<7> {
 // free of bank conflicts.
 __device__ __forceinline__ int sidx(int s, int i, int seq) { return s * seq + i + (i >> 3); }
 
+// q = x / d, r = x % d for 0 <= x < 2^22 with a float reciprocal and one
+// correction step (avoids the integer division sequence in the inner loops).
+__device__ __forceinline__ void divmod(int x, int d, float inv, int& q, int& r)
+{
+	q = __float2int_rz(__int2float_rn(x) * inv);
+	r = x - q * d;
+	if (r < 0) { q--; r += d; }
+	else if (r >= d) { q++; r -= d; }
+}
+
 // One Stockham pass of radix R over S sequences of length N, from X to Y.
 // Butterfly b of a sequence reads element b + q*N/R (q < R), applies twiddles
 // w^{q*k*N/(p*R)} with k = b mod p, runs the R-point DFT and writes element
@@ -138,18 +148,23 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ X, double2*
 	const int nbf = N / R;
 	const int total = S * nbf;
 	const int tstep = N / (p * R);
+	const float inv_nbf = 1.0f / nbf, inv_p = 1.0f / p;
 	for (int g = threadIdx.x; g < total; g += blockDim.x) {
-		const int sq = g / nbf, b = g - sq * nbf;
-		const int k = b % p;
+		int sq, b, q0, k;
+		divmod(g, nbf, inv_nbf, sq, b);
+		divmod(b, p, inv_p, q0, k);
 		double2 u[R];
 		#pragma unroll
 		for (int q = 0; q < R; q++) u[q] = X[sidx(sq, b + q * nbf, seq)];
 		if (k) {
+			// w^q by repeated multiplication from one table entry (error ~q ulp)
+			double2 w1 = __ldg(tw + k * tstep);
+			if (sign < 0) w1.y = -w1.y;
+			double2 w = w1;
 			#pragma unroll
 			for (int q = 1; q < R; q++) {
-				double2 w = __ldg(tw + q * k * tstep);
-				if (sign < 0) w.y = -w.y;
 				u[q] = cmul(u[q], w);
+				if (q + 1 < R) w = cmul(w, w1);
 			}
 		}
 		Dft<R>::run(u, sign);
@@ -181,19 +196,20 @@ __device__ __forceinline__ double2* fft_run(double2* X, double2* Y, int N, int S
 	return X;
 }
 
-__device__ __forceinline__ int seq_len(int N)
+__device__ __forceinline__ int seq_len(int N, int S)
 {
 	const int a = N + (N >> 3);
-	return a + ((2 - a) & 7);
+	return a + (((8 / S) - a) & 7);
 }
 
 // Synthesis: F[fc][m][theta] (m <= mlim) -> spatial field-component fc.
 // Sequence s of the CTA packs latitudes lat0+2s (real part) and lat0+2s+1
 // (imaginary part): Z_k = A_k + i B_k, Z_{N-k} = conj(A_k) + i conj(B_k).
-__global__ void fft_synth_kernel(FftParams p)
+template <int S>
+__global__ void __launch_bounds__(768) fft_synth_kernel(FftParams p)
 {
 	extern __shared__ double2 smem[];
-	const int N = p.N, S = p.S, T = blockDim.x, seq = seq_len(N);
+	const int N = p.N, T = blockDim.x, seq = seq_len(N, S);
 	double2* X = smem;
 	double2* Y = smem + S * seq;
 	const int fc = blockIdx.y;
@@ -206,22 +222,34 @@ __global__ void fft_synth_kernel(FftParams p)
 		const int s = e / nz, i = ml + 1 + (e - s * nz);
 		X[sidx(s, i, seq)] = make_double2(0.0, 0.0);
 	}
-	for (int e = threadIdx.x; e < (ml + 1) * S; e += T) {
-		const int k = e / S, s = e - k * S;
-		const int ra = lat0 + 2 * s;
-		double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
-		if (ra < p.nlat) {
-			a = Ff[(long)k * p.nlat + ra];
-			b = Ff[(long)k * p.nlat + ra + 1];
+	const int nload = (ml + 1) * S;
+	for (int e0 = threadIdx.x; e0 < nload; e0 += 4 * T) {
+		double2 a[4], b[4];
+		#pragma unroll
+		for (int u = 0; u < 4; u++) {
+			const int e = e0 + u * T;
+			const int k = e / S, s = e - k * S;
+			const int ra = lat0 + 2 * s;
+			a[u] = make_double2(0.0, 0.0); b[u] = make_double2(0.0, 0.0);
+			if (e < nload && ra < p.nlat) {
+				a[u] = __ldg(Ff + (long)k * p.nlat + ra);
+				b[u] = __ldg(Ff + (long)k * p.nlat + ra + 1);
+			}
 		}
-		if (k == 0) { a.y = 0.0; b.y = 0.0; }
-		X[sidx(s, k, seq)] = make_double2(a.x - b.y, a.y + b.x);
-		if (k > 0) X[sidx(s, N - k, seq)] = make_double2(a.x + b.y, b.x - a.y);
+		#pragma unroll
+		for (int u = 0; u < 4; u++) {
+			const int e = e0 + u * T;
+			if (e >= nload) continue;
+			const int k = e / S, s = e - k * S;
+			if (k == 0) { a[u].y = 0.0; b[u].y = 0.0; }
+			X[sidx(s, k, seq)] = make_double2(a[u].x - b[u].y, a[u].y + b[u].x);
+			if (k > 0) X[sidx(s, N - k, seq)] = make_double2(a[u].x + b[u].y, b[u].x - a[u].y);
+		}
 	}
 	__syncthreads();
 	X = fft_run(X, Y, N, S, seq, p.rcode, p.nradix, p.tw, +1);
 	const int c = fc / p.nf;
-	double* out = p.spat[c] + (long)(fc - c * p.nf) * p.spat_dist;
+	double* out = (c == 0 ? p.spat[0] : c == 1 ? p.spat[1] : p.spat[2]) + (long)(fc - c * p.nf) * p.spat_dist;
 	if (!p.phi_contiguous) {
 		for (int e = threadIdx.x; e < N * S; e += T) {
 			const int j = e / S, s = e - j * S;
@@ -248,26 +276,37 @@ __global__ void fft_synth_kernel(FftParams p)
 
 // Analysis: spatial field-component fc -> F[fc][m][theta] = A_m / N for m <= mlim,
 // with A_k = (Z_k + conj Z_{N-k})/2 and B_k = (Z_k - conj Z_{N-k})/(2i).
-__global__ void fft_analys_kernel(FftParams p)
+template <int S>
+__global__ void __launch_bounds__(768) fft_analys_kernel(FftParams p)
 {
 	extern __shared__ double2 smem[];
-	const int N = p.N, S = p.S, T = blockDim.x, seq = seq_len(N);
+	const int N = p.N, T = blockDim.x, seq = seq_len(N, S);
 	double2* X = smem;
 	double2* Y = smem + S * seq;
 	const int fc = blockIdx.y;
 	const int lat0 = blockIdx.x * 2 * S;
 	const int c = fc / p.nf;
-	const double* in = p.spat_in[c] + (long)(fc - c * p.nf) * p.spat_dist;
+	const double* in = (c == 0 ? p.spat_in[0] : c == 1 ? p.spat_in[1] : p.spat_in[2]) + (long)(fc - c * p.nf) * p.spat_dist;
 	if (!p.phi_contiguous) {
-		for (int e = threadIdx.x; e < N * S; e += T) {
-			const int j = e / S, s = e - j * S;
-			const int row = lat0 + 2 * s;
-			double2 v = make_double2(0.0, 0.0);
-			if (row < p.nlat) {
-				const double* i0 = in + (long)j * p.nlat + row;
-				v = p.vec2 ? *reinterpret_cast<const double2*>(i0) : make_double2(i0[0], i0[1]);
+		// 8 independent loads in flight per thread before the shared-memory stores
+		for (int e0 = threadIdx.x; e0 < N * S; e0 += 8 * T) {
+			double2 v[8];
+			#pragma unroll
+			for (int u = 0; u < 8; u++) {
+				const int e = e0 + u * T;
+				const int j = e / S, s = e - j * S;
+				const int row = lat0 + 2 * s;
+				v[u] = make_double2(0.0, 0.0);
+				if (e < N * S && row < p.nlat) {
+					const double* i0 = in + (long)j * p.nlat + row;
+					v[u] = p.vec2 ? __ldg(reinterpret_cast<const double2*>(i0)) : make_double2(__ldg(i0), __ldg(i0 + 1));
+				}
 			}
-			X[sidx(s, j, seq)] = v;
+			#pragma unroll
+			for (int u = 0; u < 8; u++) {
+				const int e = e0 + u * T;
+				if (e < N * S) { const int j = e / S, s = e - j * S; X[sidx(s, j, seq)] = v[u]; }
+			}
 		}
 	} else {
 		for (int e = threadIdx.x; e < N * S; e += T) {
@@ -296,28 +335,32 @@ __global__ void fft_analys_kernel(FftParams p)
 
 } // namespace
 
-static int seq_len_host(int N)
+static int seq_len_host(int N, int S)
 {
 	const int a = N + (N >> 3);
-	return a + ((2 - a) & 7);
+	return a + (((8 / S) - a) & 7);
 }
 
 int fft_threads(int N, int S, unsigned long long rcode, int nradix)
 {
 	(void) rcode; (void) nradix;
-	// about two radix-8 butterflies per thread
-	int T = (S * N / 16 + 31) / 32 * 32;
-	return T < 64 ? 64 : (T > 512 ? 512 : T);
+	// about one radix-8 butterfly per thread
+	int T = (S * N / 8 + 31) / 32 * 32;
+	return T < 64 ? 64 : (T > 768 ? 768 : T);
 }
 
-size_t fft_smem_bytes(int N, int S) { return 2 * sizeof(double2) * (size_t) S * seq_len_host(N); }
+size_t fft_smem_bytes(int N, int S) { return 2 * sizeof(double2) * (size_t) S * seq_len_host(N, S); }
 
 void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st)
 {
 	const int T = fft_threads(p.N, p.S, p.rcode, p.nradix);
 	const size_t smem = fft_smem_bytes(p.N, p.S);
 	dim3 grid((p.nlat + 2 * p.S - 1) / (2 * p.S), nfc);
-	fft_synth_kernel<<<grid, T, smem, st>>>(p);
+	switch (p.S) {
+		case 4: fft_synth_kernel<4><<<grid, T, smem, st>>>(p); break;
+		case 2: fft_synth_kernel<2><<<grid, T, smem, st>>>(p); break;
+		default: fft_synth_kernel<1><<<grid, T, smem, st>>>(p); break;
+	}
 	shtb_count_launch();
 }
 
@@ -326,12 +369,21 @@ void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st)
 	const int T = fft_threads(p.N, p.S, p.rcode, p.nradix);
 	const size_t smem = fft_smem_bytes(p.N, p.S);
 	dim3 grid((p.nlat + 2 * p.S - 1) / (2 * p.S), nfc);
-	fft_analys_kernel<<<grid, T, smem, st>>>(p);
+	switch (p.S) {
+		case 4: fft_analys_kernel<4><<<grid, T, smem, st>>>(p); break;
+		case 2: fft_analys_kernel<2><<<grid, T, smem, st>>>(p); break;
+		default: fft_analys_kernel<1><<<grid, T, smem, st>>>(p); break;
+	}
 	shtb_count_launch();
 }
 
 void fft_set_smem_limits()
 {
-	cudaFuncSetAttribute(fft_synth_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-	cudaFuncSetAttribute(fft_analys_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+	const int lim = 227 * 1024;
+	cudaFuncSetAttribute(fft_synth_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	cudaFuncSetAttribute(fft_synth_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	cudaFuncSetAttribute(fft_synth_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	cudaFuncSetAttribute(fft_analys_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	cudaFuncSetAttribute(fft_analys_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	cudaFuncSetAttribute(fft_analys_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }

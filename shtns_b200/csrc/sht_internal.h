@@ -16,7 +16,7 @@
 #define LG_BM 64      // synthesis: theta rows per CTA;  analysis: k rows per CTA
 #define LG_BN 64      // real columns per CTA (16 field-components x {E,O} x {re,im})
 #define LG_BK 32      // synthesis: k per chunk;  analysis: theta rows per chunk
-#define LG_SEG 32     // recurrence checkpoint spacing in k (== LG_BK)
+#define LG_SEG 32     // largest recurrence checkpoint spacing in k (== LG_BK)
 #define LG_THREADS 256
 
 // pipeline stages (for shtns_b200_stage_times)
@@ -75,6 +75,7 @@ struct shtns_info {
 	std::vector<double> l_2;             // 1/(l(l+1)), l_2[0] = 0
 	std::vector<int> koff_h, coff_h, xoff_h, voff_h, ckoff_h, tm_h, kmax_h;
 	long ktot, ctot, xtot, vtot, segtot;
+	int ckseg;                           // checkpoint spacing in k
 	std::vector<int> fft_radix;          // factorisation of nphi
 	double Y00_1, Y10_ct, Y11_st;
 	// device tables
@@ -109,6 +110,7 @@ struct shtns_info {
 struct LegParams {
 	int nlat, nlat_2, llim, mlim, mres, vec_extra;
 	int ncol, nfc;
+	int ckseg;                           // checkpoint spacing in k (8, 16 or 32)
 	int south_first, robert;
 	double mpos_inv;                     // analysis factor for m>0 (1/mpos_renorm)
 	const double *x, *x2, *sinv, *w, *c;

@@ -27,11 +27,11 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b)
 
 // ---------------------------------------------------------------------------
 // Checkpoints: thread (t, im) runs the recurrence of order m at north row t and
-// stores (Y_{32s}, Y_{32s+1}) for every segment s.  Y_0 = sin^m(theta) by
+// stores (Y_{seg*s}, Y_{seg*s+1}) for every segment s (seg = 8, 16 or 32).  Y_0 = sin^m(theta) by
 // binary powering (sint_pow_n_ext, sht_legendre.c:110-139, without the range
 // extension: below lmax 1800 an underflowed seed only drops values below
 // 1e-300), Y_1 = (c_1 x^2 + c_0) Y_0 (kernel_SH_to_spat.gen.c:303-315).
-__global__ void ck_kernel(int nlat_2, int mres, const double* __restrict__ x2g, const double* __restrict__ sing,
+__global__ void ck_kernel(int nlat_2, int mres, int seg, const double* __restrict__ x2g, const double* __restrict__ sing,
                           const double* __restrict__ c, MTables mt, const int* __restrict__ nseg, double2* __restrict__ ck)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -50,9 +50,9 @@ __global__ void ck_kernel(int nlat_2, int mres, const double* __restrict__ x2g, 
 	double2* out = ck + (long)mt.ckoff[im] * nlat_2 + t;
 	for (int s = 0; s < ns; s++) {
 		out[(long)s * nlat_2] = make_double2(y0, y1);
-		const int kb = s * LG_SEG + 1;
+		const int kb = s * seg + 1;
 		#pragma unroll 4
-		for (int j = 0; j < LG_SEG; j++) {
+		for (int j = 0; j < seg; j++) {
 			const int k = kb + j;
 			const double a = fma(cc[2 * k + 1], x2, cc[2 * k]);
 			const double y2 = fma(a, y1, y0);
@@ -263,7 +263,8 @@ __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 // of one (row, field-component) and folds north/south itself.
 #define SA_LD 68   // shared row stride in doubles: 4 mod 16 keeps fragment loads conflict-free
 
-__global__ void __launch_bounds__(LG_THREADS)
+template <int SEG>
+__global__ void __launch_bounds__(LG_THREADS, 3)
 leg_synth_kernel(LegParams p)
 {
 	__shared__ __align__(16) double As[LG_BK][SA_LD];   // [k][theta]
@@ -288,34 +289,53 @@ leg_synth_kernel(LegParams p)
 		const double* cm = p.c + p.mt.coff[im];
 		const double2* ckm = p.ck + (long)p.mt.ckoff[im] * p.nlat_2;
 		const double* qrow = p.qq + (long)p.mt.koff[im] * p.ncol;
+		// software pipeline: the B tile and checkpoint of chunk k0+32 are
+		// loaded into registers while the tensor cores work on chunk k0
+		constexpr int NBV = LG_BK * (LG_BN / 2) / LG_THREADS;   // double2 per thread
+		double2 bn[NBV];
+		// generators: thread (row gr, segment gj) produces Y_k for SEG
+		// consecutive k of the chunk from the checkpoint at its segment start
+		constexpr int NSEGC = LG_BK / SEG;
+		double2 ckn = make_double2(0.0, 0.0);
+		const int gr = tid % LG_BM, gj = tid / LG_BM;
+		const int tg = t0 + gr;
+		const bool gen = (gj < NSEGC) && (tg < p.nlat_2);
+		const double x2 = gen ? p.x2[tg] : 0.0;
+		auto load_b = [&](int k0) {
+			#pragma unroll
+			for (int u = 0; u < NBV; u++) {
+				const int e = tid + u * LG_THREADS;
+				const int kk = e / (LG_BN / 2), cc2 = (e - kk * (LG_BN / 2)) * 2;
+				const int k = k0 + kk, col = c0 + cc2;
+				bn[u] = (k < nk && col < p.ncol) ? __ldg(reinterpret_cast<const double2*>(qrow + (long)k * p.ncol + col))
+				                                 : make_double2(0.0, 0.0);
+			}
+			const int ks = k0 + gj * SEG;
+			ckn = (gen && ks < nk) ? __ldg(ckm + (long)(ks / SEG) * p.nlat_2 + tg) : make_double2(0.0, 0.0);
+		};
+		load_b(0);
 		for (int k0 = 0; k0 < nk; k0 += LG_BK) {
-			if (tid < LG_BM) {
-				const int t = t0 + tid;
-				double y0 = 0.0, y1 = 0.0, x2 = 0.0;
-				if (t < p.nlat_2) {
-					const double2 s = ckm[(long)(k0 / LG_SEG) * p.nlat_2 + t];
-					y0 = s.x; y1 = s.y; x2 = p.x2[t];
-				}
-				As[0][tid] = y0;
-				As[1][tid] = y1;
-				const double* cc = cm + 2 * k0;
-				#pragma unroll 6
-				for (int j = 2; j < LG_BK; j++) {
+			if (gj < NSEGC) {
+				double y0 = ckn.x, y1 = ckn.y;
+				As[gj * SEG][gr] = y0;
+				As[gj * SEG + 1][gr] = y1;
+				const double* cc = cm + 2 * (k0 + gj * SEG);
+				#pragma unroll
+				for (int j = 2; j < SEG; j++) {
 					const double a = fma(cc[2 * j - 1], x2, cc[2 * j - 2]);
 					const double y2 = fma(a, y1, y0);
-					As[j][tid] = y2;
+					As[gj * SEG + j][gr] = y2;
 					y0 = y1; y1 = y2;
 				}
 			}
-			for (int e = tid; e < LG_BK * (LG_BN / 2); e += LG_THREADS) {
+			#pragma unroll
+			for (int u = 0; u < NBV; u++) {
+				const int e = tid + u * LG_THREADS;
 				const int kk = e / (LG_BN / 2), cc2 = (e - kk * (LG_BN / 2)) * 2;
-				const int k = k0 + kk, col = c0 + cc2;
-				double2 v = make_double2(0.0, 0.0);
-				if (k < nk && col < p.ncol) v = *reinterpret_cast<const double2*>(qrow + (long)k * p.ncol + col);
-				Bs[kk][cc2] = v.x;
-				Bs[kk][cc2 + 1] = v.y;
+				*reinterpret_cast<double2*>(&Bs[kk][cc2]) = bn[u];
 			}
 			__syncthreads();
+			if (k0 + LG_BK < nk) load_b(k0 + LG_BK);
 			#pragma unroll
 			for (int kk = 0; kk < LG_BK; kk += 4) {
 				double a[4], b[2];
@@ -360,7 +380,8 @@ leg_synth_kernel(LegParams p)
 // 1/sin(theta) for vector components (1/sin^2 in Robert form).
 #define AA_LD 36   // As row stride (k rows x 32 theta): 4 mod 16
 
-__global__ void __launch_bounds__(LG_THREADS)
+template <int SEG>
+__global__ void __launch_bounds__(LG_THREADS, 3)
 leg_analys_kernel(LegParams p, int nkb)
 {
 	__shared__ __align__(16) double As[LG_BM][AA_LD];   // [k][theta]
@@ -385,40 +406,65 @@ leg_analys_kernel(LegParams p, int nkb)
 		#pragma unroll
 		for (int j = 0; j < 2; j++) { acc[i][j][0] = 0.0; acc[i][j][1] = 0.0; }
 
-	for (int tt0 = (tmm / LG_BK) * LG_BK; tt0 < p.nlat_2; tt0 += LG_BK) {
-		if (tid < 2 * LG_BK) {
-			const int tt = tid & (LG_BK - 1), sgi = tid / LG_BK;
-			const int t = tt0 + tt, ks = k0 + sgi * LG_SEG;
-			double y0 = 0.0, y1 = 0.0, x2 = 0.0;
-			if (t < p.nlat_2 && ks < nk) {
-				const double2 s = ckm[(long)(ks / LG_SEG) * p.nlat_2 + t];
-				y0 = s.x; y1 = s.y; x2 = p.x2[t];
+	// software pipeline: F values and checkpoints of the next theta chunk are
+	// loaded into registers while the tensor cores work on the current one
+	constexpr int NBF = LG_BK * (LG_BN / 4) / LG_THREADS;   // (theta, field-component) items per thread
+	double2 fnn[NBF], fsn[NBF];
+	// generators: thread (theta gtt, segment gsg) produces Y_k for SEG
+	// consecutive k of the CTA's k rows from the checkpoint at its segment start
+	double2 ckn = make_double2(0.0, 0.0);
+	const int gtt = tid % LG_BK, gsg = tid / LG_BK;
+	const int gks = k0 + gsg * SEG;
+	const bool gen_thread = gsg < LG_BM / SEG;
+	auto load_next = [&](int tt0) {
+		#pragma unroll
+		for (int u = 0; u < NBF; u++) {
+			const int e = tid + u * LG_THREADS;
+			const int tt = e % LG_BK, fl = e / LG_BK;
+			const int t = tt0 + tt, fc = fc0 + fl;
+			fnn[u] = make_double2(0.0, 0.0); fsn[u] = make_double2(0.0, 0.0);
+			if (t < p.nlat_2 && t >= tmm && fc < p.nfc) {
+				const int rn = p.south_first ? p.nlat - 1 - t : t;
+				const int rs = p.nlat - 1 - rn;
+				const double2* Ff = p.F + (long)fc * p.fstride + (long)im * p.nlat;
+				fnn[u] = __ldg(Ff + rn);
+				fsn[u] = __ldg(Ff + rs);
 			}
-			double* a = &As[sgi * LG_SEG][tt];
+		}
+		const int t = tt0 + gtt;
+		if (gen_thread && t < p.nlat_2 && gks < nk) ckn = __ldg(ckm + (long)(gks / SEG) * p.nlat_2 + t);
+		else ckn = make_double2(0.0, 0.0);
+	};
+	const int tstart = (tmm / LG_BK) * LG_BK;
+	if (tstart < p.nlat_2) load_next(tstart);
+	for (int tt0 = tstart; tt0 < p.nlat_2; tt0 += LG_BK) {
+		if (gen_thread) {
+			const int t = tt0 + gtt;
+			double y0 = ckn.x, y1 = ckn.y;
+			const double x2 = (t < p.nlat_2) ? p.x2[t] : 0.0;
+			double* a = &As[gsg * SEG][gtt];
 			a[0] = y0;
 			a[AA_LD] = y1;
-			if (ks < nk) {
-				const double* cc = cm + 2 * ks;
-				#pragma unroll 6
-				for (int j = 2; j < LG_SEG; j++) {
+			if (gks < nk) {
+				const double* cc = cm + 2 * gks;
+				#pragma unroll
+				for (int j = 2; j < SEG; j++) {
 					const double aa = fma(cc[2 * j - 1], x2, cc[2 * j - 2]);
 					const double y2 = fma(aa, y1, y0);
 					a[j * AA_LD] = y2;
 					y0 = y1; y1 = y2;
 				}
 			} else {
-				for (int j = 2; j < LG_SEG; j++) a[j * AA_LD] = 0.0;
+				for (int j = 2; j < SEG; j++) a[j * AA_LD] = 0.0;
 			}
 		}
-		for (int e = tid; e < LG_BK * (LG_BN / 4); e += LG_THREADS) {
+		#pragma unroll
+		for (int u = 0; u < NBF; u++) {
+			const int e = tid + u * LG_THREADS;
 			const int tt = e % LG_BK, fl = e / LG_BK;
 			const int t = tt0 + tt, fc = fc0 + fl;
 			double er = 0.0, ei = 0.0, orr = 0.0, oi = 0.0;
-			if (t < p.nlat_2 && t >= tmm && fc < p.nfc) {
-				const int rn = p.south_first ? p.nlat - 1 - t : t;
-				const int rs = p.nlat - 1 - rn;
-				const double2* Ff = p.F + (long)fc * p.fstride + (long)im * p.nlat;
-				const double2 fn = Ff[rn], fs = Ff[rs];
+			if (t < p.nlat_2 && fc < p.nfc) {
 				double w = p.w[t] * wfac;
 				if (p.ctype[fc / p.nf] != 0) {
 					double s = p.sinv[t];
@@ -426,14 +472,16 @@ leg_analys_kernel(LegParams p, int nkb)
 					w *= s;
 				}
 				const double wo = w * p.x[t];
+				const double2 fn = fnn[u], fs = fsn[u];
 				er = w * (fn.x + fs.x);  ei = w * (fn.y + fs.y);
 				orr = wo * (fn.x - fs.x); oi = wo * (fn.y - fs.y);
 			}
 			const int cb = 16 * (fl >> 2) + 2 * (fl & 3);
-			Bs[tt][cb] = er;  Bs[tt][cb + 1] = ei;
-			Bs[tt][cb + 8] = orr;  Bs[tt][cb + 9] = oi;
+			*reinterpret_cast<double2*>(&Bs[tt][cb]) = make_double2(er, ei);
+			*reinterpret_cast<double2*>(&Bs[tt][cb + 8]) = make_double2(orr, oi);
 		}
 		__syncthreads();
+		if (tt0 + LG_BK < p.nlat_2) load_next(tt0 + LG_BK);
 		#pragma unroll
 		for (int kk = 0; kk < LG_BK; kk += 4) {
 			double a[4], b[2];
@@ -468,12 +516,12 @@ leg_analys_kernel(LegParams p, int nkb)
 void launch_checkpoints(shtns_cfg s, cudaStream_t st)
 {
 	std::vector<int> nseg(s->mmax + 1);
-	for (int im = 0; im <= s->mmax; im++) nseg[im] = (s->kmax_h[im] + LG_SEG - 1) / LG_SEG;
+	for (int im = 0; im <= s->mmax; im++) nseg[im] = (s->kmax_h[im] + s->ckseg - 1) / s->ckseg;
 	int* d_nseg = nullptr;
 	if (!shtb_cuda_ok(cudaMalloc(&d_nseg, sizeof(int) * nseg.size()), "checkpoint table")) return;
 	cudaMemcpyAsync(d_nseg, nseg.data(), sizeof(int) * nseg.size(), cudaMemcpyHostToDevice, st);
 	dim3 grid((s->nlat_2 + 127) / 128, s->mmax + 1);
-	ck_kernel<<<grid, 128, 0, st>>>(s->nlat_2, s->mres, s->d_x2, s->d_s, s->d_c, s->mt, d_nseg, s->d_ck);
+	ck_kernel<<<grid, 128, 0, st>>>(s->nlat_2, s->mres, s->ckseg, s->d_x2, s->d_s, s->d_c, s->mt, d_nseg, s->d_ck);
 	shtb_count_launch();
 	shtb_cuda_ok(cudaGetLastError(), "checkpoint kernel");
 	cudaStreamSynchronize(st);
@@ -494,7 +542,11 @@ void launch_leg_synth(const LegParams& p, cudaStream_t st)
 	const int ntb = (p.nlat_2 + LG_BM - 1) / LG_BM;
 	const int nnb = (p.ncol + LG_BN - 1) / LG_BN;
 	dim3 grid(ntb * nnb, p.mlim + 1);
-	leg_synth_kernel<<<grid, LG_THREADS, 0, st>>>(p);
+	switch (p.ckseg) {
+		case 8: leg_synth_kernel<8><<<grid, LG_THREADS, 0, st>>>(p); break;
+		case 16: leg_synth_kernel<16><<<grid, LG_THREADS, 0, st>>>(p); break;
+		default: leg_synth_kernel<32><<<grid, LG_THREADS, 0, st>>>(p); break;
+	}
 	shtb_count_launch();
 }
 
@@ -503,7 +555,11 @@ void launch_leg_analys(const LegParams& p, int kmax_all, cudaStream_t st)
 	const int nkb = (kmax_all + LG_BM - 1) / LG_BM;
 	const int nnb = (p.ncol + LG_BN - 1) / LG_BN;
 	dim3 grid(nkb * nnb, p.mlim + 1);
-	leg_analys_kernel<<<grid, LG_THREADS, 0, st>>>(p, nkb);
+	switch (p.ckseg) {
+		case 8: leg_analys_kernel<8><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
+		case 16: leg_analys_kernel<16><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
+		default: leg_analys_kernel<32><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
+	}
 	shtb_count_launch();
 }
 

@@ -166,15 +166,15 @@ static void ishioka_tables(shtns_cfg s)
 	for (int im = 0; im <= mmax; im++) {
 		const int m = im * mres;
 		const int kmax = (lmax + 1 - m) / 2 + 1;         // Y_k rows for degrees up to lmax+1
-		const int nseg = (kmax + LG_SEG - 1) / LG_SEG;
+		const int nseg = (kmax + LG_SEG - 1) / LG_SEG;     // coefficient padding: whole 32-step chunks
 		s->kmax_h[im] = kmax;
 		s->koff_h[im] = (int) kt;  kt += kmax;
 		s->coff_h[im] = (int) ct;  ct += 2 * (nseg * LG_SEG + 2);
 		s->xoff_h[im] = (int) xt;  xt += 3 * (kmax + 1);
 		s->voff_h[im] = (int) vt;  vt += lmax + 3 - m;
-		s->ckoff_h[im] = (int) sg; sg += nseg;
 	}
 	s->ktot = kt; s->ctot = ct; s->xtot = xt; s->vtot = vt; s->segtot = sg;
+	(void) sg;
 	s->ish_c.assign(ct, 0.0);
 	s->ish_xs.assign(xt, 0.0);
 	s->ish_xa.assign(xt, 0.0);
@@ -529,6 +529,20 @@ extern "C" int shtns_set_grid_auto(shtns_cfg s, enum shtns_type flags, double ep
 			} while (v < eps);
 			s->tm_h[im] = it < s->nlat_2 ? it : s->nlat_2;
 		}
+	}
+	// recurrence checkpoints every 8 degrees-pairs when they take at most
+	// 512 MB (all threads of a CTA then generate its Y tile in parallel),
+	// else every 16 or 32
+	for (s->ckseg = 8; s->ckseg < LG_SEG; s->ckseg *= 2) {
+		long segs = 0;
+		for (int im = 0; im <= s->mmax; im++) segs += (s->kmax_h[im] + s->ckseg - 1) / s->ckseg;
+		if ((double) segs * s->nlat_2 * 16.0 <= 512.0 * 1024 * 1024) break;
+	}
+	s->ckoff_h.assign(s->mmax + 1, 0);
+	s->segtot = 0;
+	for (int im = 0; im <= s->mmax; im++) {
+		s->ckoff_h[im] = (int) s->segtot;
+		s->segtot += (s->kmax_h[im] + s->ckseg - 1) / s->ckseg;
 	}
 	if (init_device(s) != 0) { plan_error("GPU initialisation failed: " + g_last_error); return -1; }
 	s->grid_set = 1;
