@@ -57,6 +57,20 @@ int shtns_b200_stage_times(shtns_cfg, double* ms, long* calls);
  * reference's PolarOptimize does).  Writes mmax+1 ints; returns mmax+1. */
 int shtns_b200_polar_rows(shtns_cfg, int* tm);
 
+/* Scalar synthesis (same result as cu_SH_to_spat on device pointers) that
+ * allocates no device memory, for callers that cannot call cudaMalloc where
+ * they transform.  Its scratch is one static device array of 32 MiB that
+ * every GPU loading this library holds until the process exits; plan and
+ * batch must need at most that much (coefficient buffer + Fourier buffer,
+ * e.g. one field up to lmax=511 on 768x1536), larger requests are rejected
+ * with an error (shtns_b200_status() == 1) and nothing is written.  The
+ * first call on a device resolves the array's address (and may load this
+ * library's device code): make it before any stream capture.  All calls
+ * share the array, so calls that overlap on the GPU race and must be
+ * serialised by the caller.  Asynchronous on the plan's compute stream.
+ * No counterpart in the reference. */
+void cu_SH_to_spat_noalloc(shtns_cfg, cplx *Qlm, double *Vr, int ltr);
+
 #ifdef __cplusplus
 }
 #endif

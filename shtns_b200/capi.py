@@ -108,6 +108,7 @@ PROTOTYPES = {
     "shtns_b200_set_timing": (None, [CFG, I]),
     "shtns_b200_stage_times": (I, [CFG, P, P]),
     "shtns_b200_polar_rows": (I, [CFG, P]),
+    "cu_SH_to_spat_noalloc": (None, [CFG, P, P, I]),
 }
 
 _lib = None
