@@ -333,6 +333,263 @@ __global__ void __launch_bounds__(768) fft_analys_kernel(FftParams p)
 	}
 }
 
+// ===========================================================================
+// Fused kernels for nphi = 3 * 2^k (192 ... 6144), the sizes of Gauss grids
+// with nphi = 2 nlat = 3 (lmax+1).  The radix sequence is fixed at compile
+// time, so every index, stride and twiddle step is a constant.  The first
+// pass reads its butterfly inputs straight from global memory (no staging
+// copy) and, for synthesis, the last pass writes straight to global memory.
+// Intermediate passes work in place in one padded shared buffer: each thread
+// loads its butterflies into registers, the block synchronises, then writes.
+// Thread g of the block handles sequence g % S and butterfly g / S, so the
+// S sequences of a butterfly index are neighbours in a warp (contiguous
+// 16-byte latitude pairs in global memory).
+template <int... Rs> struct RadixList {};
+
+template <int N> struct NphiPlan;
+template <> struct NphiPlan<192>  { using L = RadixList<8, 8, 3>; };
+template <> struct NphiPlan<384>  { using L = RadixList<8, 4, 4, 3>; };
+template <> struct NphiPlan<768>  { using L = RadixList<8, 8, 4, 3>; };
+template <> struct NphiPlan<1536> { using L = RadixList<8, 8, 8, 3>; };
+template <> struct NphiPlan<3072> { using L = RadixList<8, 8, 4, 4, 3>; };
+template <> struct NphiPlan<6144> { using L = RadixList<8, 8, 8, 4, 3>; };
+
+template <int N, int S>
+struct Geo {
+	static constexpr int A = N + (N >> 3);
+	static constexpr int SEQ = A + (((8 / S) - A) & 7);
+	static constexpr int T = S * N / 8;                     // one radix-8 butterfly per thread
+	static __device__ __forceinline__ int at(int s, int i) { return s * SEQ + i + (i >> 3); }
+};
+
+// twiddle powers u[q] *= w^q, w = exp(sign 2 pi i k step / N)
+template <int R>
+__device__ __forceinline__ void twiddle(double2* u, const double2* __restrict__ tw, int idx, int sign)
+{
+	double2 w1 = __ldg(tw + idx);
+	if (sign < 0) w1.y = -w1.y;
+	double2 w = w1;
+	#pragma unroll
+	for (int q = 1; q < R; q++) {
+		u[q] = cmul(u[q], w);
+		if (q + 1 < R) w = cmul(w, w1);
+	}
+}
+
+// One middle pass (in place in X).  P = product of earlier radices.
+template <int N, int S, int R, int P>
+__device__ __forceinline__ void mid_pass(double2* X, const double2* __restrict__ tw, int sign)
+{
+	using G = Geo<N, S>;
+	constexpr int NBF = N / R, TOT = S * NBF, NB = (TOT + G::T - 1) / G::T, TSTEP = N / (P * R);
+	double2 u[NB][R];
+	int dst[NB], ss[NB];
+	#pragma unroll
+	for (int i = 0; i < NB; i++) {
+		const int g = threadIdx.x + i * G::T;
+		dst[i] = -1;
+		if (g < TOT) {
+			const int s = g % S, b = g / S, k = b % P;
+			#pragma unroll
+			for (int q = 0; q < R; q++) u[i][q] = X[G::at(s, b + q * NBF)];
+			if (P > 1 && k) twiddle<R>(u[i], tw, k * TSTEP, sign);
+			Dft<R>::run(u[i], sign);
+			dst[i] = (b - k) * R + k;
+			ss[i] = s;
+		}
+	}
+	__syncthreads();
+	#pragma unroll
+	for (int i = 0; i < NB; i++)
+		if (dst[i] >= 0) {
+			#pragma unroll
+			for (int q = 0; q < R; q++) X[G::at(ss[i], dst[i] + q * P)] = u[i][q];
+		}
+	__syncthreads();
+}
+
+// Pass chain: first pass from a loader, middle passes in shared memory, last
+// pass either to shared memory (analysis) or to a storer (synthesis).
+template <int N, int S, int P, bool TO_GLOBAL, int R, int... Rest>
+struct Chain {
+	template <class Store>
+	static __device__ __forceinline__ void run(double2* X, const double2* tw, int sign, Store& st)
+	{
+		if constexpr (sizeof...(Rest) == 0) {
+			if constexpr (TO_GLOBAL) {
+				// last pass: k = b (b < P = N/R), outputs b + q*P go to global memory
+				using G = Geo<N, S>;
+				constexpr int NBF = N / R, TOT = S * NBF, NB = (TOT + G::T - 1) / G::T, TSTEP = N / (P * R);
+				#pragma unroll
+				for (int i = 0; i < NB; i++) {
+					const int g = threadIdx.x + i * G::T;
+					if (g < TOT) {
+						const int s = g % S, b = g / S;
+						double2 u[R];
+						#pragma unroll
+						for (int q = 0; q < R; q++) u[q] = X[G::at(s, b + q * NBF)];
+						if (b) twiddle<R>(u, tw, b * TSTEP, sign);
+						Dft<R>::run(u, sign);
+						#pragma unroll
+						for (int q = 0; q < R; q++) st(s, b + q * P, u[q]);
+					}
+				}
+			} else {
+				mid_pass<N, S, R, P>(X, tw, sign);
+			}
+		} else {
+			mid_pass<N, S, R, P>(X, tw, sign);
+			Chain<N, S, P * R, TO_GLOBAL, Rest...>::run(X, tw, sign, st);
+		}
+	}
+};
+
+template <int N, int S, bool TO_GLOBAL, class Load, class Store, int R0, int... Rest>
+__device__ __forceinline__ void fused_fft(double2* X, const double2* tw, int sign, Load& ld, Store& st, RadixList<R0, Rest...>)
+{
+	// first pass: butterfly b reads elements b + q*N/R0 from global, no twiddles
+	using G = Geo<N, S>;
+	constexpr int NBF = N / R0, TOT = S * NBF, NB = (TOT + G::T - 1) / G::T;
+	double2 u[NB][R0];
+	#pragma unroll
+	for (int i = 0; i < NB; i++) {
+		const int g = threadIdx.x + i * G::T;
+		if (g < TOT) {
+			const int s = g % S, b = g / S;
+			#pragma unroll
+			for (int q = 0; q < R0; q++) u[i][q] = ld(s, b + q * NBF);
+		}
+	}
+	#pragma unroll
+	for (int i = 0; i < NB; i++) {
+		const int g = threadIdx.x + i * G::T;
+		if (g < TOT) {
+			const int s = g % S, b = g / S;
+			Dft<R0>::run(u[i], sign);
+			#pragma unroll
+			for (int q = 0; q < R0; q++) X[G::at(s, b * R0 + q)] = u[i][q];
+		}
+	}
+	__syncthreads();
+	Chain<N, S, R0, TO_GLOBAL, Rest...>::run(X, tw, sign, st);
+}
+
+template <int N, int S>
+__global__ void __launch_bounds__(Geo<N, S>::T) fft3_synth_kernel(FftParams p)
+{
+	extern __shared__ double2 smem[];
+	const int fc = blockIdx.y;
+	const int lat0 = blockIdx.x * 2 * S;
+	const double2* __restrict__ Ff = p.F + (long)fc * p.fstride;
+	const int ml = p.mlim, nlat = p.nlat;
+	auto ld = [&](int s, int j) -> double2 {
+		const int ra = lat0 + 2 * s;
+		const int k = (j <= ml) ? j : ((j >= N - ml) ? N - j : -1);
+		if (k < 0 || ra >= nlat) return make_double2(0.0, 0.0);
+		double2 a = __ldg(Ff + (long)k * nlat + ra), b = __ldg(Ff + (long)k * nlat + ra + 1);
+		if (k == 0) { a.y = 0.0; b.y = 0.0; }
+		return (j <= ml) ? make_double2(a.x - b.y, a.y + b.x) : make_double2(a.x + b.y, b.x - a.y);
+	};
+	const int c = fc / p.nf;
+	double* out = (c == 0 ? p.spat[0] : c == 1 ? p.spat[1] : p.spat[2]) + (long)(fc - c * p.nf) * p.spat_dist;
+	const bool phi = p.phi_contiguous, v2 = p.vec2;
+	auto st = [&](int s, int j, double2 z) {
+		const int row = lat0 + 2 * s;
+		if (row >= nlat) return;
+		if (!phi) {
+			double* o = out + (long)j * nlat + row;
+			if (v2) *reinterpret_cast<double2*>(o) = z;
+			else { o[0] = z.x; o[1] = z.y; }
+		} else {
+			out[(long)row * N + j] = z.x;
+			out[(long)(row + 1) * N + j] = z.y;
+		}
+	};
+	fused_fft<N, S, true>(smem, p.tw, +1, ld, st, typename NphiPlan<N>::L{});
+}
+
+template <int N, int S>
+__global__ void __launch_bounds__(Geo<N, S>::T) fft3_analys_kernel(FftParams p)
+{
+	extern __shared__ double2 smem[];
+	using G = Geo<N, S>;
+	const int fc = blockIdx.y;
+	const int lat0 = blockIdx.x * 2 * S;
+	const int nlat = p.nlat;
+	const int c = fc / p.nf;
+	const double* in = (c == 0 ? p.spat_in[0] : c == 1 ? p.spat_in[1] : p.spat_in[2]) + (long)(fc - c * p.nf) * p.spat_dist;
+	const bool phi = p.phi_contiguous, v2 = p.vec2;
+	auto ld = [&](int s, int j) -> double2 {
+		const int row = lat0 + 2 * s;
+		if (row >= nlat) return make_double2(0.0, 0.0);
+		if (!phi) {
+			const double* i0 = in + (long)j * nlat + row;
+			return v2 ? __ldg(reinterpret_cast<const double2*>(i0)) : make_double2(__ldg(i0), __ldg(i0 + 1));
+		}
+		return make_double2(__ldg(in + (long)row * N + j), __ldg(in + (long)(row + 1) * N + j));
+	};
+	int dummy = 0;
+	auto st = [&](int, int, double2) { dummy++; };
+	fused_fft<N, S, false>(smem, p.tw, -1, ld, st, typename NphiPlan<N>::L{});
+	double2* Ff = p.F + (long)fc * p.fstride;
+	const double sc = 0.5 / N;
+	for (int e = threadIdx.x; e < (p.mlim + 1) * S; e += G::T) {
+		const int k = e / S, s = e - k * S;
+		const int ra = lat0 + 2 * s;
+		const double2 z = smem[G::at(s, k)];
+		const double2 w = smem[G::at(s, k ? N - k : 0)];
+		if (ra < nlat) {
+			Ff[(long)k * nlat + ra] = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
+			Ff[(long)k * nlat + ra + 1] = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
+		}
+	}
+}
+
+template <int N, int S>
+bool launch_fft3(const FftParams& p, int nfc, cudaStream_t st, bool synth)
+{
+	using G = Geo<N, S>;
+	const size_t smem = sizeof(double2) * (size_t) S * G::SEQ;
+	dim3 grid((p.nlat + 2 * S - 1) / (2 * S), nfc);
+	if (synth) fft3_synth_kernel<N, S><<<grid, G::T, smem, st>>>(p);
+	else fft3_analys_kernel<N, S><<<grid, G::T, smem, st>>>(p);
+	return true;
+}
+
+template <int N>
+bool launch_fft3_n(const FftParams& p, int nfc, cudaStream_t st, bool synth)
+{
+	// latitude pairs per CTA: up to 4 while the block stays at <= 768 threads
+	if (4 * N / 8 <= 768 && p.S >= 4) return launch_fft3<N, 4>(p, nfc, st, synth);
+	if (2 * N / 8 <= 768 && p.S >= 2) return launch_fft3<N, 2>(p, nfc, st, synth);
+	return launch_fft3<N, 1>(p, nfc, st, synth);
+}
+
+bool launch_fused(const FftParams& p, int nfc, cudaStream_t st, bool synth)
+{
+	switch (p.N) {
+		case 192: return launch_fft3_n<192>(p, nfc, st, synth);
+		case 384: return launch_fft3_n<384>(p, nfc, st, synth);
+		case 768: return launch_fft3_n<768>(p, nfc, st, synth);
+		case 1536: return launch_fft3_n<1536>(p, nfc, st, synth);
+		case 3072: return launch_fft3_n<3072>(p, nfc, st, synth);
+		case 6144: return launch_fft3_n<6144>(p, nfc, st, synth);
+		default: return false;
+	}
+}
+
+template <int N>
+void set_fused_limits()
+{
+	const int lim = 227 * 1024;
+	cudaFuncSetAttribute(fft3_synth_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	cudaFuncSetAttribute(fft3_synth_kernel<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	cudaFuncSetAttribute(fft3_synth_kernel<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	cudaFuncSetAttribute(fft3_analys_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	cudaFuncSetAttribute(fft3_analys_kernel<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	cudaFuncSetAttribute(fft3_analys_kernel<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+}
+
 } // namespace
 
 static int seq_len_host(int N, int S)
@@ -353,6 +610,7 @@ size_t fft_smem_bytes(int N, int S) { return 2 * sizeof(double2) * (size_t) S * 
 
 void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st)
 {
+	if (!p.generic && launch_fused(p, nfc, st, true)) { shtb_count_launch(); return; }
 	const int T = fft_threads(p.N, p.S, p.rcode, p.nradix);
 	const size_t smem = fft_smem_bytes(p.N, p.S);
 	dim3 grid((p.nlat + 2 * p.S - 1) / (2 * p.S), nfc);
@@ -366,6 +624,7 @@ void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st)
 
 void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st)
 {
+	if (!p.generic && launch_fused(p, nfc, st, false)) { shtb_count_launch(); return; }
 	const int T = fft_threads(p.N, p.S, p.rcode, p.nradix);
 	const size_t smem = fft_smem_bytes(p.N, p.S);
 	dim3 grid((p.nlat + 2 * p.S - 1) / (2 * p.S), nfc);
@@ -379,6 +638,8 @@ void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st)
 
 void fft_set_smem_limits()
 {
+	set_fused_limits<192>(); set_fused_limits<384>(); set_fused_limits<768>();
+	set_fused_limits<1536>(); set_fused_limits<3072>(); set_fused_limits<6144>();
 	const int lim = 227 * 1024;
 	cudaFuncSetAttribute(fft_synth_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 	cudaFuncSetAttribute(fft_synth_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);

@@ -145,6 +145,7 @@ struct FftParams {
 	long spat_dist;
 	int phi_contiguous;
 	int vec2;                            // spatial pointers 16-byte aligned: latitude pairs moved as double2
+	int generic;                         // 1: force the generic mixed-radix kernels
 };
 
 // ---- launchers (sht_legendre.cu / sht_fft.cu) ----
