@@ -57,6 +57,19 @@ int shtns_b200_stage_times(shtns_cfg, double* ms, long* calls);
  * reference's PolarOptimize does).  Writes mmax+1 ints; returns mmax+1. */
 int shtns_b200_polar_rows(shtns_cfg, int* tm);
 
+/* Exact adjoints (transposes, real inner products with complex numbers
+ * taken as pairs of reals) of the scalar device transforms, used for
+ * reverse-mode differentiation.  cu_SH_to_spat_adjoint maps a spatial
+ * gradient Vg (nspat doubles per field) to the spectral gradient Qg:
+ *   Qg_lm = (2 - delta_m0) nphi sum_theta P_lm(theta) G_m(theta),
+ *   G_m = (1/nphi) sum_phi Vg e^{-i m phi}  (a quadrature-weight-free analysis);
+ * cu_spat_to_SH_adjoint maps a spectral gradient Qg to the spatial gradient
+ * Vg (a synthesis with the quadrature weight of each latitude).  Batched by
+ * shtns_set_batch like the other transforms; ltr as in cu_SH_to_spat.
+ * No counterpart in SHTns 3.5.2. */
+void cu_SH_to_spat_adjoint(shtns_cfg, double *Vg, cplx *Qg, int ltr);
+void cu_spat_to_SH_adjoint(shtns_cfg, cplx *Qg, double *Vg, int ltr);
+
 /* Scalar synthesis (same result as cu_SH_to_spat on device pointers) that
  * allocates no device memory, for callers that cannot call cudaMalloc where
  * they transform.  Its scratch is one static device array of 32 MiB that

@@ -109,6 +109,8 @@ PROTOTYPES = {
     "shtns_b200_stage_times": (I, [CFG, P, P]),
     "shtns_b200_polar_rows": (I, [CFG, P]),
     "cu_SH_to_spat_noalloc": (None, [CFG, P, P, I]),
+    "cu_SH_to_spat_adjoint": (None, [CFG, P, P, I]),
+    "cu_spat_to_SH_adjoint": (None, [CFG, P, P, I]),
 }
 
 _lib = None

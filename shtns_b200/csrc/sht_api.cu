@@ -68,6 +68,7 @@ LegParams leg_params(shtns_cfg s, const Job& j)
 	p.vec_extra = j.vec_extra; p.ncol = j.ncol; p.nfc = j.nfc;
 	p.south_first = s->south_first; p.robert = s->robert;
 	p.mpos_inv = 1.0 / s->mpos_renorm;
+	p.nphi = (double) s->nphi;
 	p.x = s->d_x; p.x2 = s->d_x2; p.sinv = s->d_sinv; p.w = s->d_w; p.c = s->d_c;
 	p.ck = s->d_ck; p.mt = s->mt; p.ckseg = s->ckseg;
 	p.nf = j.nf;
@@ -135,12 +136,16 @@ bool check_launch(const char* what)
 }
 
 // ---- device pipelines ----
+// adjoint = 1 runs the transpose of the analysis (ncomp must be 1): the
+// analysis Ishioka basis in the prologue and the quadrature weights applied
+// to the rows in the Legendre epilogue.
 void run_synth(shtns_cfg s, int ncomp, const int* types, const cplx* Q, const cplx* S, const cplx* T,
-               double* o0, double* o1, double* o2, int ltr)
+               double* o0, double* o1, double* o2, int ltr, int adjoint = 0)
 {
 	Job j;
 	if (!setup_job(s, j, ncomp, types, ltr)) return;
 	PrepParams pp = prep_params(s, j);
+	if (adjoint) pp.xs = s->d_xa;
 	pp.Q = reinterpret_cast<const double2*>(Q);
 	pp.S = reinterpret_cast<const double2*>(S);
 	pp.T = reinterpret_cast<const double2*>(T);
@@ -148,6 +153,7 @@ void run_synth(shtns_cfg s, int ncomp, const int* types, const cplx* Q, const cp
 	launch_prep_synth(pp, s->comp_stream);
 	shtb_stage_end(s);
 	LegParams lp = leg_params(s, j);
+	lp.adjoint = adjoint;
 	shtb_stage_begin(s, 1);
 	launch_leg_synth(lp, s->comp_stream);
 	shtb_stage_end(s);
@@ -160,8 +166,11 @@ void run_synth(shtns_cfg s, int ncomp, const int* types, const cplx* Q, const cp
 	check_launch("synthesis launch");
 }
 
+// adjoint = 1 runs the transpose of the synthesis (ncomp must be 1): no
+// quadrature weights, the factor nphi (2 - delta_m0) and the synthesis
+// Ishioka basis in the epilogue.
 void run_analys(shtns_cfg s, int ncomp, const int* types, const double* i0, const double* i1, const double* i2,
-                cplx* Qo, cplx* So, cplx* To, int ltr)
+                cplx* Qo, cplx* So, cplx* To, int ltr, int adjoint = 0)
 {
 	Job j;
 	if (!setup_job(s, j, ncomp, types, ltr)) return;
@@ -172,12 +181,14 @@ void run_analys(shtns_cfg s, int ncomp, const int* types, const double* i0, cons
 	launch_fft_analys(fp, j.nfc, s->comp_stream);
 	shtb_stage_end(s);
 	LegParams lp = leg_params(s, j);
+	lp.adjoint = adjoint;
 	int kmax_all = 0;
 	for (int im = 0; im <= j.mlim; im++) kmax_all = std::max(kmax_all, (j.llim + j.vec_extra - im * s->mres) / 2 + 1);
 	shtb_stage_begin(s, 4);
 	launch_leg_analys(lp, kmax_all, s->comp_stream);
 	shtb_stage_end(s);
 	PrepParams pp = prep_params(s, j);
+	if (adjoint) pp.xa = s->d_xs;
 	pp.Qo = reinterpret_cast<double2*>(Qo);
 	pp.So = reinterpret_cast<double2*>(So);
 	pp.To = reinterpret_cast<double2*>(To);
@@ -287,12 +298,62 @@ extern "C" void cu_SHqst_to_spat(shtns_cfg s, cplx* Qlm, cplx* Slm, cplx* Tlm, d
 extern "C" void cu_spat_to_SHqst(shtns_cfg s, double* Vr, double* Vt, double* Vp, cplx* Qlm, cplx* Slm, cplx* Tlm, int ltr)
 { run_analys(s, 3, T_QST, Vr, Vt, Vp, Qlm, Slm, Tlm, ltr); }
 
-// Single-precision device transforms (shtns_cuda.h:410,414) are not provided:
-// the FP64 path is the product; these report an error instead of computing.
-extern "C" void cu_SH_to_spat_float(shtns_cfg, cplx_f*, float*, int)
-{ shtb_set_error(1, "cu_SH_to_spat_float is not provided by shtns_b200"); }
-extern "C" void cu_spat_to_SH_float(shtns_cfg, float*, cplx_f*, int)
-{ shtb_set_error(1, "cu_spat_to_SH_float is not provided by shtns_b200"); }
+// ---- adjoints (shtns_b200.h) ----
+extern "C" void cu_SH_to_spat_adjoint(shtns_cfg s, double* Vg, cplx* Qg, int ltr)
+{ run_analys(s, 1, T_SCAL, Vg, nullptr, nullptr, Qg, nullptr, nullptr, ltr, 1); }
+
+extern "C" void cu_spat_to_SH_adjoint(shtns_cfg s, cplx* Qg, double* Vg, int ltr)
+{ run_synth(s, 1, T_SCAL, Qg, nullptr, nullptr, Vg, nullptr, nullptr, ltr, 1); }
+
+// Single-precision device transforms (shtns_cuda.h:410,414): FP32 arrays in
+// and out, converted to FP64 in the plan's staging buffer, transformed in FP64
+// and rounded back to FP32 (the reference computes these in FP32).
+namespace {
+__global__ void f2d_kernel(const float* __restrict__ in, double* __restrict__ out, long n)
+{
+	for (long i = blockIdx.x * (long) blockDim.x + threadIdx.x; i < n; i += (long) gridDim.x * blockDim.x) out[i] = in[i];
+}
+__global__ void d2f_kernel(const double* __restrict__ in, float* __restrict__ out, long n)
+{
+	for (long i = blockIdx.x * (long) blockDim.x + threadIdx.x; i < n; i += (long) gridDim.x * blockDim.x) out[i] = (float) in[i];
+}
+void convert(const float* in, double* out, long n, cudaStream_t st)
+{
+	f2d_kernel<<<(unsigned) std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(in, out, n);
+	shtb_count_launch();
+}
+void convert(const double* in, float* out, long n, cudaStream_t st)
+{
+	d2f_kernel<<<(unsigned) std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(in, out, n);
+	shtb_count_launch();
+}
+} // namespace
+
+extern "C" void cu_SH_to_spat_float(shtns_cfg s, cplx_f* Qlm, float* Vr, int ltr)
+{
+	if (!s || !s->grid_set) { shtb_set_error(1, "transform on a plan without grid"); return; }
+	Stage st;
+	if (!stage_alloc(s, 1, 1, st)) return;
+	const long nspec = 2 * ((long)(s->batch - 1) * s->spec_dist + s->nlm);
+	const long nsp = (long)(s->batch - 1) * s->spat_dist + s->nspat;
+	convert(reinterpret_cast<const float*>(Qlm), reinterpret_cast<double*>(st.spec[0]), nspec, s->comp_stream);
+	run_synth(s, 1, T_SCAL, reinterpret_cast<cplx*>(st.spec[0]), nullptr, nullptr, st.spat[0], nullptr, nullptr, ltr);
+	convert(st.spat[0], Vr, nsp, s->comp_stream);
+	shtb_cuda_ok(cudaGetLastError(), "cu_SH_to_spat_float");
+}
+
+extern "C" void cu_spat_to_SH_float(shtns_cfg s, float* Vr, cplx_f* Qlm, int ltr)
+{
+	if (!s || !s->grid_set) { shtb_set_error(1, "transform on a plan without grid"); return; }
+	Stage st;
+	if (!stage_alloc(s, 1, 1, st)) return;
+	const long nspec = 2 * ((long)(s->batch - 1) * s->spec_dist + s->nlm);
+	const long nsp = (long)(s->batch - 1) * s->spat_dist + s->nspat;
+	convert(Vr, st.spat[0], nsp, s->comp_stream);
+	run_analys(s, 1, T_SCAL, st.spat[0], nullptr, nullptr, reinterpret_cast<cplx*>(st.spec[0]), nullptr, nullptr, ltr);
+	convert(reinterpret_cast<const double*>(st.spec[0]), reinterpret_cast<float*>(Qlm), nspec, s->comp_stream);
+	shtb_cuda_ok(cudaGetLastError(), "cu_spat_to_SH_float");
+}
 
 // ---- host-pointer API (shtns.h) ----
 extern "C" void SH_to_spat(shtns_cfg s, cplx* Qlm, double* Vr) { h_synth(s, 1, T_SCAL, Qlm, nullptr, nullptr, Vr, nullptr, nullptr, s ? s->lmax : 0); }

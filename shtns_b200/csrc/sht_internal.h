@@ -113,6 +113,8 @@ struct LegParams {
 	int ckseg;                           // checkpoint spacing in k (8, 16 or 32)
 	int south_first, robert;
 	double mpos_inv;                     // analysis factor for m>0 (1/mpos_renorm)
+	int adjoint;                         // 1: adjoint transforms (see sht_api.cu)
+	double nphi;                         // longitudes (adjoint scalings)
 	const double *x, *x2, *sinv, *w, *c;
 	const double2 *ck;
 	MTables mt;

@@ -365,6 +365,11 @@ leg_synth_kernel(LegParams p)
 		double sr = fma(-cx, acc[i][1][0], acc[i][0][0]), si = fma(-cx, acc[i][1][1], acc[i][0][1]);
 		if (t < tmm) { nr = ni = sr = si = 0.0; }
 		if (vec) { const double s = p.sinv[t]; nr *= s; ni *= s; sr *= s; si *= s; }
+		if (p.adjoint) {
+			// adjoint of the analysis: row weight W_t(m) / (nphi (2 - delta_m0))
+			const double s = p.w[t] * (m > 0 ? p.mpos_inv : 1.0) / (p.nphi * (m > 0 ? 2.0 : 1.0));
+			nr *= s; ni *= s; sr *= s; si *= s;
+		}
 		const int rn = p.south_first ? p.nlat - 1 - t : t;
 		const int rs = p.nlat - 1 - rn;
 		Ff[rn] = make_double2(nr, ni);
@@ -465,7 +470,8 @@ leg_analys_kernel(LegParams p, int nkb)
 			const int t = tt0 + tt, fc = fc0 + fl;
 			double er = 0.0, ei = 0.0, orr = 0.0, oi = 0.0;
 			if (t < p.nlat_2 && fc < p.nfc) {
-				double w = p.w[t] * wfac;
+				// adjoint of the synthesis: no quadrature weight, factor nphi (2 - delta_m0)
+				double w = p.adjoint ? p.nphi * (m > 0 ? 2.0 : 1.0) : p.w[t] * wfac;
 				if (p.ctype[fc / p.nf] != 0) {
 					double s = p.sinv[t];
 					if (p.robert) s *= s;

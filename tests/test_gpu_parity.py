@@ -221,3 +221,25 @@ def test_lmax511_64_fields_round_trip():
     for a, b in ((q, Q), (s, S), (t, T)):
         assert relerr(a.cpu().numpy(), b.cpu().numpy()) < TOL
     assert shtns_b200.capi.load().shtns_b200_status() == 0
+
+
+def test_float_device_transforms():
+    """cu_SH_to_spat_float / cu_spat_to_SH_float (FP32 arrays, FP64 inside)."""
+    import ctypes as C
+    from shtns_b200 import capi
+    lib = capi.load()
+    sh = _plan((127, 127, 1, 192, 384, 0, 256))
+    dev = torch.device("cuda:0")
+    q64 = torch.from_numpy(rand_spec(127, 127, 1, 61)).to(dev)
+    v64 = sh.synth(q64)
+    q32 = q64.to(torch.complex64)
+    v32 = torch.empty(sh.spat_shape, dtype=torch.float32, device=dev)
+    sh._batch(1)
+    sh._stream()
+    lib.cu_SH_to_spat_float(sh._cfg, C.c_void_p(q32.data_ptr()), C.c_void_p(v32.data_ptr()), 127)
+    back = torch.empty(sh.nlm, dtype=torch.complex64, device=dev)
+    lib.cu_spat_to_SH_float(sh._cfg, C.c_void_p(v32.data_ptr()), C.c_void_p(back.data_ptr()), 127)
+    torch.cuda.synchronize()
+    assert lib.shtns_b200_status() == 0
+    assert relerr(v64.cpu().numpy(), v32.double().cpu().numpy()) < 1e-6
+    assert relerr(q64.cpu().numpy(), back.to(torch.complex128).cpu().numpy()) < 1e-6
