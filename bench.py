@@ -381,6 +381,105 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- uneven lmax
+UNEVEN_LMAX = (63, 127, 255, 511, 1023)
+UNEVEN_UNIT = "fields/s (SH_to_spat+spat_to_SH of one scalar field on its own grid)"
+
+
+def uneven_lmaxs(n, seed):
+    return np.random.default_rng(seed).choice(UNEVEN_LMAX, size=n)
+
+
+def uneven_flops(batch):
+    """Legendre multiply-adds x2 of one synthesis + one analysis of every field
+    (per order m, kept north row and Ishioka step: 4 FMAs per field)."""
+    from shtns_b200 import capi
+    lib = capi.load()
+    tot = 0.0
+    for sh, nf in zip(batch.plans, batch.count):
+        tm = np.zeros(sh.mmax + 1, dtype=np.int32)
+        lib.shtns_b200_polar_rows(sh._cfg, tm.ctypes.data_as(C.c_void_p))
+        rows = sh.nlat // 2 - tm
+        ks = (sh.lmax - np.arange(sh.mmax + 1)) // 2 + 1
+        tot += 8.0 * float((rows * ks).sum()) * nf
+    return 2 * tot
+
+
+def run_uneven(args):
+    """256 scalar fields, lmax uniform in {63,...,1023}, each on its own Gauss
+    grid nlat=3(lmax+1)/2, nphi=2 nlat: one step = synthesis + analysis of all
+    fields.  Forms timed: one cu_* pair per field, one batched pair per lmax
+    bucket, the plan group (one persistent Legendre launch per direction)
+    eagerly, and the plan group replayed from a CUDA graph (the value)."""
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    from shtns_b200 import batch as B
+    from tests.common import rand_spec
+    nf = args.fields if args.fields != NFIELDS else 256
+    lm = uneven_lmaxs(nf, 2024)
+    ub = B.UnevenBatch(lm, device=dev, polar_opt=EPS)
+    for b, (l, n) in enumerate(zip(ub.buckets, ub.count)):
+        ub.Q[b].copy_(torch.from_numpy(rand_spec(l, l, 1, 300 + b, power=1.0, nfields=n)))
+    tune = B.autotune(ub, use_cache=False)
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    from shtns_b200 import capi
+    lib = capi.load()
+    ms_field = timed(ub.pair_per_field, max(3, args.steps // 20))
+    ms_bucket = timed(ub.pair_per_bucket, args.steps)
+    ms_group = timed(ub.pair, args.steps)
+    ub.capture()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    ms_graph = timed(ub.replay, args.steps)
+    clk = clocks.stop()
+    n0 = lib.shtns_b200_launch_count()
+    ub.pair()
+    torch.cuda.synchronize()
+    launches_pair = lib.shtns_b200_launch_count() - n0
+    rt = max(float((q - r).abs().max() / q.abs().max()) for q, r in zip(ub.Q, ub.R))
+    flops = uneven_flops(ub)
+    peak = fp64_gemm_peak(torch, dev)
+    ach = flops / (ms_graph * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": nf / (ms_graph * 1e-3), "unit": UNEVEN_UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_graph, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1)/(l+1))",
+        "config": {"workload": "uneven_lmax_256fields", "fields": nf,
+                   "fields_per_lmax": dict(zip(map(str, ub.buckets), ub.count)),
+                   "grids": {str(l): list(B.grid_for(l)) for l in ub.buckets}, "polar_eps": EPS,
+                   "layout": "theta-contiguous", "form": "plan group replayed from a CUDA graph"},
+        "forms_fields_per_s": {"per_field_launches": nf / (ms_field * 1e-3),
+                               "per_bucket_batched": nf / (ms_bucket * 1e-3),
+                               "group_eager": nf / (ms_group * 1e-3),
+                               "group_cuda_graph": nf / (ms_graph * 1e-3)},
+        "speedup_vs_per_field": ms_field / ms_graph,
+        "autotune": tune["options"],
+        "roofline": {"kernel": "whole step (Legendre flops / step time: lower bound for leg_multi_kernel)",
+                     "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                     "traffic": None, "peak_source": "measured in this run: cuBLAS DGEMM 8192^3"},
+        "roundtrip_relerr": rt,
+        "gpu_launches": int(launches_pair),    # per step; the graph replays the same kernels
+        "clocks": clk,
+    }
+    ub.release_graph()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -390,8 +489,13 @@ def main():
     ap.add_argument("--fields", type=int, default=NFIELDS)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="qst", choices=["qst", "uneven"],
+                    help="qst: lmax=511 vector transforms of 64 fields (default); "
+                         "uneven: 256 scalar fields of lmax 63..1023 through a plan group")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.workload == "uneven" and args.impl != "reference":
+        run_uneven(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

@@ -70,6 +70,33 @@ int shtns_b200_polar_rows(shtns_cfg, int* tm);
 void cu_SH_to_spat_adjoint(shtns_cfg, double *Vg, cplx *Qg, int ltr);
 void cu_spat_to_SH_adjoint(shtns_cfg, cplx *Qg, double *Vg, int ltr);
 
+/* Tuning options of a plan.  option 1: latitude pairs per FFT CTA (1, 2, 4;
+ * 0 = automatic); option 2: recurrence checkpoint spacing (8, 16, 32; rebuilds
+ * the checkpoint table; not for clones or plans that have clones); option 3:
+ * 1 = always use the generic mixed-radix FFT kernels.  Return 0 or -1.
+ * No counterpart in SHTns 3.5.2. */
+int shtns_b200_set_option(shtns_cfg, int option, int value);
+int shtns_b200_get_option(shtns_cfg, int option);
+
+/* Plan groups: scalar transforms of fields of different lmax, each on the grid
+ * of its own plan, with the Legendre stage of all plans in one persistent
+ * launch whose CTAs take work items (plan, order, tile) from a queue in
+ * decreasing cost order.  Qlm[i] / Vr[i] hold nfields[i] contiguous fields of
+ * plan i (device pointers; spec_dist = nlm, spat_dist = nspat of that plan).
+ * All launches go to the compute stream of the first plan, so a call can be
+ * captured in a CUDA graph (after one call with the same field counts, which
+ * allocates the work buffers and the work list).  Plans in a group get a
+ * common checkpoint spacing.  No counterpart in SHTns 3.5.2. */
+typedef struct shtns_b200_group* shtns_group;
+shtns_group shtns_b200_group_create(int nplans, shtns_cfg* plans);
+void shtns_b200_group_destroy(shtns_group);
+/* option 1: work order, 0 by decreasing cost (default), 1 plan/order/tile;
+ * option 2: CTAs of the persistent launch per SM, 1-3 (0: 3);
+ * option 3: checkpoint spacing of all plans, 8, 16 or 32.  Return 0 or -1. */
+int shtns_b200_group_set_option(shtns_group, int option, int value);
+void shtns_b200_group_synth(shtns_group, cplx **Qlm, double **Vr, const int *nfields, int ltr);
+void shtns_b200_group_analys(shtns_group, double **Vr, cplx **Qlm, const int *nfields, int ltr);
+
 /* Scalar synthesis (same result as cu_SH_to_spat on device pointers) that
  * allocates no device memory, for callers that cannot call cudaMalloc where
  * they transform.  Its scratch is one static device array of 32 MiB that

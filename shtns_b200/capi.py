@@ -111,6 +111,13 @@ PROTOTYPES = {
     "cu_SH_to_spat_noalloc": (None, [CFG, P, P, I]),
     "cu_SH_to_spat_adjoint": (None, [CFG, P, P, I]),
     "cu_spat_to_SH_adjoint": (None, [CFG, P, P, I]),
+    "shtns_b200_set_option": (I, [CFG, I, I]),
+    "shtns_b200_get_option": (I, [CFG, I]),
+    "shtns_b200_group_create": (P, [I, P]),
+    "shtns_b200_group_destroy": (None, [P]),
+    "shtns_b200_group_set_option": (I, [P, I, I]),
+    "shtns_b200_group_synth": (None, [P, P, P, P, I]),
+    "shtns_b200_group_analys": (None, [P, P, P, P, I]),
 }
 
 _lib = None

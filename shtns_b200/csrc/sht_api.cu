@@ -110,9 +110,10 @@ FftParams fft_params(shtns_cfg s, const Job& j)
 	// overrides (tuning knob, clamped to what fits in 227 KB).
 	int S = 4;
 	while (S > 1 && fft_smem_bytes(s->nphi, S) > 112 * 1024) S /= 2;
-	if (const char* e = getenv("SHTNS_B200_FFT_PAIRS")) {
-		int v = atoi(e);
-		if (v == 1 || v == 2 || v == 4) S = v;
+	int want = s->fft_pairs;
+	if (const char* e = getenv("SHTNS_B200_FFT_PAIRS")) want = atoi(e);
+	if (want == 1 || want == 2 || want == 4) {
+		S = want;
 		while (S > 1 && fft_smem_bytes(s->nphi, S) > 227 * 1024) S /= 2;
 	}
 	while (S > 1 && 2 * S > (int) s->nlat) S /= 2;
@@ -121,6 +122,7 @@ FftParams fft_params(shtns_cfg s, const Job& j)
 	p.fstride = (long)(s->mmax + 1) * s->nlat;
 	p.nf = j.nf; p.spat_dist = s->spat_dist;
 	p.phi_contiguous = s->phi_contiguous;
+	p.generic = s->fft_generic;
 	return p;
 }
 
@@ -386,3 +388,256 @@ extern "C" void spat_to_SHqst(shtns_cfg s, double* Vr, double* Vt, double* Vp, c
 { h_analys(s, 3, T_QST, Vr, Vt, Vp, Qlm, Slm, Tlm, s ? s->lmax : 0); }
 extern "C" void spat_to_SHqst_l(shtns_cfg s, double* Vr, double* Vt, double* Vp, cplx* Qlm, cplx* Slm, cplx* Tlm, int ltr)
 { h_analys(s, 3, T_QST, Vr, Vt, Vp, Qlm, Slm, Tlm, ltr); }
+
+// ---------------------------------------------------------------------------
+// Plan groups: scalar transforms of several plans (fields of different lmax,
+// each on its own grid) where the Legendre stage of all plans is one
+// persistent launch.  The per-plan prologue, FFT and epilogue launches and
+// the persistent launch all go to the stream of the first plan, so the whole
+// group is one stream sequence that a CUDA graph can capture.
+// Work list of one direction (synthesis or analysis): per-plan parameters and
+// (plan, order, tile, column tile) items, in pinned host memory and on the
+// device.  The host copies are rewritten only after the stream has drained,
+// so an upload still in flight never reads a half-written list, and each
+// direction keeps its own buffers, so a captured graph holds both uploads
+// (if any) with the right contents.
+struct GroupWork {
+	std::vector<int> key;            // field counts + ltr + order of the cached list
+	LegParams* h_plist = nullptr; LegParams* d_plist = nullptr; int plist_cap = 0;
+	int4* h_work = nullptr; int4* d_work = nullptr; int work_cap = 0; int nwork = 0;
+	int* d_counter = nullptr;
+	void release()
+	{
+		if (h_plist) cudaFreeHost(h_plist);
+		if (d_plist) cudaFree(d_plist);
+		if (h_work) cudaFreeHost(h_work);
+		if (d_work) cudaFree(d_work);
+		if (d_counter) cudaFree(d_counter);
+		*this = GroupWork();
+	}
+};
+
+struct shtns_b200_group {
+	std::vector<shtns_cfg> plans;
+	int ckseg;
+	int order;                       // 0: work items by decreasing cost, 1: plan/order/tile order
+	int nsm;
+	int ctas_per_sm;                 // CTAs of the persistent launch per SM (1-3)
+	GroupWork dir[2];                // [0] analysis, [1] synthesis
+};
+
+namespace {
+
+bool group_ok(shtns_group g)
+{
+	if (!g || g->plans.empty()) { shtb_set_error(1, "empty plan group"); return false; }
+	return true;
+}
+
+// A list must change: refuse under stream capture (the host buffers would be
+// read at replay time), else drain the stream so that no copy or kernel still
+// uses the old list.
+bool group_may_rewrite(cudaStream_t st)
+{
+	cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+	cudaStreamIsCapturing(st, &cs);
+	if (cs != cudaStreamCaptureStatusNone) {
+		shtb_set_error(1, "plan group: work list changed during stream capture "
+		                  "(make one call with the same field counts before capturing)");
+		return false;
+	}
+	return shtb_cuda_ok(cudaStreamSynchronize(st), "plan group stream");
+}
+
+// build (or reuse) the work list of the persistent Legendre launch
+bool group_work(shtns_group g, const std::vector<LegParams>& lp, const int* nfields, bool synth)
+{
+	GroupWork& W = g->dir[synth ? 1 : 0];
+	cudaStream_t st = g->plans[0]->comp_stream;
+	const int np = (int) g->plans.size();
+	std::vector<int> key;
+	for (int i = 0; i < np; i++) { key.push_back(nfields[i]); key.push_back(lp[i].llim); }
+	key.push_back(g->order);
+	bool params_changed = W.plist_cap < np;
+	for (int i = 0; i < np && !params_changed; i++)
+		params_changed = memcmp(&W.h_plist[i], &lp[i], sizeof(LegParams)) != 0;
+	const bool list_changed = key != W.key;
+	if (!params_changed && !list_changed) return true;
+	if (!group_may_rewrite(st)) return false;
+	if (W.plist_cap < np) {
+		if (W.h_plist) cudaFreeHost(W.h_plist);
+		if (W.d_plist) cudaFree(W.d_plist);
+		W.h_plist = nullptr; W.d_plist = nullptr; W.plist_cap = 0;
+		if (cudaMallocHost(&W.h_plist, sizeof(LegParams) * np) != cudaSuccess ||
+		    cudaMalloc(&W.d_plist, sizeof(LegParams) * np) != cudaSuccess) {
+			cudaGetLastError(); shtb_set_error(3, "out of memory for plan group"); return false;
+		}
+		W.plist_cap = np;
+	}
+	if (!W.d_counter && cudaMalloc(&W.d_counter, sizeof(int)) != cudaSuccess) {
+		cudaGetLastError(); shtb_set_error(3, "out of memory for plan group"); return false;
+	}
+	if (params_changed) {
+		for (int i = 0; i < np; i++) W.h_plist[i] = lp[i];
+		cudaMemcpyAsync(W.d_plist, W.h_plist, sizeof(LegParams) * np, cudaMemcpyHostToDevice, st);
+	}
+	if (!list_changed) return true;
+	struct Item { int4 w; double cost; };
+	std::vector<Item> items;
+	for (int i = 0; i < np; i++) {
+		if (nfields[i] <= 0) continue;
+		const shtns_cfg s = g->plans[i];
+		const LegParams& p = lp[i];
+		const int nnb = (p.ncol + LG_BN - 1) / LG_BN;
+		for (int im = 0; im <= p.mlim; im++) {
+			const int m = im * s->mres;
+			const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
+			const int tm = s->tm_h[im];
+			if (synth) {
+				const int ntb = (s->nlat_2 + LG_BM - 1) / LG_BM;
+				for (int tb = 0; tb < ntb; tb++) {
+					const bool live = tb * LG_BM + LG_BM > tm;
+					const double cost = live ? (double) nk * LG_BM : 1.0;
+					for (int nb = 0; nb < nnb; nb++) items.push_back({make_int4(i, im, tb, nb), cost});
+				}
+			} else {
+				const int nkb = (nk + LG_BM - 1) / LG_BM;
+				for (int kb = 0; kb < nkb; kb++) {
+					const double cost = (double) (s->nlat_2 - (tm / LG_BK) * LG_BK) * std::min(LG_BM, nk - kb * LG_BM);
+					for (int nb = 0; nb < nnb; nb++) items.push_back({make_int4(i, im, kb, nb), cost});
+				}
+			}
+		}
+	}
+	if (g->order == 0)
+		std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.cost > b.cost; });
+	const int n = (int) items.size();
+	if (W.work_cap < std::max(n, 1)) {
+		if (W.h_work) cudaFreeHost(W.h_work);
+		if (W.d_work) cudaFree(W.d_work);
+		W.h_work = nullptr; W.d_work = nullptr; W.work_cap = 0;
+		if (cudaMallocHost(&W.h_work, sizeof(int4) * std::max(n, 1)) != cudaSuccess ||
+		    cudaMalloc(&W.d_work, sizeof(int4) * std::max(n, 1)) != cudaSuccess) {
+			cudaGetLastError(); shtb_set_error(3, "out of memory for plan group"); W.key.clear(); return false;
+		}
+		W.work_cap = std::max(n, 1);
+	}
+	for (int i = 0; i < n; i++) W.h_work[i] = items[i].w;
+	if (n > 0) cudaMemcpyAsync(W.d_work, W.h_work, sizeof(int4) * n, cudaMemcpyHostToDevice, st);
+	W.nwork = n;
+	W.key = key;
+	return true;
+}
+
+} // namespace
+
+extern "C" shtns_group shtns_b200_group_create(int nplans, shtns_cfg* plans)
+{
+	if (nplans < 1 || !plans) { shtb_set_error(1, "shtns_b200_group_create: no plans"); return nullptr; }
+	int seg = plans[0] ? plans[0]->ckseg : 0;
+	for (int i = 0; i < nplans; i++) {
+		if (!plans[i] || !plans[i]->grid_set) { shtb_set_error(1, "shtns_b200_group_create: plan without grid"); return nullptr; }
+		if (plans[i]->dev != plans[0]->dev) { shtb_set_error(1, "shtns_b200_group_create: plans on different devices"); return nullptr; }
+		seg = std::max(seg, plans[i]->ckseg);
+	}
+	// one persistent kernel instance serves all plans: same checkpoint spacing
+	for (int i = 0; i < nplans; i++)
+		if (plans[i]->ckseg != seg && shtns_b200_set_option(plans[i], 2, seg) != 0) {
+			shtb_set_error(1, "shtns_b200_group_create: cannot align checkpoint spacing");
+			return nullptr;
+		}
+	shtns_group g = new shtns_b200_group();
+	g->plans.assign(plans, plans + nplans);
+	g->ckseg = seg;
+	g->order = 0;
+	g->ctas_per_sm = 3;
+	cudaDeviceGetAttribute(&g->nsm, cudaDevAttrMultiProcessorCount, plans[0]->dev);
+	return g;
+}
+
+extern "C" void shtns_b200_group_destroy(shtns_group g)
+{
+	if (!g) return;
+	if (!g->plans.empty()) cudaStreamSynchronize(g->plans[0]->comp_stream);
+	g->dir[0].release();
+	g->dir[1].release();
+	delete g;
+}
+
+extern "C" int shtns_b200_group_set_option(shtns_group g, int option, int value)
+{
+	if (!g) return -1;
+	if (option == 1 && (value == 0 || value == 1)) { g->order = value; return 0; }
+	if (option == 2 && value >= 0 && value <= 3) { g->ctas_per_sm = value ? value : 3; return 0; }
+	if (option == 3 && (value == 8 || value == 16 || value == 32)) {
+		for (shtns_cfg s : g->plans)
+			if (s->ckseg != value && shtns_b200_set_option(s, 2, value) != 0) return -1;
+		g->ckseg = value;
+		return 0;
+	}
+	return -1;
+}
+
+extern "C" void shtns_b200_group_synth(shtns_group g, cplx** Qlm, double** Vr, const int* nfields, int ltr)
+{
+	if (!group_ok(g)) return;
+	const int np = (int) g->plans.size();
+	cudaStream_t st = g->plans[0]->comp_stream;
+	std::vector<Job> jobs(np);
+	std::vector<LegParams> lp(np);
+	for (int i = 0; i < np; i++) {
+		shtns_cfg s = g->plans[i];
+		shtns_set_batch(s, std::max(1, nfields[i]), s->nlm, s->nspat);
+		if (!setup_job(s, jobs[i], 1, T_SCAL, std::min<int>(ltr, s->lmax))) return;
+		lp[i] = leg_params(s, jobs[i]);
+	}
+	if (!group_work(g, lp, nfields, true)) return;
+	for (int i = 0; i < np; i++) {
+		if (nfields[i] <= 0) continue;
+		PrepParams pp = prep_params(g->plans[i], jobs[i]);
+		pp.Q = reinterpret_cast<const double2*>(Qlm[i]);
+		launch_prep_synth(pp, st);
+	}
+	const GroupWork& W = g->dir[1];
+	launch_leg_multi(W.d_plist, W.d_work, W.nwork, W.d_counter, g->ckseg, true, g->nsm * g->ctas_per_sm, st);
+	for (int i = 0; i < np; i++) {
+		if (nfields[i] <= 0) continue;
+		FftParams fp = fft_params(g->plans[i], jobs[i]);
+		fp.spat[0] = Vr[i];
+		fp.vec2 = aligned16(Vr[i], Vr[i], Vr[i], g->plans[i]->spat_dist);
+		launch_fft_synth(fp, jobs[i].nfc, st);
+	}
+	check_launch("group synthesis launch");
+}
+
+extern "C" void shtns_b200_group_analys(shtns_group g, double** Vr, cplx** Qlm, const int* nfields, int ltr)
+{
+	if (!group_ok(g)) return;
+	const int np = (int) g->plans.size();
+	cudaStream_t st = g->plans[0]->comp_stream;
+	std::vector<Job> jobs(np);
+	std::vector<LegParams> lp(np);
+	for (int i = 0; i < np; i++) {
+		shtns_cfg s = g->plans[i];
+		shtns_set_batch(s, std::max(1, nfields[i]), s->nlm, s->nspat);
+		if (!setup_job(s, jobs[i], 1, T_SCAL, std::min<int>(ltr, s->lmax))) return;
+		lp[i] = leg_params(s, jobs[i]);
+	}
+	if (!group_work(g, lp, nfields, false)) return;
+	for (int i = 0; i < np; i++) {
+		if (nfields[i] <= 0) continue;
+		FftParams fp = fft_params(g->plans[i], jobs[i]);
+		fp.spat_in[0] = Vr[i];
+		fp.vec2 = aligned16(Vr[i], Vr[i], Vr[i], g->plans[i]->spat_dist);
+		launch_fft_analys(fp, jobs[i].nfc, st);
+	}
+	const GroupWork& W = g->dir[0];
+	launch_leg_multi(W.d_plist, W.d_work, W.nwork, W.d_counter, g->ckseg, false, g->nsm * g->ctas_per_sm, st);
+	for (int i = 0; i < np; i++) {
+		if (nfields[i] <= 0) continue;
+		PrepParams pp = prep_params(g->plans[i], jobs[i]);
+		pp.Qo = reinterpret_cast<double2*>(Qlm[i]);
+		launch_post_analys_m(pp, g->plans[i]->mmax, st);
+	}
+	check_launch("group analysis launch");
+}

@@ -76,6 +76,8 @@ struct shtns_info {
 	std::vector<int> koff_h, coff_h, xoff_h, voff_h, ckoff_h, tm_h, kmax_h;
 	long ktot, ctot, xtot, vtot, segtot;
 	int ckseg;                           // checkpoint spacing in k
+	int fft_pairs;                       // latitude pairs per FFT CTA (0: automatic)
+	int fft_generic;                     // 1: always use the generic mixed-radix FFT kernels
 	std::vector<int> fft_radix;          // factorisation of nphi
 	double Y00_1, Y10_ct, Y11_st;
 	// device tables
@@ -156,6 +158,8 @@ void launch_prep_synth(const PrepParams& p, cudaStream_t st);
 void launch_post_analys_m(const PrepParams& p, int mmax, cudaStream_t st);
 void launch_leg_synth(const LegParams& p, cudaStream_t st);
 void launch_leg_analys(const LegParams& p, int kmax_all, cudaStream_t st);
+void launch_leg_multi(const LegParams* d_plist, const int4* d_work, int nwork, int* d_counter, int ckseg, bool synth,
+                      int nctas, cudaStream_t st);
 int fft_threads(int N, int S, unsigned long long rcode, int nradix);
 size_t fft_smem_bytes(int N, int S);
 void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st);
@@ -168,3 +172,4 @@ bool shtb_cuda_ok(cudaError_t e, const char* where);
 void shtb_stage_begin(shtns_cfg s, int stage);
 void shtb_stage_end(shtns_cfg s);
 void shtb_timing_release(shtns_cfg s);
+extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value);

@@ -17,6 +17,8 @@
 // start at any k and the recurrence of one tile is only 32 dependent steps.
 #include "sht_internal.h"
 
+#include <algorithm>
+
 namespace {
 
 __device__ __forceinline__ void dmma(double (&c)[2], double a, double b)
@@ -264,15 +266,11 @@ __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 #define SA_LD 68   // shared row stride in doubles: 4 mod 16 keeps fragment loads conflict-free
 
 template <int SEG>
-__global__ void __launch_bounds__(LG_THREADS, 3)
-leg_synth_kernel(LegParams p)
+__device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int tb, int nb)
 {
 	__shared__ __align__(16) double As[LG_BK][SA_LD];   // [k][theta]
 	__shared__ __align__(16) double Bs[LG_BK][SA_LD];   // [k][col]
-	const int im = blockIdx.y;
 	const int m = im * p.mres;
-	const int ntb = (p.nlat_2 + LG_BM - 1) / LG_BM;
-	const int tb = blockIdx.x % ntb, nb = blockIdx.x / ntb;
 	const int t0 = tb * LG_BM, c0 = nb * LG_BN;
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	const int wm = warp >> 2, wn = warp & 3;
@@ -386,14 +384,11 @@ leg_synth_kernel(LegParams p)
 #define AA_LD 36   // As row stride (k rows x 32 theta): 4 mod 16
 
 template <int SEG>
-__global__ void __launch_bounds__(LG_THREADS, 3)
-leg_analys_kernel(LegParams p, int nkb)
+__device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int kb, int nb)
 {
 	__shared__ __align__(16) double As[LG_BM][AA_LD];   // [k][theta]
 	__shared__ __align__(16) double Bs[LG_BK][SA_LD];   // [theta][col]
-	const int im = blockIdx.y;
 	const int m = im * p.mres;
-	const int kb = blockIdx.x % nkb, nb = blockIdx.x / nkb;
 	const int k0 = kb * LG_BM, c0 = nb * LG_BN;
 	const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
 	if (k0 >= nk) return;
@@ -516,6 +511,40 @@ leg_analys_kernel(LegParams p, int nkb)
 	}
 }
 
+// Single-plan kernels: blockIdx.y = order, blockIdx.x = (row tile, column tile).
+template <int SEG>
+__global__ void __launch_bounds__(LG_THREADS, 3) leg_synth_kernel(LegParams p)
+{
+	const int ntb = (p.nlat_2 + LG_BM - 1) / LG_BM;
+	leg_synth_tile<SEG>(p, blockIdx.y, blockIdx.x % ntb, blockIdx.x / ntb);
+}
+
+template <int SEG>
+__global__ void __launch_bounds__(LG_THREADS, 3) leg_analys_kernel(LegParams p, int nkb)
+{
+	leg_analys_tile<SEG>(p, blockIdx.y, blockIdx.x % nkb, blockIdx.x / nkb);
+}
+
+// Persistent multi-plan kernels: CTAs (one wave) take work items (plan,
+// order, row or k tile, column tile) from a queue in decreasing cost order,
+// so plans of different lmax share one launch and balance over the SMs.
+template <int SEG, bool SYNTH>
+__global__ void __launch_bounds__(LG_THREADS, 3)
+leg_multi_kernel(const LegParams* __restrict__ plist, const int4* __restrict__ work, int nwork, int* __restrict__ counter)
+{
+	__shared__ int wi;
+	for (;;) {
+		if (threadIdx.x == 0) wi = atomicAdd(counter, 1);
+		__syncthreads();
+		const int w = wi;
+		__syncthreads();
+		if (w >= nwork) break;
+		const int4 it = work[w];
+		if (SYNTH) leg_synth_tile<SEG>(plist[it.x], it.y, it.z, it.w);
+		else leg_analys_tile<SEG>(plist[it.x], it.y, it.z, it.w);
+	}
+}
+
 } // namespace
 
 // ---------------------------------------------------------------------------
@@ -575,5 +604,27 @@ void launch_post_analys_m(const PrepParams& p, int mmax, cudaStream_t st)
 	const int nft = (p.nf + PE_F - 1) / PE_F;
 	dim3 grid((p.lmax + 1 + PE_J - 1) / PE_J, nft * ngroups, mmax + 1);
 	post_analys_kernel<<<grid, 256, 0, st>>>(p);
+	shtb_count_launch();
+}
+
+void launch_leg_multi(const LegParams* d_plist, const int4* d_work, int nwork, int* d_counter, int ckseg, bool synth,
+                      int nctas, cudaStream_t st)
+{
+	const int grid = std::max(1, std::min(nwork, nctas));
+	cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+	switch (ckseg) {
+		case 8:
+			if (synth) leg_multi_kernel<8, true><<<grid, LG_THREADS, 0, st>>>(d_plist, d_work, nwork, d_counter);
+			else leg_multi_kernel<8, false><<<grid, LG_THREADS, 0, st>>>(d_plist, d_work, nwork, d_counter);
+			break;
+		case 16:
+			if (synth) leg_multi_kernel<16, true><<<grid, LG_THREADS, 0, st>>>(d_plist, d_work, nwork, d_counter);
+			else leg_multi_kernel<16, false><<<grid, LG_THREADS, 0, st>>>(d_plist, d_work, nwork, d_counter);
+			break;
+		default:
+			if (synth) leg_multi_kernel<32, true><<<grid, LG_THREADS, 0, st>>>(d_plist, d_work, nwork, d_counter);
+			else leg_multi_kernel<32, false><<<grid, LG_THREADS, 0, st>>>(d_plist, d_work, nwork, d_counter);
+			break;
+	}
 	shtb_count_launch();
 }

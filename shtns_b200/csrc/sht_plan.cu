@@ -323,6 +323,17 @@ static int fft_factorize(int n, std::vector<int>& f)
 	return n == 1 && (int) f.size() <= FFT_MAX_FACTORS && fft_smem_bytes(n0, 1) <= 227 * 1024;
 }
 
+// first checkpoint segment of every order for the current spacing s->ckseg
+static void checkpoint_offsets(shtns_cfg s)
+{
+	s->ckoff_h.assign(s->mmax + 1, 0);
+	s->segtot = 0;
+	for (int im = 0; im <= s->mmax; im++) {
+		s->ckoff_h[im] = (int) s->segtot;
+		s->segtot += (s->kmax_h[im] + s->ckseg - 1) / s->ckseg;
+	}
+}
+
 // ---------------------------------------------------------------------------
 static void free_device(shtns_cfg s)
 {
@@ -530,7 +541,7 @@ extern "C" int shtns_set_grid_auto(shtns_cfg s, enum shtns_type flags, double ep
 			s->tm_h[im] = it < s->nlat_2 ? it : s->nlat_2;
 		}
 	}
-	// recurrence checkpoints every 8 degrees-pairs when they take at most
+	// recurrence checkpoints every 8 degree-pairs when they take at most
 	// 512 MB (all threads of a CTA then generate its Y tile in parallel),
 	// else every 16 or 32
 	for (s->ckseg = 8; s->ckseg < LG_SEG; s->ckseg *= 2) {
@@ -538,12 +549,7 @@ extern "C" int shtns_set_grid_auto(shtns_cfg s, enum shtns_type flags, double ep
 		for (int im = 0; im <= s->mmax; im++) segs += (s->kmax_h[im] + s->ckseg - 1) / s->ckseg;
 		if ((double) segs * s->nlat_2 * 16.0 <= 512.0 * 1024 * 1024) break;
 	}
-	s->ckoff_h.assign(s->mmax + 1, 0);
-	s->segtot = 0;
-	for (int im = 0; im <= s->mmax; im++) {
-		s->ckoff_h[im] = (int) s->segtot;
-		s->segtot += (s->kmax_h[im] + s->ckseg - 1) / s->ckseg;
-	}
+	checkpoint_offsets(s);
 	if (init_device(s) != 0) { plan_error("GPU initialisation failed: " + g_last_error); return -1; }
 	s->grid_set = 1;
 	if (s->spat_dist < (long) s->nspat) s->spat_dist = s->nspat;
@@ -759,4 +765,59 @@ extern "C" int shtns_b200_polar_rows(shtns_cfg s, int* tm)
 	if (!s || !s->grid_set) return 0;
 	for (int im = 0; im <= s->mmax; im++) tm[im] = s->tm_h[im];
 	return s->mmax + 1;
+}
+
+// ---------------------------------------------------------------------------
+// Tuning options (shtns_b200_set_option).  Checkpoint spacing rebuilds the
+// recurrence checkpoint table of the plan (not allowed on clones, which share
+// it).
+extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
+{
+	if (!s) return -1;
+	switch (option) {
+		case 1:   // latitude pairs per FFT CTA
+			if (value != 0 && value != 1 && value != 2 && value != 4) return -1;
+			s->fft_pairs = value;
+			return 0;
+		case 2: { // recurrence checkpoint spacing
+			if (value != 8 && value != 16 && value != 32) return -1;
+			if (!s->grid_set || s->is_clone || s->nclones > 0) return -1;
+			if (value == s->ckseg) return 0;
+			cudaDeviceSynchronize();
+			double2* old = s->d_ck;
+			const int old_seg = s->ckseg;
+			s->ckseg = value;
+			checkpoint_offsets(s);
+			double2* nck = nullptr;
+			if (cudaMalloc(&nck, sizeof(double2) * (size_t) s->segtot * s->nlat_2) != cudaSuccess) {
+				cudaGetLastError();
+				s->ckseg = old_seg;
+				checkpoint_offsets(s);
+				shtb_set_error(3, "out of device memory for checkpoints");
+				return -1;
+			}
+			cudaFree(old);
+			s->d_ck = nck;
+			const int nm = s->mmax + 1;
+			cudaMemcpy(s->d_mint + 4 * nm, s->ckoff_h.data(), sizeof(int) * nm, cudaMemcpyHostToDevice);
+			launch_checkpoints(s, 0);
+			return shtb_cuda_ok(cudaDeviceSynchronize(), "checkpoint rebuild") ? 0 : -1;
+		}
+		case 3:   // force the generic FFT kernels
+			s->fft_generic = value ? 1 : 0;
+			return 0;
+		default:
+			return -1;
+	}
+}
+
+extern "C" int shtns_b200_get_option(shtns_cfg s, int option)
+{
+	if (!s) return -1;
+	switch (option) {
+		case 1: return s->fft_pairs;
+		case 2: return s->ckseg;
+		case 3: return s->fft_generic;
+		default: return -1;
+	}
 }
