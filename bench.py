@@ -44,6 +44,17 @@ def spectral_inputs(nf, seed):
     return q, s, t
 
 
+# DRAM bytes (read + write) per field of one launch of each Legendre kernel on
+# this workload, from an ncu capture of the 8-field case (dram__bytes_read.sum +
+# dram__bytes_write.sum; profiles/leg_kernels_lmax511_qst_8fields.md); the
+# traffic grows in proportion to the field count.
+TRAFFIC_PER_FIELD = {"legendre_synthesis": (98.216960e6 + 92.500992e6) / 8,
+                     "legendre_analysis": (153.142784e6 + 34.128384e6) / 8,
+                     "fft_synthesis": (151.062784e6 + 178.811648e6) / 8,
+                     "fft_analysis": (226.558976e6 + 114.498816e6) / 8}
+TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 8-field case, scaled by fields"
+
+
 def legendre_flops(tm, nfields, kind="qst"):
     """Multiply-adds of the even/odd-folded Legendre contraction, x2 flops.
     Per order m, latitude row kept by the polar threshold, field-component and
@@ -343,13 +354,15 @@ def run_gpu(args):
         if dom in (1, 4):
             ach = flops / (per_launch[dom] * 1e-3) / 1e12
             roof = {"kernel": names[dom], "bound": "tensor", "achieved": ach, "peak": peak_fp64,
-                    "unit": "TFLOP/s", "frac": ach / peak_fp64, "traffic": None,
+                    "unit": "TFLOP/s", "frac": ach / peak_fp64, "traffic": TRAFFIC_PER_FIELD[names[dom]] * nf,
+                    "traffic_source": TRAFFIC_SOURCE,
                     "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 on the FP64 tensor cores",
                     "work_per_launch": f"{flops:.4e} flop (8 per theta-row x field-component x Ishioka step)"}
         else:
             ach = fft_bytes / (per_launch[dom] * 1e-3) / 1e9
             roof = {"kernel": names[dom], "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                    "frac": ach / hbm, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
+                    "frac": ach / hbm, "traffic": TRAFFIC_PER_FIELD[names[dom]] * nf, "traffic_source": TRAFFIC_SOURCE,
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
