@@ -46,8 +46,7 @@ def spectral_inputs(nf, seed):
 
 # DRAM bytes (read + write) per field of one launch of each Legendre kernel on
 # this workload, from an ncu capture of the 8-field case (dram__bytes_read.sum +
-# dram__bytes_write.sum; profiles/leg_kernels_lmax511_qst_8fields.md); the
-# traffic grows in proportion to the field count.
+# dram__bytes_write.sum); the traffic grows in proportion to the field count.
 TRAFFIC_PER_FIELD = {"legendre_synthesis": (98.216960e6 + 92.500992e6) / 8,
                      "legendre_analysis": (153.142784e6 + 34.128384e6) / 8,
                      "fft_synthesis": (151.062784e6 + 178.811648e6) / 8,
