@@ -72,7 +72,8 @@ def gauss_nodes(n):
     x = np.concatenate([z, -z[::-1]]).astype(np.float64)
     w = (2 * s2 / (pp * pp)).astype(np.float64)
     w = np.concatenate([w, w[::-1]])
-    st = np.sqrt(s2).astype(np.float64)
+    zr = z.astype(np.float64).astype(LD)                 # sin(theta) of the rounded node
+    st = np.sqrt((1 - zr) * (1 + zr)).astype(np.float64)
     st = np.concatenate([st, st[::-1]])
     return x, st, w
 

@@ -122,7 +122,7 @@ FftParams fft_params(shtns_cfg s, const Job& j)
 	p.fstride = (long)(s->mmax + 1) * s->nlat;
 	p.nf = j.nf; p.spat_dist = s->spat_dist;
 	p.phi_contiguous = s->phi_contiguous;
-	p.generic = s->fft_generic;
+	p.generic = s->fft_generic && fft_smem_bytes(s->nphi, 1) <= 227 * 1024;   // generic kernels need two buffers
 	return p;
 }
 

@@ -353,12 +353,14 @@ template <> struct NphiPlan<768>  { using L = RadixList<8, 8, 4, 3>; };
 template <> struct NphiPlan<1536> { using L = RadixList<8, 8, 8, 3>; };
 template <> struct NphiPlan<3072> { using L = RadixList<8, 8, 4, 4, 3>; };
 template <> struct NphiPlan<6144> { using L = RadixList<8, 8, 8, 4, 3>; };
+template <> struct NphiPlan<12288> { using L = RadixList<8, 8, 8, 8, 3>; };
 
 template <int N, int S>
 struct Geo {
 	static constexpr int A = N + (N >> 3);
 	static constexpr int SEQ = A + (((8 / S) - A) & 7);
-	static constexpr int T = S * N / 8;                     // one radix-8 butterfly per thread
+	// one radix-8 butterfly per thread, at most 768 threads (two or more per thread beyond)
+	static constexpr int T = (S * N / 8 <= 768) ? S * N / 8 : 768;
 	static __device__ __forceinline__ int at(int s, int i) { return s * SEQ + i + (i >> 3); }
 };
 
@@ -560,8 +562,8 @@ template <int N>
 bool launch_fft3_n(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 {
 	// latitude pairs per CTA: up to 4 while the block stays at <= 768 threads
-	if (4 * N / 8 <= 768 && p.S >= 4) return launch_fft3<N, 4>(p, nfc, st, synth);
-	if (2 * N / 8 <= 768 && p.S >= 2) return launch_fft3<N, 2>(p, nfc, st, synth);
+	if constexpr (4 * N / 8 <= 768) if (p.S >= 4) return launch_fft3<N, 4>(p, nfc, st, synth);
+	if constexpr (2 * N / 8 <= 768) if (p.S >= 2) return launch_fft3<N, 2>(p, nfc, st, synth);
 	return launch_fft3<N, 1>(p, nfc, st, synth);
 }
 
@@ -574,6 +576,7 @@ bool launch_fused(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 		case 1536: return launch_fft3_n<1536>(p, nfc, st, synth);
 		case 3072: return launch_fft3_n<3072>(p, nfc, st, synth);
 		case 6144: return launch_fft3_n<6144>(p, nfc, st, synth);
+		case 12288: return launch_fft3_n<12288>(p, nfc, st, synth);
 		default: return false;
 	}
 }
@@ -583,11 +586,15 @@ void set_fused_limits()
 {
 	const int lim = 227 * 1024;
 	cudaFuncSetAttribute(fft3_synth_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-	cudaFuncSetAttribute(fft3_synth_kernel<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-	cudaFuncSetAttribute(fft3_synth_kernel<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 	cudaFuncSetAttribute(fft3_analys_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-	cudaFuncSetAttribute(fft3_analys_kernel<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-	cudaFuncSetAttribute(fft3_analys_kernel<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	if constexpr (2 * N / 8 <= 768) {
+		cudaFuncSetAttribute(fft3_synth_kernel<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+		cudaFuncSetAttribute(fft3_analys_kernel<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	}
+	if constexpr (4 * N / 8 <= 768) {
+		cudaFuncSetAttribute(fft3_synth_kernel<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+		cudaFuncSetAttribute(fft3_analys_kernel<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	}
 }
 
 } // namespace
@@ -607,6 +614,16 @@ int fft_threads(int N, int S, unsigned long long rcode, int nradix)
 }
 
 size_t fft_smem_bytes(int N, int S) { return 2 * sizeof(double2) * (size_t) S * seq_len_host(N, S); }
+
+// sizes with a fused pass chain (one in-place buffer: these may exceed the
+// generic kernels' two-buffer limit)
+bool fft_fused_available(int N)
+{
+	switch (N) {
+		case 192: case 384: case 768: case 1536: case 3072: case 6144: case 12288: return true;
+		default: return false;
+	}
+}
 
 void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st)
 {
@@ -639,7 +656,7 @@ void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st)
 void fft_set_smem_limits()
 {
 	set_fused_limits<192>(); set_fused_limits<384>(); set_fused_limits<768>();
-	set_fused_limits<1536>(); set_fused_limits<3072>(); set_fused_limits<6144>();
+	set_fused_limits<1536>(); set_fused_limits<3072>(); set_fused_limits<6144>(); set_fused_limits<12288>();
 	const int lim = 227 * 1024;
 	cudaFuncSetAttribute(fft_synth_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 	cudaFuncSetAttribute(fft_synth_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);

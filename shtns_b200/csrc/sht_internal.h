@@ -161,6 +161,7 @@ void launch_leg_analys(const LegParams& p, int kmax_all, cudaStream_t st);
 void launch_leg_multi(const LegParams* d_plist, const int4* d_work, int nwork, int* d_counter, int ckseg, bool synth,
                       int nctas, cudaStream_t st);
 int fft_threads(int N, int S, unsigned long long rcode, int nradix);
+bool fft_fused_available(int N);
 size_t fft_smem_bytes(int N, int S);
 void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st);
 void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st);

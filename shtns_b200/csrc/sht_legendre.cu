@@ -29,10 +29,22 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b)
 
 // ---------------------------------------------------------------------------
 // Checkpoints: thread (t, im) runs the recurrence of order m at north row t and
-// stores (Y_{seg*s}, Y_{seg*s+1}) for every segment s (seg = 8, 16 or 32).  Y_0 = sin^m(theta) by
-// binary powering (sint_pow_n_ext, sht_legendre.c:110-139, without the range
-// extension: below lmax 1800 an underflowed seed only drops values below
-// 1e-300), Y_1 = (c_1 x^2 + c_0) Y_0 (kernel_SH_to_spat.gen.c:303-315).
+// stores (Y_{seg*s}, Y_{seg*s+1}) for every segment s (seg = 8, 16 or 32).
+// Y_0 = sin^m(theta) (sint_pow_n_ext, sht_legendre.c:110-139) and
+// Y_1 = (c_1 x^2 + c_0) Y_0 (kernel_SH_to_spat.gen.c:303-315).
+// Extended exponent: above degree ~1800, sin^m(theta) falls below the double
+// range at latitudes where Y_k later grows to O(1).  The seed is formed as a
+// mantissa times 2^E by binary powering with frexp normalisation, and the
+// recurrence runs on scaled values y * 2^E (it is linear and homogeneous, so
+// scaling by a power of two is exact) until the values have grown enough for
+// E to be folded back to 0.  Each checkpoint stores y * 2^E as a plain double:
+// a checkpoint that underflows is below 2^-1022 and stays below ~1e-280 over
+// the next 32 steps, far under any threshold.  The reference keeps the same
+// kind of scaled seed (sint_pow_n_ext, sht_legendre.c:109-139) and rescales
+// its recurrence when values become significant (sht_legendre.c:159-187,
+// sht_func.c:200-233).
+#define CK_FOLD 600          // fold E into the values when E >= -CK_FOLD
+#define CK_BIG 0x1p500       // rescale scaled values above this magnitude
 __global__ void ck_kernel(int nlat_2, int mres, int seg, const double* __restrict__ x2g, const double* __restrict__ sing,
                           const double* __restrict__ c, MTables mt, const int* __restrict__ nseg, double2* __restrict__ ck)
 {
@@ -41,25 +53,35 @@ __global__ void ck_kernel(int nlat_2, int mres, int seg, const double* __restric
 	if (t >= nlat_2) return;
 	const int m = im * mres;
 	const double x2 = x2g[t];
-	double y0 = 1.0, b = sing[t];
-	for (int n = m; n; n >>= 1) {
-		if (n & 1) y0 *= b;
-		b *= b;
+	// sin^m = y0 * 2^E, y0 in [0.5, 1)
+	double y0 = 1.0;
+	int E = 0;
+	{
+		int be, te;
+		double b = frexp(sing[t], &be);
+		for (int n = m; n; n >>= 1) {
+			if (n & 1) { y0 = frexp(y0 * b, &te); E += be + te; }
+			b = frexp(b * b, &te); be = 2 * be + te;
+		}
 	}
+	if (E >= -CK_FOLD) { y0 = ldexp(y0, E); E = 0; }
 	const double* cc = c + mt.coff[im];
 	double y1 = fma(cc[1], x2, cc[0]) * y0;
 	const int ns = nseg[im];
 	double2* out = ck + (long)mt.ckoff[im] * nlat_2 + t;
 	for (int s = 0; s < ns; s++) {
-		out[(long)s * nlat_2] = make_double2(y0, y1);
+		out[(long)s * nlat_2] = E ? make_double2(ldexp(y0, E), ldexp(y1, E)) : make_double2(y0, y1);
 		const int kb = s * seg + 1;
-		#pragma unroll 4
 		for (int j = 0; j < seg; j++) {
 			const int k = kb + j;
 			const double a = fma(cc[2 * k + 1], x2, cc[2 * k]);
 			const double y2 = fma(a, y1, y0);
 			y0 = y1;
 			y1 = y2;
+			if (E && fabs(y1) > CK_BIG) {
+				if (E >= -CK_FOLD) { y0 = ldexp(y0, E); y1 = ldexp(y1, E); E = 0; }
+				else { y0 *= 0x1p-500; y1 *= 0x1p-500; E += 500; }
+			}
 		}
 	}
 }

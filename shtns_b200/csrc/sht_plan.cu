@@ -320,7 +320,7 @@ static int fft_factorize(int n, std::vector<int>& f)
 	for (int r : f) rmin = r < rmin ? r : rmin;
 	(void) rmin;
 	// one CTA holds two padded buffers of a latitude pair in shared memory
-	return n == 1 && (int) f.size() <= FFT_MAX_FACTORS && fft_smem_bytes(n0, 1) <= 227 * 1024;
+	return n == 1 && (int) f.size() <= FFT_MAX_FACTORS && (fft_smem_bytes(n0, 1) <= 227 * 1024 || fft_fused_available(n0));
 }
 
 // first checkpoint segment of every order for the current spacing s->ckseg
@@ -502,7 +502,7 @@ extern "C" int shtns_set_grid_auto(shtns_cfg s, enum shtns_type flags, double ep
 	if (np <= 2 * s->mmax) { plan_error("the sampling condition Nphi > 2*Mmax is not met."); return -1; }
 	if (nl > 65534 || np > 65534) { plan_error("Nlat or Nphi too large"); return -1; }
 	std::vector<int> rad;
-	if (!fft_factorize(np, rad)) { plan_error("Nphi must factor into 2, 3, 5 and 7 and not exceed 6400"); return -1; }
+	if (!fft_factorize(np, rad)) { plan_error("Nphi must factor into 2, 3, 5 and 7 and not exceed 6400 (or be 3*2^k up to 12288)"); return -1; }
 	if (layout & SHT_PHI_CONTIGUOUS && layout & SHT_THETA_CONTIGUOUS) { plan_error("conflicting layout flags"); return -1; }
 	shtns_unset_grid(s);
 	s->fft_radix = rad;
@@ -519,8 +519,13 @@ extern "C" int shtns_set_grid_auto(shtns_cfg s, enum shtns_type flags, double ep
 	s->ct_v.assign(nl, 0.0); s->st_v.assign(nl, 0.0);
 	s->wq.assign(s->nlat_2, 0.0);
 	const double latdir = s->south_first ? -1.0 : 1.0;
+	// sin(theta) of the node as rounded to double, not of the extended-precision
+	// node: every table then describes the same point.  Near the poles an
+	// inconsistent pair is amplified (|d sin / sin| = x |dx| / sin^2: 4e-10 at
+	// the first row of a 6144-point grid), which would scale the m >= 1 terms.
 	for (int t = 0; t < s->nlat_2; t++) {
-		const double st = (double) std::sqrt((1.0L - xg[t]) * (1.0L + xg[t]));
+		const long double xr = (long double)(double) xg[t];
+		const double st = (double) std::sqrt((1.0L - xr) * (1.0L + xr));
 		s->ct_v[t] = latdir * (double) xg[t];
 		s->ct_v[nl - 1 - t] = -latdir * (double) xg[t];
 		s->st_v[t] = st; s->st_v[nl - 1 - t] = st;
@@ -536,7 +541,8 @@ extern "C" int shtns_set_grid_auto(shtns_cfg s, enum shtns_type flags, double ep
 			do {
 				it++;
 				if (it >= s->nlat_2) break;
-				v = max_plm(s, im, xg[it], std::sqrt((1.0L - xg[it]) * (1.0L + xg[it])));
+				const long double xr = (long double)(double) xg[it];
+				v = max_plm(s, im, xr, std::sqrt((1.0L - xr) * (1.0L + xr)));
 			} while (v < eps);
 			s->tm_h[im] = it < s->nlat_2 ? it : s->nlat_2;
 		}
