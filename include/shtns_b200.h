@@ -78,6 +78,15 @@ void cu_spat_to_SH_adjoint(shtns_cfg, cplx *Qg, double *Vg, int ltr);
 int shtns_b200_set_option(shtns_cfg, int option, int value);
 int shtns_b200_get_option(shtns_cfg, int option);
 
+/* Option 4 of shtns_b200_set_option: split-precision Legendre synthesis on
+ * the FP16 tensor cores with 3, 4 or 5 balanced 8-bit slices per operand
+ * (about 24, 32, 40 bits; products summed exactly in FP32 over windows of 256
+ * steps and in FP64 across them); 0 (default) keeps the FP64 contraction.
+ * Waits for the plan's stream; returns 1 (and clears it) if a bounded wait of
+ * the split-precision kernel gave up since the last call, else 0.
+ * No counterpart in SHTns 3.5.2. */
+int shtns_b200_kernel_errors(shtns_cfg);
+
 /* Plan groups: scalar transforms of fields of different lmax, each on the grid
  * of its own plan, with the Legendre stage of all plans in one persistent
  * launch whose CTAs take work items (plan, order, tile) from a queue in

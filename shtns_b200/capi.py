@@ -112,6 +112,7 @@ PROTOTYPES = {
     "cu_SH_to_spat_adjoint": (None, [CFG, P, P, I]),
     "cu_spat_to_SH_adjoint": (None, [CFG, P, P, I]),
     "shtns_b200_set_option": (I, [CFG, I, I]),
+    "shtns_b200_kernel_errors": (I, [CFG]),
     "shtns_b200_get_option": (I, [CFG, I]),
     "shtns_b200_group_create": (P, [I, P]),
     "shtns_b200_group_destroy": (None, [P]),

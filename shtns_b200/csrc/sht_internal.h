@@ -94,6 +94,17 @@ struct shtns_info {
 	double *d_qq; size_t qq_cap;         // k-major coefficient buffer [row][col]
 	double2 *d_F; size_t F_cap;          // Fourier coefficients [fc][im][theta]
 	void *d_stage; size_t stage_cap;     // device staging for host-pointer transforms
+	// split-precision synthesis (shtns_b200_set_option 4): slices per operand
+	// (0 = FP64 contraction) and its tables and buffers, allocated on first use
+	// and owned by each plan object (clones included)
+	int split_ns;
+	short *d_yexp;                       // row exponents [im][north row]
+	int *d_boff;                         // first 64-step chunk of each order in d_bsl
+	long split_chunks;                   // chunks over all orders
+	int split_kc;                        // steps per chunk of d_boff
+	void *d_bsl; size_t bsl_cap;         // coefficient slices
+	int *d_bexp; size_t bexp_cap;        // column exponents [im][column]
+	int *d_split_err;                    // set by the kernel when a wait gives up
 	cudaStream_t comp_stream, xfer_stream;
 	int own_xfer;
 	int is_clone;
@@ -158,6 +169,8 @@ void launch_prep_synth(const PrepParams& p, cudaStream_t st);
 void launch_post_analys_m(const PrepParams& p, int mmax, cudaStream_t st);
 void launch_leg_synth(const LegParams& p, cudaStream_t st);
 void launch_leg_analys(const LegParams& p, int kmax_all, cudaStream_t st);
+void launch_leg_synth_split(shtns_cfg s, const LegParams& p, cudaStream_t st);
+void free_split(shtns_cfg s);
 void launch_leg_multi(const LegParams* d_plist, const int4* d_work, int nwork, int* d_counter, int ckseg, bool synth,
                       int nctas, cudaStream_t st);
 int fft_threads(int N, int S, unsigned long long rcode, int nradix);

@@ -343,6 +343,7 @@ static void free_device(shtns_cfg s)
 		void* ptrs[] = {s->d_x, s->d_c, s->d_ck, s->d_tw, s->d_mint};
 		for (void* p : ptrs) if (p) cudaFree(p);
 	}
+	free_split(s);
 	if (s->d_qq) cudaFree(s->d_qq);
 	if (s->d_F) cudaFree(s->d_F);
 	if (s->d_stage) cudaFree(s->d_stage);
@@ -674,6 +675,8 @@ extern "C" shtns_cfg cushtns_clone(shtns_cfg b, cudaStream_t compute_stream, cud
 	s->base->nclones++;
 	s->d_qq = nullptr; s->qq_cap = 0; s->d_F = nullptr; s->F_cap = 0;
 	s->d_stage = nullptr; s->stage_cap = 0;
+	s->d_yexp = nullptr; s->d_boff = nullptr; s->split_chunks = 0; s->split_kc = 0;
+	s->d_bsl = nullptr; s->bsl_cap = 0; s->d_bexp = nullptr; s->bexp_cap = 0; s->d_split_err = nullptr;
 	s->xfer_stream = nullptr; s->own_xfer = 0;
 	s->ev.clear(); s->ev_stage.clear(); s->ev_used = 0; s->timing = 0;
 	cushtns_set_streams(s, compute_stream, transfer_stream);
@@ -785,6 +788,10 @@ extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
 			if (value != 0 && value != 1 && value != 2 && value != 4) return -1;
 			s->fft_pairs = value;
 			return 0;
+		case 4:   // split-precision synthesis: slices per operand (0 = FP64)
+			if (value != 0 && (value < 3 || value > 7)) return -1;
+			s->split_ns = value;
+			return 0;
 		case 2: { // recurrence checkpoint spacing
 			if (value != 8 && value != 16 && value != 32) return -1;
 			if (!s->grid_set || s->is_clone || s->nclones > 0) return -1;
@@ -824,6 +831,7 @@ extern "C" int shtns_b200_get_option(shtns_cfg s, int option)
 		case 1: return s->fft_pairs;
 		case 2: return s->ckseg;
 		case 3: return s->fft_generic;
+		case 4: return s->split_ns;
 		default: return -1;
 	}
 }

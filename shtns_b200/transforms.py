@@ -145,6 +145,18 @@ class sht:
         c._clone_of = self
         return c
 
+    def set_split(self, nslices):
+        """Split-precision Legendre synthesis on the FP16 tensor cores with
+        `nslices` (3 to 7) 8-bit slices per operand; 0 restores the FP64
+        contraction.  Analysis always runs in FP64."""
+        if self._lib.shtns_b200_set_option(self._cfg, 4, int(nslices)) != 0:
+            raise ValueError("nslices must be 0 or 3..7")
+
+    def kernel_errors(self):
+        """1 if a bounded wait inside a split-precision kernel gave up (the
+        result of that call is not valid), else 0; clears the flag."""
+        return self._lib.shtns_b200_kernel_errors(self._cfg)
+
     def device_bytes(self):
         return self._lib.shtns_b200_device_bytes(self._cfg)
 
