@@ -31,6 +31,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 LMAX, NLAT, NPHI, NFIELDS, EPS = 511, 768, 1536, 64, 1e-10
+E2E_CHUNKS = 16
 METRIC = "SH_to_spat+spat_to_SH pairs/s vs lmax; FP64 plain vs batched/split-prec at 1e-11"
 UNIT = "field-pairs/s (SHqst_to_spat+spat_to_SHqst, lmax=511, 768x1536)"
 WORKLOAD = "lmax511_qst_64fields"
@@ -295,18 +296,32 @@ def run_gpu(args):
     # correctness of what was timed
     rt_err = max(float((a - b).abs().max() / a.abs().max()) for a, b in zip(spec, back))
 
-    # end to end through the public API: pinned host spectra in, spectra out
+    # end to end through the public API: pinned host spectra in, spectra out.
+    # The step's fields go in E2E_CHUNKS chunks, each on its own stream with
+    # its own plan clone (cushtns_clone), so that the host->device copy of one
+    # chunk, the transforms of another and the device->host copy of a third
+    # overlap (one copy engine per direction).
     host_in = [torch.from_numpy(a).pin_memory() for a in (qn, sn, tn)]
     host_out = [torch.empty((nf, sh.nlm), dtype=torch.complex128).pin_memory() for _ in range(3)]
     e2e_steps = max(3, min(args.steps, 20))
+    nch = max(1, min(args.e2e_chunks, nf))
+    bounds = [(c * nf // nch, (c + 1) * nf // nch) for c in range(nch)]
+    streams = [torch.cuda.Stream(device=dev) for _ in range(nch)]
+    clones = [sh.clone(stream=st.cuda_stream) for st in streams]
 
     def e2e_step():
-        for d, h in zip(spec, host_in):
-            d.copy_(h, non_blocking=True)
-        sh.synth_into(spec, spat)
-        sh.analys_into(spat, back)
-        for h, d in zip(host_out, back):
-            h.copy_(d, non_blocking=True)
+        main = torch.cuda.current_stream()
+        for (a, b), st, pl in zip(bounds, streams, clones):
+            st.wait_stream(main)
+            with torch.cuda.stream(st):
+                for d, h in zip(spec, host_in):
+                    d[a:b].copy_(h[a:b], non_blocking=True)
+                pl.synth_into([x[a:b] for x in spec], [x[a:b] for x in spat])
+                pl.analys_into([x[a:b] for x in spat], [x[a:b] for x in back])
+                for h, d in zip(host_out, back):
+                    h[a:b].copy_(d[a:b], non_blocking=True)
+        for st in streams:
+            main.wait_stream(st)
 
     for _ in range(2):
         e2e_step()
@@ -376,7 +391,8 @@ def run_gpu(args):
             "roundtrip_relerr": rt_err,
             "gpu_launches": int(launches),
             "e2e": {"value": world * nf / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
-                    "d2h_bytes_per_step": bytes_io},
+                    "d2h_bytes_per_step": bytes_io,
+                    "form": f"{nch} field chunks on {nch} streams with plan clones: copies overlap transforms"},
             "clocks": clk,
         }
         if world == 1 and not args.no_cpu:
@@ -492,6 +508,110 @@ def run_uneven(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- high degree
+HD_L, HD_NLAT, HD_NPHI, HD_NF = 4095, 6144, 12288, 8
+HD_UNIT = "field-pairs/s (SH_to_spat+spat_to_SH, lmax=4095, 6144x12288)"
+
+
+def run_highdeg(args):
+    """lmax=4095 on the 6144 x 12288 Gauss grid, 8 scalar fields: the FP64
+    transform pair against split-precision synthesis (FP16 tensor cores, 5, 6
+    and 7 slices per operand; analysis stays FP64).  value = FP64 pairs/s;
+    each split form reports its synthesis and pair rates and its max / RMS
+    error against the FP64 synthesis of the same coefficients."""
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    import shtns_b200
+    from shtns_b200 import capi
+    from tests.common import rand_spec
+    lib = capi.load()
+    nf = args.fields if args.fields != NFIELDS else HD_NF
+    sh = shtns_b200.sht(HD_L)
+    sh.set_grid(HD_NLAT, HD_NPHI, flags=shtns_b200.sht_quick_init | shtns_b200.SHT_THETA_CONTIGUOUS, polar_opt=EPS)
+    q = torch.from_numpy(rand_spec(HD_L, HD_L, 1, 400, power=1.0, nfields=nf)).to(dev)
+    v = torch.empty((nf,) + sh.spat_shape, dtype=torch.float64, device=dev)
+    r = torch.empty_like(q)
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def synth():
+        sh.synth_into([q], [v])
+
+    def pair():
+        sh.synth_into([q], [v])
+        sh.analys_into([v], [r])
+
+    steps = max(3, min(args.steps, 10))
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    sh.set_split(0)
+    ms_pair = timed(pair, steps)
+    ms_syn = timed(synth, steps)
+    v64 = v.clone()
+    rt = float((r - q).abs().max() / q.abs().max())
+    lib.shtns_b200_set_timing(sh._cfg, 1)
+    synth()
+    torch.cuda.synchronize()
+    st = np.zeros(6)
+    ca = np.zeros(6, dtype=np.int64)
+    lib.shtns_b200_stage_times(sh._cfg, st.ctypes.data_as(C.c_void_p), ca.ctypes.data_as(C.c_void_p))
+    lib.shtns_b200_set_timing(sh._cfg, 0)
+    forms = {"fp64": {"synth_ms": ms_syn, "pair_ms": ms_pair, "legendre_synth_ms": st[1] / max(ca[1], 1),
+                      "pairs_per_s": nf / (ms_pair * 1e-3)}}
+    for ns in (5, 6, 7):
+        sh.set_split(ns)
+        ms_s = timed(synth, steps)
+        d = v - v64
+        err_max = float(d.abs().max() / v64.abs().max())
+        err_rms = float((d * d).mean().sqrt() / (v64 * v64).mean().sqrt())
+        ms_p = timed(pair, steps)
+        lib.shtns_b200_set_timing(sh._cfg, 1)
+        synth()
+        torch.cuda.synchronize()
+        st[:] = 0
+        ca[:] = 0
+        lib.shtns_b200_stage_times(sh._cfg, st.ctypes.data_as(C.c_void_p), ca.ctypes.data_as(C.c_void_p))
+        lib.shtns_b200_set_timing(sh._cfg, 0)
+        forms["split%d" % ns] = {"synth_ms": ms_s, "pair_ms": ms_p, "legendre_synth_ms": st[1] / max(ca[1], 1),
+                                 "pairs_per_s": nf / (ms_p * 1e-3), "max_rel_err": err_max, "rms_rel_err": err_rms,
+                                 "kernel_errors": int(sh.kernel_errors())}
+    sh.set_split(0)
+    clk = clocks.stop()
+    tm = np.zeros(HD_L + 1, dtype=np.int32)
+    lib.shtns_b200_polar_rows(sh._cfg, tm.ctypes.data_as(C.c_void_p))
+    rows = HD_NLAT // 2 - tm
+    ks = (HD_L - np.arange(HD_L + 1)) // 2 + 1
+    flops = 8.0 * float((rows * ks).sum()) * nf
+    peak = fp64_gemm_peak(torch, dev)
+    ach = flops / (forms["fp64"]["legendre_synth_ms"] * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": nf / (ms_pair * 1e-3), "unit": HD_UNIT, "n_gpus": 1, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": ms_pair, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1)/(l+1))",
+        "config": {"workload": "lmax4095_8fields", "lmax": HD_L, "nlat": HD_NLAT, "nphi": HD_NPHI, "fields": nf,
+                   "polar_eps": EPS, "layout": "theta-contiguous", "form": "FP64 synthesis + analysis"},
+        "forms": forms,
+        "roofline": {"kernel": "leg_synth_kernel (FP64)", "bound": "tensor", "achieved": ach, "peak": peak,
+                     "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+                     "peak_source": "measured in this run: cuBLAS DGEMM 8192^3"},
+        "roundtrip_relerr": rt,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -501,12 +621,17 @@ def main():
     ap.add_argument("--fields", type=int, default=NFIELDS)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="qst", choices=["qst", "uneven"],
+    ap.add_argument("--e2e-chunks", type=int, default=E2E_CHUNKS,
+                    help="field chunks (streams) of the end-to-end step")
+    ap.add_argument("--workload", default="qst", choices=["qst", "uneven", "highdeg"],
                     help="qst: lmax=511 vector transforms of 64 fields (default); "
-                         "uneven: 256 scalar fields of lmax 63..1023 through a plan group")
+                         "uneven: 256 scalar fields of lmax 63..1023 through a plan group; "
+                         "highdeg: lmax=4095, 8 fields, FP64 and split-precision synthesis")
     args = ap.parse_args()
     if args.workload == "uneven" and args.impl != "reference":
         run_uneven(args)
+    elif args.workload == "highdeg" and args.impl != "reference":
+        run_highdeg(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
