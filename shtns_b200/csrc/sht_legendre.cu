@@ -305,6 +305,12 @@ __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int t
 		#pragma unroll
 		for (int j = 0; j < 2; j++) { acc[i][j][0] = 0.0; acc[i][j][1] = 0.0; }
 
+	// 8 x 8 fragments of this warp that carry results: rows in [tmm, nlat/2),
+	// columns below ncol (the others are discarded by the epilogue)
+	const int wr = t0 + wm * 32, wc = c0 + wn * 16;
+	const int ri0 = min(4, max(0, (tmm - wr) / 8));
+	const int ri1 = min(4, max(0, (p.nlat_2 - wr + 7) / 8));
+	const int cj1 = min(2, max(0, (p.ncol - wc + 7) / 8));
 	if (t0 + LG_BM > tmm) {
 		const double* cm = p.c + p.mt.coff[im];
 		const double2* ckm = p.ck + (long)p.mt.ckoff[im] * p.nlat_2;
@@ -356,8 +362,10 @@ __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int t
 			}
 			__syncthreads();
 			if (k0 + LG_BK < nk) load_b(k0 + LG_BK);
+			const int kv = nk - k0;                      // steps of this chunk below nk
 			#pragma unroll
 			for (int kk = 0; kk < LG_BK; kk += 4) {
+				if (kk >= kv) break;                      // rows of Bs beyond nk are zero
 				double a[4], b[2];
 				#pragma unroll
 				for (int i = 0; i < 4; i++) a[i] = As[kk + (lane & 3)][wm * 32 + i * 8 + (lane >> 2)];
@@ -366,7 +374,8 @@ __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int t
 				#pragma unroll
 				for (int i = 0; i < 4; i++)
 					#pragma unroll
-					for (int j = 0; j < 2; j++) dmma(acc[i][j], a[i], b[j]);
+					for (int j = 0; j < 2; j++)
+						if (i >= ri0 && i < ri1 && j < cj1) dmma(acc[i][j], a[i], b[j]);
 			}
 			__syncthreads();
 		}
@@ -421,6 +430,10 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 	const double* cm = p.c + p.mt.coff[im];
 	const double2* ckm = p.ck + (long)p.mt.ckoff[im] * p.nlat_2;
 	const int fc0 = c0 / 4;
+	// 8 x 8 fragments of this warp that carry results: k below nk, columns
+	// below ncol (the others are not stored)
+	const int ki1 = min(4, max(0, (nk - k0 - wm * 32 + 7) / 8));
+	const int cj1 = min(2, max(0, (p.ncol - c0 - wn * 16 + 7) / 8));
 
 	double acc[4][2][2];
 	#pragma unroll
@@ -515,7 +528,8 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 			#pragma unroll
 			for (int i = 0; i < 4; i++)
 				#pragma unroll
-				for (int j = 0; j < 2; j++) dmma(acc[i][j], a[i], b[j]);
+				for (int j = 0; j < 2; j++)
+					if (i < ki1 && j < cj1) dmma(acc[i][j], a[i], b[j]);
 		}
 		__syncthreads();
 	}
