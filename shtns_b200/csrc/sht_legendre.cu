@@ -287,15 +287,18 @@ __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 // of one (row, field-component) and folds north/south itself.
 #define SA_LD 68   // shared row stride in doubles: 4 mod 16 keeps fragment loads conflict-free
 
-template <int SEG>
+// WM = warps along the rows (2: 64 rows x 64 columns per CTA; 4: 128 rows x
+// 32 columns, for calls with at most 8 field-components).
+template <int SEG, int WM>
 __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int tb, int nb)
 {
-	__shared__ __align__(16) double As[LG_BK][SA_LD];   // [k][theta]
-	__shared__ __align__(16) double Bs[LG_BK][SA_LD];   // [k][col]
+	constexpr int WN = 8 / WM, BM = 32 * WM, BN = 16 * WN;
+	__shared__ __align__(16) double As[LG_BK][BM + 4];   // [k][theta]; strides 4 mod 16:
+	__shared__ __align__(16) double Bs[LG_BK][BN + 4];   // [k][col]    conflict-free fragment loads
 	const int m = im * p.mres;
-	const int t0 = tb * LG_BM, c0 = nb * LG_BN;
+	const int t0 = tb * BM, c0 = nb * BN;
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-	const int wm = warp >> 2, wn = warp & 3;
+	const int wm = warp / WN, wn = warp % WN;
 	const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
 	const int tmm = p.mt.tm[im];
 
@@ -311,53 +314,64 @@ __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int t
 	const int ri0 = min(4, max(0, (tmm - wr) / 8));
 	const int ri1 = min(4, max(0, (p.nlat_2 - wr + 7) / 8));
 	const int cj1 = min(2, max(0, (p.ncol - wc + 7) / 8));
-	if (t0 + LG_BM > tmm) {
+	if (t0 + BM > tmm) {
 		const double* cm = p.c + p.mt.coff[im];
 		const double2* ckm = p.ck + (long)p.mt.ckoff[im] * p.nlat_2;
 		const double* qrow = p.qq + (long)p.mt.koff[im] * p.ncol;
 		// software pipeline: the B tile and checkpoint of chunk k0+32 are
 		// loaded into registers while the tensor cores work on chunk k0
-		constexpr int NBV = LG_BK * (LG_BN / 2) / LG_THREADS;   // double2 per thread
+		constexpr int NBV = LG_BK * (BN / 2) / LG_THREADS;   // double2 per thread
 		double2 bn[NBV];
-		// generators: thread (row gr, segment gj) produces Y_k for SEG
-		// consecutive k of the chunk from the checkpoint at its segment start
-		constexpr int NSEGC = LG_BK / SEG;
-		double2 ckn = make_double2(0.0, 0.0);
-		const int gr = tid % LG_BM, gj = tid / LG_BM;
+		// generators: thread (row gr, segment sg = gj + u GPR) produces Y_k for
+		// SEG consecutive k of the chunk from the checkpoint at its segment start
+		constexpr int NSEGC = LG_BK / SEG;                    // segments per chunk
+		constexpr int GPR = LG_THREADS / BM;                  // generator threads per row
+		constexpr int SPT = (NSEGC + GPR - 1) / GPR;          // segments per generator thread
+		double2 ckn[SPT];
+		const int gr = tid % BM, gj = tid / BM;
 		const int tg = t0 + gr;
-		const bool gen = (gj < NSEGC) && (tg < p.nlat_2);
+		const bool gen = tg < p.nlat_2;
 		const double x2 = gen ? p.x2[tg] : 0.0;
 		auto load_b = [&](int k0) {
 			#pragma unroll
 			for (int u = 0; u < NBV; u++) {
 				const int e = tid + u * LG_THREADS;
-				const int kk = e / (LG_BN / 2), cc2 = (e - kk * (LG_BN / 2)) * 2;
+				const int kk = e / (BN / 2), cc2 = (e - kk * (BN / 2)) * 2;
 				const int k = k0 + kk, col = c0 + cc2;
 				bn[u] = (k < nk && col < p.ncol) ? __ldg(reinterpret_cast<const double2*>(qrow + (long)k * p.ncol + col))
 				                                 : make_double2(0.0, 0.0);
 			}
-			const int ks = k0 + gj * SEG;
-			ckn = (gen && ks < nk) ? __ldg(ckm + (long)(ks / SEG) * p.nlat_2 + tg) : make_double2(0.0, 0.0);
+			#pragma unroll
+			for (int u = 0; u < SPT; u++) {
+				const int sg = gj + u * GPR;
+				const int ks = k0 + sg * SEG;
+				ckn[u] = (sg < NSEGC && gen && ks < nk) ? __ldg(ckm + (long)(ks / SEG) * p.nlat_2 + tg)
+				                                       : make_double2(0.0, 0.0);
+			}
 		};
 		load_b(0);
 		for (int k0 = 0; k0 < nk; k0 += LG_BK) {
-			if (gj < NSEGC) {
-				double y0 = ckn.x, y1 = ckn.y;
-				As[gj * SEG][gr] = y0;
-				As[gj * SEG + 1][gr] = y1;
-				const double* cc = cm + 2 * (k0 + gj * SEG);
-				#pragma unroll
-				for (int j = 2; j < SEG; j++) {
-					const double a = fma(cc[2 * j - 1], x2, cc[2 * j - 2]);
-					const double y2 = fma(a, y1, y0);
-					As[gj * SEG + j][gr] = y2;
-					y0 = y1; y1 = y2;
+			#pragma unroll
+			for (int u = 0; u < SPT; u++) {
+				const int sg = gj + u * GPR;
+				if (sg < NSEGC) {
+					double y0 = ckn[u].x, y1 = ckn[u].y;
+					As[sg * SEG][gr] = y0;
+					As[sg * SEG + 1][gr] = y1;
+					const double* cc = cm + 2 * (k0 + sg * SEG);
+					#pragma unroll
+					for (int j = 2; j < SEG; j++) {
+						const double a = fma(cc[2 * j - 1], x2, cc[2 * j - 2]);
+						const double y2 = fma(a, y1, y0);
+						As[sg * SEG + j][gr] = y2;
+						y0 = y1; y1 = y2;
+					}
 				}
 			}
 			#pragma unroll
 			for (int u = 0; u < NBV; u++) {
 				const int e = tid + u * LG_THREADS;
-				const int kk = e / (LG_BN / 2), cc2 = (e - kk * (LG_BN / 2)) * 2;
+				const int kk = e / (BN / 2), cc2 = (e - kk * (BN / 2)) * 2;
 				*reinterpret_cast<double2*>(&Bs[kk][cc2]) = bn[u];
 			}
 			__syncthreads();
@@ -414,17 +428,20 @@ __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int t
 // 1/sin(theta) for vector components (1/sin^2 in Robert form).
 #define AA_LD 36   // As row stride (k rows x 32 theta): 4 mod 16
 
-template <int SEG>
+// WM = warps along the k rows (2: 64 k x 64 columns per CTA; 4: 128 k x 32
+// columns, for calls with at most 8 field-components).
+template <int SEG, int WM>
 __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int kb, int nb)
 {
-	__shared__ __align__(16) double As[LG_BM][AA_LD];   // [k][theta]
-	__shared__ __align__(16) double Bs[LG_BK][SA_LD];   // [theta][col]
+	constexpr int WN = 8 / WM, BM = 32 * WM, BN = 16 * WN;
+	__shared__ __align__(16) double As[BM][AA_LD];       // [k][theta]
+	__shared__ __align__(16) double Bs[LG_BK][BN + 4];   // [theta][col]
 	const int m = im * p.mres;
-	const int k0 = kb * LG_BM, c0 = nb * LG_BN;
+	const int k0 = kb * BM, c0 = nb * BN;
 	const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
 	if (k0 >= nk) return;
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-	const int wm = warp >> 2, wn = warp & 3;
+	const int wm = warp / WN, wn = warp % WN;
 	const int tmm = p.mt.tm[im];
 	const double wfac = (m > 0) ? p.mpos_inv : 1.0;
 	const double* cm = p.c + p.mt.coff[im];
@@ -443,14 +460,16 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 
 	// software pipeline: F values and checkpoints of the next theta chunk are
 	// loaded into registers while the tensor cores work on the current one
-	constexpr int NBF = LG_BK * (LG_BN / 4) / LG_THREADS;   // (theta, field-component) items per thread
+	constexpr int NBF = LG_BK * (BN / 4) / LG_THREADS;   // (theta, field-component) items per thread
 	double2 fnn[NBF], fsn[NBF];
-	// generators: thread (theta gtt, segment gsg) produces Y_k for SEG
-	// consecutive k of the CTA's k rows from the checkpoint at its segment start
-	double2 ckn = make_double2(0.0, 0.0);
+	// generators: thread (theta gtt, segment sg = gsg + u GPT) produces Y_k
+	// for SEG consecutive k of the CTA's k rows from the checkpoint at its
+	// segment start
+	constexpr int NSG = BM / SEG;                         // segments per tile
+	constexpr int GPT = LG_THREADS / LG_BK;               // generator threads per theta
+	constexpr int SPT = (NSG + GPT - 1) / GPT;            // segments per generator thread
+	double2 ckn[SPT];
 	const int gtt = tid % LG_BK, gsg = tid / LG_BK;
-	const int gks = k0 + gsg * SEG;
-	const bool gen_thread = gsg < LG_BM / SEG;
 	auto load_next = [&](int tt0) {
 		#pragma unroll
 		for (int u = 0; u < NBF; u++) {
@@ -467,30 +486,39 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 			}
 		}
 		const int t = tt0 + gtt;
-		if (gen_thread && t < p.nlat_2 && gks < nk) ckn = __ldg(ckm + (long)(gks / SEG) * p.nlat_2 + t);
-		else ckn = make_double2(0.0, 0.0);
+		#pragma unroll
+		for (int u = 0; u < SPT; u++) {
+			const int sg = gsg + u * GPT, gks = k0 + sg * SEG;
+			ckn[u] = (sg < NSG && t < p.nlat_2 && gks < nk) ? __ldg(ckm + (long)(gks / SEG) * p.nlat_2 + t)
+			                                               : make_double2(0.0, 0.0);
+		}
 	};
 	const int tstart = (tmm / LG_BK) * LG_BK;
 	if (tstart < p.nlat_2) load_next(tstart);
 	for (int tt0 = tstart; tt0 < p.nlat_2; tt0 += LG_BK) {
-		if (gen_thread) {
+		{
 			const int t = tt0 + gtt;
-			double y0 = ckn.x, y1 = ckn.y;
 			const double x2 = (t < p.nlat_2) ? p.x2[t] : 0.0;
-			double* a = &As[gsg * SEG][gtt];
-			a[0] = y0;
-			a[AA_LD] = y1;
-			if (gks < nk) {
-				const double* cc = cm + 2 * gks;
-				#pragma unroll
-				for (int j = 2; j < SEG; j++) {
-					const double aa = fma(cc[2 * j - 1], x2, cc[2 * j - 2]);
-					const double y2 = fma(aa, y1, y0);
-					a[j * AA_LD] = y2;
-					y0 = y1; y1 = y2;
+			#pragma unroll
+			for (int u = 0; u < SPT; u++) {
+				const int sg = gsg + u * GPT, gks = k0 + sg * SEG;
+				if (sg >= NSG) break;
+				double y0 = ckn[u].x, y1 = ckn[u].y;
+				double* a = &As[sg * SEG][gtt];
+				a[0] = y0;
+				a[AA_LD] = y1;
+				if (gks < nk) {
+					const double* cc = cm + 2 * gks;
+					#pragma unroll
+					for (int j = 2; j < SEG; j++) {
+						const double aa = fma(cc[2 * j - 1], x2, cc[2 * j - 2]);
+						const double y2 = fma(aa, y1, y0);
+						a[j * AA_LD] = y2;
+						y0 = y1; y1 = y2;
+					}
+				} else {
+					for (int j = 2; j < SEG; j++) a[j * AA_LD] = 0.0;
 				}
-			} else {
-				for (int j = 2; j < SEG; j++) a[j * AA_LD] = 0.0;
 			}
 		}
 		#pragma unroll
@@ -548,17 +576,17 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 }
 
 // Single-plan kernels: blockIdx.y = order, blockIdx.x = (row tile, column tile).
-template <int SEG>
+template <int SEG, int WM>
 __global__ void __launch_bounds__(LG_THREADS, 3) leg_synth_kernel(LegParams p)
 {
-	const int ntb = (p.nlat_2 + LG_BM - 1) / LG_BM;
-	leg_synth_tile<SEG>(p, blockIdx.y, blockIdx.x % ntb, blockIdx.x / ntb);
+	const int ntb = (p.nlat_2 + 32 * WM - 1) / (32 * WM);
+	leg_synth_tile<SEG, WM>(p, blockIdx.y, blockIdx.x % ntb, blockIdx.x / ntb);
 }
 
-template <int SEG>
+template <int SEG, int WM>
 __global__ void __launch_bounds__(LG_THREADS, 3) leg_analys_kernel(LegParams p, int nkb)
 {
-	leg_analys_tile<SEG>(p, blockIdx.y, blockIdx.x % nkb, blockIdx.x / nkb);
+	leg_analys_tile<SEG, WM>(p, blockIdx.y, blockIdx.x % nkb, blockIdx.x / nkb);
 }
 
 // Persistent multi-plan kernels: CTAs (one wave) take work items (plan,
@@ -576,8 +604,8 @@ leg_multi_kernel(const LegParams* __restrict__ plist, const int4* __restrict__ w
 		__syncthreads();
 		if (w >= nwork) break;
 		const int4 it = work[w];
-		if (SYNTH) leg_synth_tile<SEG>(plist[it.x], it.y, it.z, it.w);
-		else leg_analys_tile<SEG>(plist[it.x], it.y, it.z, it.w);
+		if (SYNTH) leg_synth_tile<SEG, 2>(plist[it.x], it.y, it.z, it.w);
+		else leg_analys_tile<SEG, 2>(plist[it.x], it.y, it.z, it.w);
 	}
 }
 
@@ -608,29 +636,51 @@ void launch_prep_synth(const PrepParams& p, cudaStream_t st)
 	shtb_count_launch();
 }
 
-void launch_leg_synth(const LegParams& p, cudaStream_t st)
+namespace {
+
+template <int WM>
+void launch_leg_synth_wm(const LegParams& p, cudaStream_t st)
 {
-	const int ntb = (p.nlat_2 + LG_BM - 1) / LG_BM;
-	const int nnb = (p.ncol + LG_BN - 1) / LG_BN;
+	constexpr int BM = 32 * WM, BN = 16 * (8 / WM);
+	const int ntb = (p.nlat_2 + BM - 1) / BM;
+	const int nnb = (p.ncol + BN - 1) / BN;
 	dim3 grid(ntb * nnb, p.mlim + 1);
 	switch (p.ckseg) {
-		case 8: leg_synth_kernel<8><<<grid, LG_THREADS, 0, st>>>(p); break;
-		case 16: leg_synth_kernel<16><<<grid, LG_THREADS, 0, st>>>(p); break;
-		default: leg_synth_kernel<32><<<grid, LG_THREADS, 0, st>>>(p); break;
+		case 8: leg_synth_kernel<8, WM><<<grid, LG_THREADS, 0, st>>>(p); break;
+		case 16: leg_synth_kernel<16, WM><<<grid, LG_THREADS, 0, st>>>(p); break;
+		default: leg_synth_kernel<32, WM><<<grid, LG_THREADS, 0, st>>>(p); break;
 	}
+}
+
+template <int WM>
+void launch_leg_analys_wm(const LegParams& p, int kmax_all, cudaStream_t st)
+{
+	constexpr int BM = 32 * WM, BN = 16 * (8 / WM);
+	const int nkb = (kmax_all + BM - 1) / BM;
+	const int nnb = (p.ncol + BN - 1) / BN;
+	dim3 grid(nkb * nnb, p.mlim + 1);
+	switch (p.ckseg) {
+		case 8: leg_analys_kernel<8, WM><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
+		case 16: leg_analys_kernel<16, WM><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
+		default: leg_analys_kernel<32, WM><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
+	}
+}
+
+} // namespace
+
+// Calls with at most 32 GEMM columns (8 field-components) use the narrow
+// 128 x 32 tiles, which leave no column padding; wider calls the 64 x 64 ones.
+void launch_leg_synth(const LegParams& p, cudaStream_t st)
+{
+	if (p.ncol <= 32) launch_leg_synth_wm<4>(p, st);
+	else launch_leg_synth_wm<2>(p, st);
 	shtb_count_launch();
 }
 
 void launch_leg_analys(const LegParams& p, int kmax_all, cudaStream_t st)
 {
-	const int nkb = (kmax_all + LG_BM - 1) / LG_BM;
-	const int nnb = (p.ncol + LG_BN - 1) / LG_BN;
-	dim3 grid(nkb * nnb, p.mlim + 1);
-	switch (p.ckseg) {
-		case 8: leg_analys_kernel<8><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
-		case 16: leg_analys_kernel<16><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
-		default: leg_analys_kernel<32><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
-	}
+	if (p.ncol <= 32) launch_leg_analys_wm<4>(p, kmax_all, st);
+	else launch_leg_analys_wm<2>(p, kmax_all, st);
 	shtb_count_launch();
 }
 
