@@ -78,7 +78,11 @@ void cu_spat_to_SH_adjoint(shtns_cfg, cplx *Qg, double *Vg, int ltr);
 int shtns_b200_set_option(shtns_cfg, int option, int value);
 int shtns_b200_get_option(shtns_cfg, int option);
 
-/* Option 4 of shtns_b200_set_option: split-precision Legendre synthesis on
+/* Option 5 of shtns_b200_set_option: shape of the FP64 Legendre tiles, warps
+ * along the rows: 1 = 32 rows x 128 columns, 2 = 64 x 64, 4 = 128 x 32;
+ * 0 (default) picks 128 x 32 for calls with at most 32 GEMM columns (8
+ * field-components) and 64 x 64 otherwise.  Plan groups always use 64 x 64.
+ * Option 4 of shtns_b200_set_option: split-precision Legendre synthesis on
  * the FP16 tensor cores with 3, 4 or 5 balanced 8-bit slices per operand
  * (about 24, 32, 40 bits; products summed exactly in FP32 over windows of 256
  * steps and in FP64 across them); 0 (default) keeps the FP64 contraction.

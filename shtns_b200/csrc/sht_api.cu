@@ -70,7 +70,7 @@ LegParams leg_params(shtns_cfg s, const Job& j)
 	p.mpos_inv = 1.0 / s->mpos_renorm;
 	p.nphi = (double) s->nphi;
 	p.x = s->d_x; p.x2 = s->d_x2; p.sinv = s->d_sinv; p.w = s->d_w; p.c = s->d_c;
-	p.ck = s->d_ck; p.mt = s->mt; p.ckseg = s->ckseg;
+	p.ck = s->d_ck; p.mt = s->mt; p.ckseg = s->ckseg; p.tile_wm = s->tile_wm;
 	p.nf = j.nf;
 	for (int c = 0; c < 3; c++) p.ctype[c] = j.type[c];
 	p.qq = s->d_qq; p.F = s->d_F;

@@ -78,6 +78,7 @@ struct shtns_info {
 	int ckseg;                           // checkpoint spacing in k
 	int fft_pairs;                       // latitude pairs per FFT CTA (0: automatic)
 	int fft_generic;                     // 1: always use the generic mixed-radix FFT kernels
+	int tile_wm;                         // Legendre tile shape option (0 automatic)
 	std::vector<int> fft_radix;          // factorisation of nphi
 	double Y00_1, Y10_ct, Y11_st;
 	// device tables
@@ -124,6 +125,7 @@ struct LegParams {
 	int nlat, nlat_2, llim, mlim, mres, vec_extra;
 	int ncol, nfc;
 	int ckseg;                           // checkpoint spacing in k (8, 16 or 32)
+	int tile_wm;                         // Legendre tile: warps along the rows (1, 2, 4; 0 automatic)
 	int south_first, robert;
 	double mpos_inv;                     // analysis factor for m>0 (1/mpos_renorm)
 	int adjoint;                         // 1: adjoint transforms (see sht_api.cu)

@@ -577,14 +577,14 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 
 // Single-plan kernels: blockIdx.y = order, blockIdx.x = (row tile, column tile).
 template <int SEG, int WM>
-__global__ void __launch_bounds__(LG_THREADS, 3) leg_synth_kernel(LegParams p)
+__global__ void __launch_bounds__(LG_THREADS, WM == 1 ? 2 : 3) leg_synth_kernel(LegParams p)
 {
 	const int ntb = (p.nlat_2 + 32 * WM - 1) / (32 * WM);
 	leg_synth_tile<SEG, WM>(p, blockIdx.y, blockIdx.x % ntb, blockIdx.x / ntb);
 }
 
 template <int SEG, int WM>
-__global__ void __launch_bounds__(LG_THREADS, 3) leg_analys_kernel(LegParams p, int nkb)
+__global__ void __launch_bounds__(LG_THREADS, WM == 1 ? 2 : 3) leg_analys_kernel(LegParams p, int nkb)
 {
 	leg_analys_tile<SEG, WM>(p, blockIdx.y, blockIdx.x % nkb, blockIdx.x / nkb);
 }
@@ -668,19 +668,33 @@ void launch_leg_analys_wm(const LegParams& p, int kmax_all, cudaStream_t st)
 
 } // namespace
 
-// Calls with at most 32 GEMM columns (8 field-components) use the narrow
-// 128 x 32 tiles, which leave no column padding; wider calls the 64 x 64 ones.
+// Tile shape (p.tile_wm, warps along the rows): 1 = 32 x 128, 2 = 64 x 64,
+// 4 = 128 x 32.  Automatic (0): calls with at most 32 GEMM columns (8
+// field-components) use 128 x 32, which leaves no column padding; wider
+// calls 64 x 64.
+static int tile_wm(const LegParams& p)
+{
+	if (p.tile_wm == 1 || p.tile_wm == 2 || p.tile_wm == 4) return p.tile_wm;
+	return p.ncol <= 32 ? 4 : 2;
+}
+
 void launch_leg_synth(const LegParams& p, cudaStream_t st)
 {
-	if (p.ncol <= 32) launch_leg_synth_wm<4>(p, st);
-	else launch_leg_synth_wm<2>(p, st);
+	switch (tile_wm(p)) {
+		case 1: launch_leg_synth_wm<1>(p, st); break;
+		case 4: launch_leg_synth_wm<4>(p, st); break;
+		default: launch_leg_synth_wm<2>(p, st); break;
+	}
 	shtb_count_launch();
 }
 
 void launch_leg_analys(const LegParams& p, int kmax_all, cudaStream_t st)
 {
-	if (p.ncol <= 32) launch_leg_analys_wm<4>(p, kmax_all, st);
-	else launch_leg_analys_wm<2>(p, kmax_all, st);
+	switch (tile_wm(p)) {
+		case 1: launch_leg_analys_wm<1>(p, kmax_all, st); break;
+		case 4: launch_leg_analys_wm<4>(p, kmax_all, st); break;
+		default: launch_leg_analys_wm<2>(p, kmax_all, st); break;
+	}
 	shtb_count_launch();
 }
 

@@ -788,6 +788,10 @@ extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
 			if (value != 0 && value != 1 && value != 2 && value != 4) return -1;
 			s->fft_pairs = value;
 			return 0;
+		case 5:   // Legendre tile shape: warps along the rows (0 automatic)
+			if (value != 0 && value != 1 && value != 2 && value != 4) return -1;
+			s->tile_wm = value;
+			return 0;
 		case 4:   // split-precision synthesis: slices per operand (0 = FP64)
 			if (value != 0 && (value < 3 || value > 7)) return -1;
 			s->split_ns = value;
@@ -832,6 +836,7 @@ extern "C" int shtns_b200_get_option(shtns_cfg s, int option)
 		case 2: return s->ckseg;
 		case 3: return s->fft_generic;
 		case 4: return s->split_ns;
+		case 5: return s->tile_wm;
 		default: return -1;
 	}
 }

@@ -243,3 +243,23 @@ def test_float_device_transforms():
     assert lib.shtns_b200_status() == 0
     assert relerr(v64.cpu().numpy(), v32.double().cpu().numpy()) < 1e-6
     assert relerr(q64.cpu().numpy(), back.to(torch.complex128).cpu().numpy()) < 1e-6
+
+
+def test_legendre_tile_shapes_agree():
+    """Option 5 (Legendre tile shape: 32x128, 64x64, 128x32): the same sums in
+    the same order, so synthesis and analysis agree bit for bit."""
+    import shtns_b200
+    from shtns_b200 import capi
+    lib = capi.load()
+    dev = torch.device("cuda:0")
+    sh = shtns_b200.sht(255)
+    sh.set_grid(384, 768, flags=shtns_b200.sht_quick_init | shtns_b200.SHT_THETA_CONTIGUOUS, polar_opt=1e-10)
+    q = torch.from_numpy(rand_spec(255, 255, 1, 21, nfields=12)).to(dev)
+    outs = []
+    for wm in (2, 4, 1, 0):
+        assert lib.shtns_b200_set_option(sh._cfg, 5, wm) == 0
+        v = sh.synth(q)
+        outs.append((v, sh.analys(v)))
+    assert lib.shtns_b200_set_option(sh._cfg, 5, 3) == -1
+    for v, r in outs[1:]:
+        assert torch.equal(v, outs[0][0]) and torch.equal(r, outs[0][1])
