@@ -70,8 +70,8 @@ int shtns_b200_polar_rows(shtns_cfg, int* tm);
 void cu_SH_to_spat_adjoint(shtns_cfg, double *Vg, cplx *Qg, int ltr);
 void cu_spat_to_SH_adjoint(shtns_cfg, cplx *Qg, double *Vg, int ltr);
 
-/* Tuning options of a plan.  option 1: latitude pairs per FFT CTA (1, 2, 4;
- * 0 = automatic); option 2: recurrence checkpoint spacing (8, 16, 32; rebuilds
+/* Tuning options of a plan.  option 1: latitude pairs per FFT CTA (1, 2, 4,
+ * 8 where the fused chain's buffer fits; 0 = automatic); option 2: recurrence checkpoint spacing (8, 16, 32; rebuilds
  * the checkpoint table; not for clones or plans that have clones); option 3:
  * 1 = always use the generic mixed-radix FFT kernels.  Return 0 or -1.
  * No counterpart in SHTns 3.5.2. */

@@ -250,7 +250,7 @@ def _cache_path(path):
 def autotune(batch, reps=3, cache=None, use_cache=True, log=None):
     """Choose the options of an UnevenBatch by timing them on the device.
 
-    Search: for each bucket, latitude pairs per FFT CTA in {1, 2, 4}, timed on
+    Search: for each bucket, latitude pairs per FFT CTA in {1, 2, 4, 8}, timed on
     that bucket's batched transforms; then for the group, checkpoint spacing
     in {8, 16, 32} x work order {cost, natural} x CTAs per SM {2, 3}, timed on
     pair().  The choice is applied, cached (JSON, keyed by device name and the
@@ -278,7 +278,7 @@ def autotune(batch, reps=3, cache=None, use_cache=True, log=None):
             sh.synth_into([q], [v])
             sh.analys_into([v], [r])
         best = None
-        for S in (1, 2, 4):
+        for S in (1, 2, 4, 8):
             lib.shtns_b200_set_option(sh._cfg, 1, S)
             t = _time(run, reps)
             trials.append({"bucket": batch.buckets[b], "fft_pairs": S, "ms": t})

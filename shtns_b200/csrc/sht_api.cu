@@ -112,9 +112,12 @@ FftParams fft_params(shtns_cfg s, const Job& j)
 	while (S > 1 && fft_smem_bytes(s->nphi, S) > 112 * 1024) S /= 2;
 	int want = s->fft_pairs;
 	if (const char* e = getenv("SHTNS_B200_FFT_PAIRS")) want = atoi(e);
-	if (want == 1 || want == 2 || want == 4) {
+	if (want == 1 || want == 2 || want == 4 || want == 8) {
+		// fused chains keep one buffer, the generic kernels two
+		const bool fused = fft_fused_available(s->nphi) && !s->fft_generic;
 		S = want;
-		while (S > 1 && fft_smem_bytes(s->nphi, S) > 227 * 1024) S /= 2;
+		while (S > 1 && fft_smem_bytes(s->nphi, S) / (fused ? 2 : 1) > 227 * 1024) S /= 2;
+		if (!fused && S > 4) S = 4;
 	}
 	while (S > 1 && 2 * S > (int) s->nlat) S /= 2;
 	p.S = S;

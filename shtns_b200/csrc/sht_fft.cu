@@ -561,7 +561,10 @@ bool launch_fft3(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 template <int N>
 bool launch_fft3_n(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 {
-	// latitude pairs per CTA: up to 4 while the block stays at <= 768 threads
+	// latitude pairs per CTA: 8 (full 128-byte lines of a theta-contiguous
+	// grid, two butterflies per thread) where the buffer fits, else up to 4
+	// while the block stays at <= 768 threads
+	if constexpr (8 * (N + (N >> 3) + 1) * 16 <= 227 * 1024) if (p.S >= 8) return launch_fft3<N, 8>(p, nfc, st, synth);
 	if constexpr (4 * N / 8 <= 768) if (p.S >= 4) return launch_fft3<N, 4>(p, nfc, st, synth);
 	if constexpr (2 * N / 8 <= 768) if (p.S >= 2) return launch_fft3<N, 2>(p, nfc, st, synth);
 	return launch_fft3<N, 1>(p, nfc, st, synth);
@@ -594,6 +597,10 @@ void set_fused_limits()
 	if constexpr (4 * N / 8 <= 768) {
 		cudaFuncSetAttribute(fft3_synth_kernel<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 		cudaFuncSetAttribute(fft3_analys_kernel<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	}
+	if constexpr (8 * (N + (N >> 3) + 1) * 16 <= 227 * 1024) {
+		cudaFuncSetAttribute(fft3_synth_kernel<N, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+		cudaFuncSetAttribute(fft3_analys_kernel<N, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 	}
 }
 

@@ -540,7 +540,10 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 				er = w * (fn.x + fs.x);  ei = w * (fn.y + fs.y);
 				orr = wo * (fn.x - fs.x); oi = wo * (fn.y - fs.y);
 			}
-			const int cb = 16 * (fl >> 2) + 2 * (fl & 3);
+			// columns swizzled by row: bits 1-2 of the column XOR (row / 4) % 4, so
+			// that the 16 rows a half-warp stores hit distinct banks; the fragment
+			// loads read 4 consecutive rows (one swizzle) and stay conflict-free
+			const int cb = (16 * (fl >> 2) + 2 * (fl & 3)) ^ (2 * ((tt >> 2) & 3));
 			*reinterpret_cast<double2*>(&Bs[tt][cb]) = make_double2(er, ei);
 			*reinterpret_cast<double2*>(&Bs[tt][cb + 8]) = make_double2(orr, oi);
 		}
@@ -552,7 +555,7 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 			#pragma unroll
 			for (int i = 0; i < 4; i++) a[i] = As[wm * 32 + i * 8 + (lane >> 2)][kk + (lane & 3)];
 			#pragma unroll
-			for (int j = 0; j < 2; j++) b[j] = Bs[kk + (lane & 3)][wn * 16 + j * 8 + (lane >> 2)];
+			for (int j = 0; j < 2; j++) b[j] = Bs[kk + (lane & 3)][(wn * 16 + j * 8 + (lane >> 2)) ^ (2 * ((kk >> 2) & 3))];
 			#pragma unroll
 			for (int i = 0; i < 4; i++)
 				#pragma unroll

@@ -785,7 +785,7 @@ extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
 	if (!s) return -1;
 	switch (option) {
 		case 1:   // latitude pairs per FFT CTA
-			if (value != 0 && value != 1 && value != 2 && value != 4) return -1;
+			if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8) return -1;
 			s->fft_pairs = value;
 			return 0;
 		case 5:   // Legendre tile shape: warps along the rows (0 automatic)

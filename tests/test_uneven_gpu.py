@@ -118,11 +118,11 @@ def test_autotune_options_agree(small, tmp_path):
     path = str(tmp_path / "tune.json")
     rec = B.autotune(ub, reps=1, cache=path)
     assert set(rec["options"]) == {"fft_pairs", "ckseg", "order", "ctas_per_sm"}
-    assert len(rec["trials"]) == 3 * len(ub.plans) + 12
+    assert len(rec["trials"]) == 4 * len(ub.plans) + 12
     db = json.load(open(path))
     assert len(db) == 1 and list(db.values())[0]["options"] == rec["options"]
     for seg in (8, 16, 32):
-        for pairs in (1, 2, 4):
+        for pairs in (1, 2, 4, 8):
             ub.apply_options({"fft_pairs": [pairs] * len(ub.plans), "ckseg": seg, "order": 0, "ctas_per_sm": 3})
             ub.pair()
             torch.cuda.synchronize()
