@@ -137,6 +137,17 @@ void SHtor_to_spat(shtns_cfg, cplx *Tlm, double *Vt, double *Vp);
 void spat_to_SHqst(shtns_cfg, double *Vr, double *Vt, double *Vp, cplx *Qlm, cplx *Slm, cplx *Tlm);
 void SHqst_to_spat(shtns_cfg, cplx *Qlm, cplx *Slm, cplx *Tlm, double *Vr, double *Vt, double *Vp);
 /* truncated transforms (shtns.h:315-324) */
+/* Legendre transforms at one order m = |im|*mres, no FFT (shtns.h:329-342):
+ * spectral lmax+1-m coefficients of that order, spatial nlat complex values */
+void spat_to_SH_ml(shtns_cfg, int im, cplx *Vr, cplx *Ql, int ltr);                                  /* shtns.h:333 */
+void SH_to_spat_ml(shtns_cfg, int im, cplx *Ql, cplx *Vr, int ltr);                                  /* shtns.h:334 */
+void spat_to_SHsphtor_ml(shtns_cfg, int im, cplx *Vt, cplx *Vp, cplx *Sl, cplx *Tl, int ltr);        /* shtns.h:336 */
+void SHsphtor_to_spat_ml(shtns_cfg, int im, cplx *Sl, cplx *Tl, cplx *Vt, cplx *Vp, int ltr);        /* shtns.h:337 */
+void SHsph_to_spat_ml(shtns_cfg, int im, cplx *Sl, cplx *Vt, cplx *Vp, int ltr);                     /* shtns.h:338 */
+void SHtor_to_spat_ml(shtns_cfg, int im, cplx *Tl, cplx *Vt, cplx *Vp, int ltr);                     /* shtns.h:339 */
+void spat_to_SHqst_ml(shtns_cfg, int im, cplx *Vr, cplx *Vt, cplx *Vp, cplx *Ql, cplx *Sl, cplx *Tl, int ltr); /* shtns.h:341 */
+void SHqst_to_spat_ml(shtns_cfg, int im, cplx *Ql, cplx *Sl, cplx *Tl, cplx *Vr, cplx *Vt, cplx *Vp, int ltr); /* shtns.h:342 */
+
 void spat_to_SH_l(shtns_cfg, double *Vr, cplx *Qlm, int ltr);
 void SH_to_spat_l(shtns_cfg, cplx *Qlm, double *Vr, int ltr);
 void SHsphtor_to_spat_l(shtns_cfg, cplx *Slm, cplx *Tlm, double *Vt, double *Vp, int ltr);

@@ -112,6 +112,14 @@ PROTOTYPES = {
     "cu_SH_to_spat_adjoint": (None, [CFG, P, P, I]),
     "cu_spat_to_SH_adjoint": (None, [CFG, P, P, I]),
     "shtns_b200_set_option": (I, [CFG, I, I]),
+    "SH_to_spat_ml": (None, [CFG, I, P, P, I]),
+    "spat_to_SH_ml": (None, [CFG, I, P, P, I]),
+    "SHsphtor_to_spat_ml": (None, [CFG, I, P, P, P, P, I]),
+    "spat_to_SHsphtor_ml": (None, [CFG, I, P, P, P, P, I]),
+    "SHsph_to_spat_ml": (None, [CFG, I, P, P, P, I]),
+    "SHtor_to_spat_ml": (None, [CFG, I, P, P, P, I]),
+    "SHqst_to_spat_ml": (None, [CFG, I, P, P, P, P, P, P, I]),
+    "spat_to_SHqst_ml": (None, [CFG, I, P, P, P, P, P, P, I]),
     "shtns_b200_kernel_errors": (I, [CFG]),
     "shtns_b200_get_option": (I, [CFG, I]),
     "shtns_b200_group_create": (P, [I, P]),

@@ -645,3 +645,139 @@ extern "C" void shtns_b200_group_analys(shtns_group g, double** Vr, cplx** Qlm, 
 	}
 	check_launch("group analysis launch");
 }
+
+// ---------------------------------------------------------------------------
+// Legendre transforms of one order m = |im|*mres, no FFT (shtns.h:329-342,
+// sht_com.c:95-126; a negative im changes the sign of m in the vector terms,
+// fly_SH_to_spat.gen.c:294-296).  Host arrays: spectral lmax+1-m complex coefficients of
+// that order, spatial nlat complex values (the order's Fourier coefficient
+// per grid row: v = sum_m (2 - delta_m0) Re(V_m e^{i m phi})).  The pipeline
+// is the whole transform's prologue, Legendre and epilogue kernels launched
+// for the single order (im0 = mlim = im), with the plan's Fourier buffer as
+// the spatial side.
+namespace {
+
+long lm_first(shtns_cfg s, int im)   // LM(m, m), shtns.h:104-106
+{
+	return (long) im * (2 * s->lmax + 2 - (im + 1) * s->mres) / 2 + (long) im * s->mres;
+}
+
+template <class T> T* shifted(T* p, long n)   // p - n elements, for base[off + d] addressing
+{
+	return p ? reinterpret_cast<T*>(reinterpret_cast<uintptr_t>(p) - n * (long) sizeof(T)) : nullptr;
+}
+
+bool ml_job(shtns_cfg s, int im, int ncomp, const int* types, int ltr, Job& j)
+{
+	if (!s || !s->grid_set) { shtb_set_error(1, "transform on a plan without grid"); return false; }
+	if (im > s->mmax || -im > s->mmax) { shtb_set_error(1, "fixed-order transform: order index out of range"); return false; }
+	const int saved = s->batch;
+	s->batch = 1;
+	const bool ok = setup_job(s, j, ncomp, types, ltr);
+	s->batch = saved;
+	return ok;
+}
+
+void ml_synth(shtns_cfg s, int im, int ncomp, const int* types, const cplx* Q, const cplx* S, const cplx* T,
+              cplx* o0, cplx* o1, cplx* o2, int ltr)
+{
+	Job j;
+	if (!ml_job(s, im, ncomp, types, ltr, j)) return;
+	const int msign = im < 0 ? -1 : 1;           // scalar terms use |m|, vector terms the signed m
+	im = im < 0 ? -im : im;
+	const int m = im * s->mres, nl = s->lmax + 1 - m;
+	cplx* outs[3] = {o0, o1, o2};
+	if (m > j.llim) {
+		for (int c = 0; c < ncomp; c++) memset(outs[c], 0, sizeof(cplx) * s->nlat);
+		return;
+	}
+	cudaStream_t cs = s->comp_stream;
+	size_t cap = s->stage_cap;
+	if (!ensure(&s->d_stage, &cap, sizeof(double2) * 3 * (size_t) nl, "staging buffers")) { s->stage_cap = 0; return; }
+	s->stage_cap = cap;
+	double2* st = static_cast<double2*>(s->d_stage);
+	const cplx* ins[3] = {Q, S, T};
+	for (int c = 0; c < 3; c++)
+		if (ins[c]) cudaMemcpyAsync(st + c * nl, ins[c], sizeof(double2) * nl, cudaMemcpyHostToDevice, cs);
+	const long off = lm_first(s, im);
+	PrepParams pp = prep_params(s, j);
+	pp.im0 = im; pp.mlim = im; pp.spec_dist = nl; pp.msign = msign;
+	pp.Q = Q ? shifted<const double2>(st, off) : nullptr;
+	pp.S = S ? shifted<const double2>(st + nl, off) : nullptr;
+	pp.T = T ? shifted<const double2>(st + 2 * nl, off) : nullptr;
+	launch_prep_synth(pp, cs);
+	LegParams lp = leg_params(s, j);
+	lp.im0 = im; lp.mlim = im;
+	launch_leg_synth(lp, cs);
+	check_launch("fixed-order synthesis launch");
+	const long fstride = (long)(s->mmax + 1) * s->nlat;
+	for (int c = 0; c < ncomp; c++)
+		cudaMemcpyAsync(outs[c], s->d_F + c * fstride + (long) im * s->nlat, sizeof(double2) * s->nlat,
+		                cudaMemcpyDeviceToHost, cs);
+	shtb_cuda_ok(cudaStreamSynchronize(cs), "fixed-order synthesis");
+}
+
+void ml_analys(shtns_cfg s, int im, int ncomp, const int* types, const cplx* i0, const cplx* i1, const cplx* i2,
+               cplx* Qo, cplx* So, cplx* To, int ltr)
+{
+	Job j;
+	if (!ml_job(s, im, ncomp, types, ltr, j)) return;
+	const int msign = im < 0 ? -1 : 1;
+	im = im < 0 ? -im : im;
+	const int m = im * s->mres, nl = s->lmax + 1 - m;
+	cplx* outs[3] = {Qo, So, To};
+	if (m > j.llim) {
+		for (int c = 0; c < 3; c++) if (outs[c]) memset(outs[c], 0, sizeof(cplx) * nl);
+		return;
+	}
+	cudaStream_t cs = s->comp_stream;
+	const long fstride = (long)(s->mmax + 1) * s->nlat;
+	const cplx* ins[3] = {i0, i1, i2};
+	for (int c = 0; c < ncomp; c++)
+		cudaMemcpyAsync(s->d_F + c * fstride + (long) im * s->nlat, ins[c], sizeof(double2) * s->nlat,
+		                cudaMemcpyHostToDevice, cs);
+	LegParams lp = leg_params(s, j);
+	lp.im0 = im; lp.mlim = im;
+	launch_leg_analys(lp, (j.llim + j.vec_extra - m) / 2 + 1, cs);
+	size_t cap = s->stage_cap;
+	if (!ensure(&s->d_stage, &cap, sizeof(double2) * 3 * (size_t) nl, "staging buffers")) { s->stage_cap = 0; return; }
+	s->stage_cap = cap;
+	double2* st = static_cast<double2*>(s->d_stage);
+	const long off = lm_first(s, im);
+	PrepParams pp = prep_params(s, j);
+	pp.im0 = im; pp.mlim = im; pp.spec_dist = nl; pp.msign = msign;
+	pp.Qo = Qo ? shifted<double2>(st, off) : nullptr;
+	pp.So = So ? shifted<double2>(st + nl, off) : nullptr;
+	pp.To = To ? shifted<double2>(st + 2 * nl, off) : nullptr;
+	launch_post_analys_m(pp, im, cs);
+	check_launch("fixed-order analysis launch");
+	for (int c = 0; c < 3; c++)
+		if (outs[c]) cudaMemcpyAsync(outs[c], st + c * nl, sizeof(double2) * nl, cudaMemcpyDeviceToHost, cs);
+	shtb_cuda_ok(cudaStreamSynchronize(cs), "fixed-order analysis");
+}
+
+} // namespace
+
+extern "C" void SH_to_spat_ml(shtns_cfg s, int im, cplx* Ql, cplx* Vr, int ltr)
+{ ml_synth(s, im, 1, T_SCAL, Ql, nullptr, nullptr, Vr, nullptr, nullptr, ltr); }
+
+extern "C" void spat_to_SH_ml(shtns_cfg s, int im, cplx* Vr, cplx* Ql, int ltr)
+{ ml_analys(s, im, 1, T_SCAL, Vr, nullptr, nullptr, Ql, nullptr, nullptr, ltr); }
+
+extern "C" void SHsphtor_to_spat_ml(shtns_cfg s, int im, cplx* Sl, cplx* Tl, cplx* Vt, cplx* Vp, int ltr)
+{ ml_synth(s, im, 2, T_VEC, nullptr, Sl, Tl, Vt, Vp, nullptr, ltr); }
+
+extern "C" void spat_to_SHsphtor_ml(shtns_cfg s, int im, cplx* Vt, cplx* Vp, cplx* Sl, cplx* Tl, int ltr)
+{ ml_analys(s, im, 2, T_VEC, Vt, Vp, nullptr, nullptr, Sl, Tl, ltr); }
+
+extern "C" void SHsph_to_spat_ml(shtns_cfg s, int im, cplx* Sl, cplx* Vt, cplx* Vp, int ltr)
+{ ml_synth(s, im, 2, T_VEC, nullptr, Sl, nullptr, Vt, Vp, nullptr, ltr); }
+
+extern "C" void SHtor_to_spat_ml(shtns_cfg s, int im, cplx* Tl, cplx* Vt, cplx* Vp, int ltr)
+{ ml_synth(s, im, 2, T_VEC, nullptr, nullptr, Tl, Vt, Vp, nullptr, ltr); }
+
+extern "C" void SHqst_to_spat_ml(shtns_cfg s, int im, cplx* Ql, cplx* Sl, cplx* Tl, cplx* Vr, cplx* Vt, cplx* Vp, int ltr)
+{ ml_synth(s, im, 3, T_QST, Ql, Sl, Tl, Vr, Vt, Vp, ltr); }
+
+extern "C" void spat_to_SHqst_ml(shtns_cfg s, int im, cplx* Vr, cplx* Vt, cplx* Vp, cplx* Ql, cplx* Sl, cplx* Tl, int ltr)
+{ ml_analys(s, im, 3, T_QST, Vr, Vt, Vp, Ql, Sl, Tl, ltr); }

@@ -123,6 +123,7 @@ struct shtns_info {
 // ---- kernel parameter blocks ----
 struct LegParams {
 	int nlat, nlat_2, llim, mlim, mres, vec_extra;
+	int im0;                             // first order of the launch (orders im0..mlim; 0 for whole transforms)
 	int ncol, nfc;
 	int ckseg;                           // checkpoint spacing in k (8, 16 or 32)
 	int tile_wm;                         // Legendre tile: warps along the rows (1, 2, 4; 0 automatic)
@@ -142,6 +143,8 @@ struct LegParams {
 
 struct PrepParams {
 	int lmax, llim, mlim, mres, nf, ncomp, ncol, comp_type[3];   // comp_type: 0 scalar Q, 1 V (from S,T), 2 W (from S,T)
+	int im0;                             // first order of the launch (0 for whole transforms)
+	int msign;                           // -1: order -m in the vector terms (negative im of the _ml transforms)
 	const double2 *Q, *S, *T;            // spectral inputs (may be null: zeros)
 	double2 *Qo, *So, *To;               // spectral outputs (analysis)
 	long spec_dist;

@@ -105,7 +105,7 @@ __global__ void ck_kernel(int nlat_2, int mres, int seg, const double* __restric
 __global__ void __launch_bounds__(256) prep_synth_kernel(PrepParams p)
 {
 	__shared__ double2 win[2][PT_F][PT_W];
-	const int im = blockIdx.z;
+	const int im = p.im0 + blockIdx.z;
 	if (im > p.mlim) return;
 	const int m = im * p.mres;
 	const int kmax = (p.llim + 1 - m) / 2 + 1;
@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(256) prep_synth_kernel(PrepParams p)
 	}
 	__syncthreads();
 	const int voff = p.mt.voff[im];
-	const double em = (double) m;
+	const double em = (p.msign < 0) ? -(double) m : (double) m;   // signed m (negative orders of the _ml transforms)
 	for (int e = threadIdx.x; e < PT_K * PT_F; e += blockDim.x) {
 		const int kl = e / PT_F, fl = e - kl * PT_F;
 		const int k = k0 + kl, fc = fc0 + fl;
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 {
 	__shared__ double2 sv[PE_R][PE_F][2];     // first component of the group (Q, or V)
 	__shared__ double2 sw[PE_R][PE_F][2];     // second component (W) for the vector group
-	const int im = blockIdx.z;
+	const int im = p.im0 + blockIdx.z;
 	const int m = im * p.mres;
 	const int nl = p.lmax - m + 1;
 	const int j0 = blockIdx.x * PE_J;
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 	__syncthreads();
 	const double* X = p.xa + p.mt.xoff[im];
 	const int voff = p.mt.voff[im];
-	const double em = (double) m;
+	const double em = (p.msign < 0) ? -(double) m : (double) m;   // signed m (negative orders of the _ml transforms)
 	for (int e = threadIdx.x; e < PE_J * PE_F; e += blockDim.x) {
 		const int fl = e / PE_J, jl = e - fl * PE_J;
 		const int j = j0 + jl, f = f0 + fl;
@@ -578,18 +578,18 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 	}
 }
 
-// Single-plan kernels: blockIdx.y = order, blockIdx.x = (row tile, column tile).
+// Single-plan kernels: blockIdx.y = order - p.im0, blockIdx.x = (row tile, column tile).
 template <int SEG, int WM>
 __global__ void __launch_bounds__(LG_THREADS, WM == 1 ? 2 : 3) leg_synth_kernel(LegParams p)
 {
 	const int ntb = (p.nlat_2 + 32 * WM - 1) / (32 * WM);
-	leg_synth_tile<SEG, WM>(p, blockIdx.y, blockIdx.x % ntb, blockIdx.x / ntb);
+	leg_synth_tile<SEG, WM>(p, p.im0 + blockIdx.y, blockIdx.x % ntb, blockIdx.x / ntb);
 }
 
 template <int SEG, int WM>
 __global__ void __launch_bounds__(LG_THREADS, WM == 1 ? 2 : 3) leg_analys_kernel(LegParams p, int nkb)
 {
-	leg_analys_tile<SEG, WM>(p, blockIdx.y, blockIdx.x % nkb, blockIdx.x / nkb);
+	leg_analys_tile<SEG, WM>(p, p.im0 + blockIdx.y, blockIdx.x % nkb, blockIdx.x / nkb);
 }
 
 // Persistent multi-plan kernels: CTAs (one wave) take work items (plan,
@@ -634,7 +634,7 @@ void launch_prep_synth(const PrepParams& p, cudaStream_t st)
 {
 	const int nfc = p.nf * p.ncomp;
 	const int kmax0 = (p.llim + 1) / 2 + 1;
-	dim3 grid((kmax0 + PT_K - 1) / PT_K, (nfc + PT_F - 1) / PT_F, p.mlim + 1);
+	dim3 grid((kmax0 + PT_K - 1) / PT_K, (nfc + PT_F - 1) / PT_F, p.mlim + 1 - p.im0);
 	prep_synth_kernel<<<grid, 256, 0, st>>>(p);
 	shtb_count_launch();
 }
@@ -647,7 +647,7 @@ void launch_leg_synth_wm(const LegParams& p, cudaStream_t st)
 	constexpr int BM = 32 * WM, BN = 16 * (8 / WM);
 	const int ntb = (p.nlat_2 + BM - 1) / BM;
 	const int nnb = (p.ncol + BN - 1) / BN;
-	dim3 grid(ntb * nnb, p.mlim + 1);
+	dim3 grid(ntb * nnb, p.mlim + 1 - p.im0);
 	switch (p.ckseg) {
 		case 8: leg_synth_kernel<8, WM><<<grid, LG_THREADS, 0, st>>>(p); break;
 		case 16: leg_synth_kernel<16, WM><<<grid, LG_THREADS, 0, st>>>(p); break;
@@ -661,7 +661,7 @@ void launch_leg_analys_wm(const LegParams& p, int kmax_all, cudaStream_t st)
 	constexpr int BM = 32 * WM, BN = 16 * (8 / WM);
 	const int nkb = (kmax_all + BM - 1) / BM;
 	const int nnb = (p.ncol + BN - 1) / BN;
-	dim3 grid(nkb * nnb, p.mlim + 1);
+	dim3 grid(nkb * nnb, p.mlim + 1 - p.im0);
 	switch (p.ckseg) {
 		case 8: leg_analys_kernel<8, WM><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
 		case 16: leg_analys_kernel<16, WM><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
@@ -705,7 +705,7 @@ void launch_post_analys_m(const PrepParams& p, int mmax, cudaStream_t st)
 {
 	const int ngroups = (p.comp_type[0] == 0) ? 1 + (p.ncomp > 1 ? 1 : 0) : 1;
 	const int nft = (p.nf + PE_F - 1) / PE_F;
-	dim3 grid((p.lmax + 1 + PE_J - 1) / PE_J, nft * ngroups, mmax + 1);
+	dim3 grid((p.lmax + 1 + PE_J - 1) / PE_J, nft * ngroups, mmax + 1 - p.im0);
 	post_analys_kernel<<<grid, 256, 0, st>>>(p);
 	shtb_count_launch();
 }

@@ -314,3 +314,43 @@ class sht:
         else:
             L.cu_spat_to_SHqst(self._cfg, P[0], P[1], P[2], O[0], O[1], O[2], ltr)
         capi.check(L)
+
+    # ---------------- fixed order, no FFT (shtns_numpy.i:661-704) ----------------
+    def _ml_check(self, im, spec, spat):
+        self._need_grid()
+        nel = self.lmax + 1 - abs(int(im)) * self.mres
+        for a in spec:
+            if a.dtype != np.complex128 or a.size != nel or not a.flags.c_contiguous:
+                raise RuntimeError("spectral array of an order must be contiguous complex128 of size %d" % nel)
+        for a in spat:
+            if a.dtype != np.complex128 or a.size != self.nlat or not a.flags.c_contiguous:
+                raise RuntimeError("spatial array of an order must be contiguous complex128 of size nlat")
+
+    def _ml(self, fn, im, *arrays):
+        P = [a.ctypes.data_as(C.c_void_p) for a in arrays]
+        getattr(self._lib, fn)(self._cfg, int(im), *P, int(self.lmax))
+        capi.check(self._lib)
+
+    def spat_to_SH_m(self, Vr, Qlm, im):
+        self._ml_check(im, [Qlm], [Vr]); self._ml("spat_to_SH_ml", im, Vr, Qlm)
+
+    def SH_to_spat_m(self, Qlm, Vr, im):
+        self._ml_check(im, [Qlm], [Vr]); self._ml("SH_to_spat_ml", im, Qlm, Vr)
+
+    def spat_to_SHsphtor_m(self, Vt, Vp, Slm, Tlm, im):
+        self._ml_check(im, [Slm, Tlm], [Vt, Vp]); self._ml("spat_to_SHsphtor_ml", im, Vt, Vp, Slm, Tlm)
+
+    def SHsphtor_to_spat_m(self, Slm, Tlm, Vt, Vp, im):
+        self._ml_check(im, [Slm, Tlm], [Vt, Vp]); self._ml("SHsphtor_to_spat_ml", im, Slm, Tlm, Vt, Vp)
+
+    def SHsph_to_spat_m(self, Slm, Vt, Vp, im):
+        self._ml_check(im, [Slm], [Vt, Vp]); self._ml("SHsph_to_spat_ml", im, Slm, Vt, Vp)
+
+    def SHtor_to_spat_m(self, Tlm, Vt, Vp, im):
+        self._ml_check(im, [Tlm], [Vt, Vp]); self._ml("SHtor_to_spat_ml", im, Tlm, Vt, Vp)
+
+    def spat_to_SHqst_m(self, Vr, Vt, Vp, Qlm, Slm, Tlm, im):
+        self._ml_check(im, [Qlm, Slm, Tlm], [Vr, Vt, Vp]); self._ml("spat_to_SHqst_ml", im, Vr, Vt, Vp, Qlm, Slm, Tlm)
+
+    def SHqst_to_spat_m(self, Qlm, Slm, Tlm, Vr, Vt, Vp, im):
+        self._ml_check(im, [Qlm, Slm, Tlm], [Vr, Vt, Vp]); self._ml("SHqst_to_spat_ml", im, Qlm, Slm, Tlm, Vr, Vt, Vp)
