@@ -137,6 +137,15 @@ void SHtor_to_spat(shtns_cfg, cplx *Tlm, double *Vt, double *Vp);
 void spat_to_SHqst(shtns_cfg, double *Vr, double *Vt, double *Vp, cplx *Qlm, cplx *Slm, cplx *Tlm);
 void SHqst_to_spat(shtns_cfg, cplx *Qlm, cplx *Slm, cplx *Tlm, double *Vr, double *Vt, double *Vp);
 /* truncated transforms (shtns.h:315-324) */
+/* Complex-valued fields, mres = 1 (shtns.h:268-309): alm[LM_cplx(l, m)],
+ * -l <= m <= l, nlm_cplx coefficients; complex spatial arrays of nspat */
+void SH_to_spat_cplx(shtns_cfg, cplx *alm, cplx *z);                                               /* shtns.h:272 */
+void spat_cplx_to_SH(shtns_cfg, cplx *z, cplx *alm);                                               /* shtns.h:277 */
+void SHsphtor_to_spat_cplx(shtns_cfg, cplx *Slm, cplx *Tlm, cplx *Vt, cplx *Vp);                   /* shtns.h:294 */
+void spat_cplx_to_SHsphtor(shtns_cfg, cplx *Vt, cplx *Vp, cplx *Slm, cplx *Tlm);                   /* shtns.h:292 */
+void SHqst_to_spat_cplx(shtns_cfg, cplx *Qlm, cplx *Slm, cplx *Tlm, cplx *Vr, cplx *Vt, cplx *Vp); /* shtns.h:309 */
+void spat_cplx_to_SHqst(shtns_cfg, cplx *Vr, cplx *Vt, cplx *Vp, cplx *Qlm, cplx *Slm, cplx *Tlm); /* shtns.h:308 */
+
 /* Legendre transforms at one order m = |im|*mres, no FFT (shtns.h:329-342):
  * spectral lmax+1-m coefficients of that order, spatial nlat complex values */
 void spat_to_SH_ml(shtns_cfg, int im, cplx *Vr, cplx *Ql, int ltr);                                  /* shtns.h:333 */

@@ -112,6 +112,12 @@ PROTOTYPES = {
     "cu_SH_to_spat_adjoint": (None, [CFG, P, P, I]),
     "cu_spat_to_SH_adjoint": (None, [CFG, P, P, I]),
     "shtns_b200_set_option": (I, [CFG, I, I]),
+    "SH_to_spat_cplx": (None, [CFG, P, P]),
+    "spat_cplx_to_SH": (None, [CFG, P, P]),
+    "SHsphtor_to_spat_cplx": (None, [CFG, P, P, P, P]),
+    "spat_cplx_to_SHsphtor": (None, [CFG, P, P, P, P]),
+    "SHqst_to_spat_cplx": (None, [CFG, P, P, P, P, P, P]),
+    "spat_cplx_to_SHqst": (None, [CFG, P, P, P, P, P, P]),
     "SH_to_spat_ml": (None, [CFG, I, P, P, I]),
     "spat_to_SH_ml": (None, [CFG, I, P, P, I]),
     "SHsphtor_to_spat_ml": (None, [CFG, I, P, P, P, P, I]),

@@ -781,3 +781,231 @@ extern "C" void SHqst_to_spat_ml(shtns_cfg s, int im, cplx* Ql, cplx* Sl, cplx* 
 
 extern "C" void spat_to_SHqst_ml(shtns_cfg s, int im, cplx* Vr, cplx* Vt, cplx* Vp, cplx* Ql, cplx* Sl, cplx* Tl, int ltr)
 { ml_analys(s, im, 3, T_QST, Vr, Vt, Vp, Ql, Sl, Tl, ltr); }
+
+// ---------------------------------------------------------------------------
+// Complex-valued fields (shtns.h:268-309, sht_func.c:939-1210): z(theta, phi)
+// = sum_{l, -l<=m<=l} alm[LM_cplx(l, m)] Y_l^m, mres = 1.  Built from the
+// real-field pipeline with two fields per component: field A carries the
+// orders +m (A_lm = alm[l, m]; at m = 0 the real part), field B the orders -m
+// (B_lm = (-1)^m alm[l, -m], with -m in the vector terms; at m = 0 the
+// imaginary part).  The Legendre stage gives Q_{+m} (rows of A) and Q_{-m}
+// (rows of B); in Fourier space these become the order-m coefficients of
+// x = Re z and y = Im z,
+//   X_m = (Q_m + conj Q_{-m}) / 2,  Y_m = (-i Q_m + i conj Q_{-m}) / 2  (m > 0),
+// which the real FFT turns into the grids x and y, interleaved into z.  The
+// analysis runs the same steps backwards (Q_m = X_m + i Y_m,
+// Q_{-m} = conj X_m + i conj Y_m).
+namespace {
+
+__device__ __forceinline__ long lm_real_idx(int lmax, int im, int l)        // LM(l, m), mres = 1
+{
+	return (long) im * (2 * lmax + 1 - im) / 2 + l;
+}
+
+__device__ __forceinline__ long lm_cplx_idx(int lmax, int mmax, int l, int m)   // LM_cplx(l, m), shtns.h:114
+{
+	return (l <= mmax) ? (long) l * (l + 1) + m : (long) mmax * (2 * l - mmax) + l + m;
+}
+
+// alm (ncomp arrays of nlm_cplx) -> AB[comp][field][nlm]; grid (l blocks, im, comp)
+__global__ void cplx_gather_kernel(const double2* __restrict__ a0, const double2* __restrict__ a1,
+                                   const double2* __restrict__ a2, double2* __restrict__ ab, int lmax, int mmax, long nlm)
+{
+	const int im = blockIdx.y, c = blockIdx.z;
+	const int l = im + blockIdx.x * blockDim.x + threadIdx.x;
+	if (l > lmax) return;
+	const double2* a = (c == 0) ? a0 : (c == 1 ? a1 : a2);
+	const double2 p = a[lm_cplx_idx(lmax, mmax, l, im)];
+	double2 A, B;
+	if (im == 0) { A = make_double2(p.x, 0.0); B = make_double2(p.y, 0.0); }
+	else {
+		const double2 n = a[lm_cplx_idx(lmax, mmax, l, -im)];
+		A = p;
+		B = (im & 1) ? make_double2(-n.x, -n.y) : n;
+	}
+	const long r = lm_real_idx(lmax, im, l);
+	ab[(2L * c) * nlm + r] = A;
+	ab[(2L * c + 1) * nlm + r] = B;
+}
+
+// AB -> alm (inverse of the gather)
+__global__ void cplx_scatter_kernel(const double2* __restrict__ ab, double2* __restrict__ a0, double2* __restrict__ a1,
+                                    double2* __restrict__ a2, int lmax, int mmax, long nlm)
+{
+	const int im = blockIdx.y, c = blockIdx.z;
+	const int l = im + blockIdx.x * blockDim.x + threadIdx.x;
+	if (l > lmax) return;
+	double2* a = (c == 0) ? a0 : (c == 1 ? a1 : a2);
+	const long r = lm_real_idx(lmax, im, l);
+	const double2 A = ab[(2L * c) * nlm + r], B = ab[(2L * c + 1) * nlm + r];
+	if (im == 0) { a[lm_cplx_idx(lmax, mmax, l, 0)] = make_double2(A.x, B.x); return; }
+	a[lm_cplx_idx(lmax, mmax, l, im)] = A;
+	a[lm_cplx_idx(lmax, mmax, l, -im)] = (im & 1) ? make_double2(-B.x, -B.y) : B;
+}
+
+// Fourier rows: (Q_m, Q_{-m}) <-> (X_m, Y_m), in place in the (A, B) slots
+__global__ void cplx_fourier_kernel(double2* __restrict__ F, long fstride, int nlat, int mlim, int ncomp, int to_xy)
+{
+	const long n = (long)(mlim + 1) * nlat;
+	const long e = (long) blockIdx.x * blockDim.x + threadIdx.x;
+	const int c = blockIdx.y;
+	if (e >= n || c >= ncomp) return;
+	const int m = (int)(e / nlat);
+	double2* pa = F + (2L * c) * fstride + e;
+	double2* pb = F + (2L * c + 1) * fstride + e;
+	const double2 a = *pa, b = *pb;
+	if (m == 0) {
+		*pa = make_double2(a.x, 0.0);
+		*pb = make_double2(b.x, 0.0);
+	} else if (to_xy) {      // a = Q_m, b = Q_{-m}
+		*pa = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+		*pb = make_double2(0.5 * (a.y + b.y), 0.5 * (b.x - a.x));
+	} else {                 // a = X_m, b = Y_m
+		*pa = make_double2(a.x - b.y, a.y + b.x);
+		*pb = make_double2(a.x + b.y, b.x - a.y);
+	}
+}
+
+// z[i] = (x[i], y[i]) and back; grid (blocks over nspat, comp)
+__global__ void cplx_interleave_kernel(double2* __restrict__ z, long zdist, double* __restrict__ xy, long nspat, int to_z)
+{
+	const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nspat) return;
+	const int c = blockIdx.y;
+	double* x = xy + (2L * c) * nspat;
+	double* y = x + nspat;
+	double2* zc = z + c * zdist;
+	if (to_z) zc[i] = make_double2(x[i], y[i]);
+	else { const double2 v = zc[i]; x[i] = v.x; y[i] = v.y; }
+}
+
+struct CplxStage {
+	double2* alm;       // ncomp x nlm_cplx
+	double2* ab;        // ncomp x 2 x nlm
+	double* xy;         // ncomp x 2 x nspat
+	double2* z;         // ncomp x nspat
+};
+
+bool cplx_begin(shtns_cfg s, int ncomp, const int* types, Job& j, CplxStage& cs)
+{
+	if (!s || !s->grid_set) { shtb_set_error(1, "transform on a plan without grid"); return false; }
+	if (s->mres != 1) { shtb_set_error(1, "complex-valued transforms require mres = 1"); return false; }
+	const int saved = s->batch;
+	s->batch = 2;
+	const bool ok = setup_job(s, j, ncomp, types, s->lmax);
+	s->batch = saved;
+	if (!ok) return false;
+	const size_t nlmc = (size_t) s->nlm_cplx, nlm = s->nlm, nspat = s->nspat;
+	auto al = [](size_t b) { return (b + 255) & ~(size_t) 255; };
+	const size_t b_alm = al(sizeof(double2) * ncomp * nlmc), b_ab = al(sizeof(double2) * ncomp * 2 * nlm);
+	const size_t b_xy = al(sizeof(double) * ncomp * 2 * nspat), b_z = al(sizeof(double2) * ncomp * nspat);
+	size_t cap = s->stage_cap;
+	if (!ensure(&s->d_stage, &cap, b_alm + b_ab + b_xy + b_z, "staging buffers")) { s->stage_cap = 0; return false; }
+	s->stage_cap = cap;
+	char* b = static_cast<char*>(s->d_stage);
+	cs.alm = reinterpret_cast<double2*>(b);
+	cs.ab = reinterpret_cast<double2*>(b + b_alm);
+	cs.xy = reinterpret_cast<double*>(b + b_alm + b_ab);
+	cs.z = reinterpret_cast<double2*>(b + b_alm + b_ab + b_xy);
+	return true;
+}
+
+void cplx_synth(shtns_cfg s, int ncomp, const int* types, const cplx* const* alm, cplx* const* z)
+{
+	Job j;
+	CplxStage cs;
+	if (!cplx_begin(s, ncomp, types, j, cs)) return;
+	cudaStream_t st = s->comp_stream;
+	const long nlmc = s->nlm_cplx, nlm = s->nlm, nspat = s->nspat;
+	for (int c = 0; c < ncomp; c++)
+		cudaMemcpyAsync(cs.alm + c * nlmc, alm[c], sizeof(double2) * nlmc, cudaMemcpyHostToDevice, st);
+	dim3 gg((s->lmax + 1 + 127) / 128, s->mmax + 1, ncomp);
+	cplx_gather_kernel<<<gg, 128, 0, st>>>(cs.alm, cs.alm + nlmc, cs.alm + 2 * nlmc, cs.ab, s->lmax, s->mmax, nlm);
+	shtb_count_launch();
+	PrepParams pp = prep_params(s, j);
+	pp.spec_dist = nlm; pp.neg_from = 1;
+	const double2* comps[3] = {cs.ab, cs.ab + 2 * nlm, cs.ab + 4 * nlm};
+	if (ncomp == 1) pp.Q = comps[0];
+	else if (ncomp == 2) { pp.S = comps[0]; pp.T = comps[1]; }
+	else { pp.Q = comps[0]; pp.S = comps[1]; pp.T = comps[2]; }
+	launch_prep_synth(pp, st);
+	LegParams lp = leg_params(s, j);
+	launch_leg_synth(lp, st);
+	const long fstride = (long)(s->mmax + 1) * s->nlat;
+	dim3 gf((unsigned)(((long)(j.mlim + 1) * s->nlat + 255) / 256), ncomp);
+	cplx_fourier_kernel<<<gf, 256, 0, st>>>(s->d_F, fstride, s->nlat, j.mlim, ncomp, 1);
+	shtb_count_launch();
+	FftParams fp = fft_params(s, j);
+	fp.spat_dist = nspat;
+	for (int c = 0; c < ncomp; c++) fp.spat[c] = cs.xy + 2L * c * nspat;
+	fp.vec2 = aligned16(fp.spat[0], fp.spat[ncomp > 1 ? 1 : 0], fp.spat[ncomp > 2 ? 2 : 0], nspat);
+	launch_fft_synth(fp, j.nfc, st);
+	dim3 gi((unsigned)((nspat + 255) / 256), ncomp);
+	cplx_interleave_kernel<<<gi, 256, 0, st>>>(cs.z, nspat, cs.xy, nspat, 1);
+	shtb_count_launch();
+	check_launch("complex synthesis launch");
+	for (int c = 0; c < ncomp; c++)
+		cudaMemcpyAsync(z[c], cs.z + c * nspat, sizeof(double2) * nspat, cudaMemcpyDeviceToHost, st);
+	shtb_cuda_ok(cudaStreamSynchronize(st), "complex synthesis");
+}
+
+void cplx_analys(shtns_cfg s, int ncomp, const int* types, const cplx* const* z, cplx* const* alm)
+{
+	Job j;
+	CplxStage cs;
+	if (!cplx_begin(s, ncomp, types, j, cs)) return;
+	cudaStream_t st = s->comp_stream;
+	const long nlmc = s->nlm_cplx, nlm = s->nlm, nspat = s->nspat;
+	for (int c = 0; c < ncomp; c++)
+		cudaMemcpyAsync(cs.z + c * nspat, z[c], sizeof(double2) * nspat, cudaMemcpyHostToDevice, st);
+	dim3 gi((unsigned)((nspat + 255) / 256), ncomp);
+	cplx_interleave_kernel<<<gi, 256, 0, st>>>(cs.z, nspat, cs.xy, nspat, 0);
+	shtb_count_launch();
+	FftParams fp = fft_params(s, j);
+	fp.spat_dist = nspat;
+	for (int c = 0; c < ncomp; c++) fp.spat_in[c] = cs.xy + 2L * c * nspat;
+	fp.vec2 = aligned16(fp.spat_in[0], fp.spat_in[ncomp > 1 ? 1 : 0], fp.spat_in[ncomp > 2 ? 2 : 0], nspat);
+	launch_fft_analys(fp, j.nfc, st);
+	const long fstride = (long)(s->mmax + 1) * s->nlat;
+	dim3 gf((unsigned)(((long)(j.mlim + 1) * s->nlat + 255) / 256), ncomp);
+	cplx_fourier_kernel<<<gf, 256, 0, st>>>(s->d_F, fstride, s->nlat, j.mlim, ncomp, 0);
+	shtb_count_launch();
+	LegParams lp = leg_params(s, j);
+	int kmax_all = 0;
+	for (int im = 0; im <= j.mlim; im++) kmax_all = std::max(kmax_all, (j.llim + j.vec_extra - im) / 2 + 1);
+	launch_leg_analys(lp, kmax_all, st);
+	PrepParams pp = prep_params(s, j);
+	pp.spec_dist = nlm; pp.neg_from = 1;
+	double2* comps[3] = {cs.ab, cs.ab + 2 * nlm, cs.ab + 4 * nlm};
+	if (ncomp == 1) pp.Qo = comps[0];
+	else if (ncomp == 2) { pp.So = comps[0]; pp.To = comps[1]; }
+	else { pp.Qo = comps[0]; pp.So = comps[1]; pp.To = comps[2]; }
+	launch_post_analys_m(pp, s->mmax, st);
+	dim3 gg((s->lmax + 1 + 127) / 128, s->mmax + 1, ncomp);
+	cplx_scatter_kernel<<<gg, 128, 0, st>>>(cs.ab, cs.alm, cs.alm + nlmc, cs.alm + 2 * nlmc, s->lmax, s->mmax, nlm);
+	shtb_count_launch();
+	check_launch("complex analysis launch");
+	for (int c = 0; c < ncomp; c++)
+		cudaMemcpyAsync(alm[c], cs.alm + c * nlmc, sizeof(double2) * nlmc, cudaMemcpyDeviceToHost, st);
+	shtb_cuda_ok(cudaStreamSynchronize(st), "complex analysis");
+}
+
+} // namespace
+
+extern "C" void SH_to_spat_cplx(shtns_cfg s, cplx* alm, cplx* z)
+{ const cplx* a[1] = {alm}; cplx* o[1] = {z}; cplx_synth(s, 1, T_SCAL, a, o); }
+
+extern "C" void spat_cplx_to_SH(shtns_cfg s, cplx* z, cplx* alm)
+{ const cplx* i[1] = {z}; cplx* o[1] = {alm}; cplx_analys(s, 1, T_SCAL, i, o); }
+
+extern "C" void SHsphtor_to_spat_cplx(shtns_cfg s, cplx* Slm, cplx* Tlm, cplx* Vt, cplx* Vp)
+{ const cplx* a[2] = {Slm, Tlm}; cplx* o[2] = {Vt, Vp}; cplx_synth(s, 2, T_VEC, a, o); }
+
+extern "C" void spat_cplx_to_SHsphtor(shtns_cfg s, cplx* Vt, cplx* Vp, cplx* Slm, cplx* Tlm)
+{ const cplx* i[2] = {Vt, Vp}; cplx* o[2] = {Slm, Tlm}; cplx_analys(s, 2, T_VEC, i, o); }
+
+extern "C" void SHqst_to_spat_cplx(shtns_cfg s, cplx* Qlm, cplx* Slm, cplx* Tlm, cplx* Vr, cplx* Vt, cplx* Vp)
+{ const cplx* a[3] = {Qlm, Slm, Tlm}; cplx* o[3] = {Vr, Vt, Vp}; cplx_synth(s, 3, T_QST, a, o); }
+
+extern "C" void spat_cplx_to_SHqst(shtns_cfg s, cplx* Vr, cplx* Vt, cplx* Vp, cplx* Qlm, cplx* Slm, cplx* Tlm)
+{ const cplx* i[3] = {Vr, Vt, Vp}; cplx* o[3] = {Qlm, Slm, Tlm}; cplx_analys(s, 3, T_QST, i, o); }

@@ -145,6 +145,7 @@ struct PrepParams {
 	int lmax, llim, mlim, mres, nf, ncomp, ncol, comp_type[3];   // comp_type: 0 scalar Q, 1 V (from S,T), 2 W (from S,T)
 	int im0;                             // first order of the launch (0 for whole transforms)
 	int msign;                           // -1: order -m in the vector terms (negative im of the _ml transforms)
+	int neg_from;                        // > 0: fields f >= neg_from use -m in the vector terms (complex-field transforms)
 	const double2 *Q, *S, *T;            // spectral inputs (may be null: zeros)
 	double2 *Qo, *So, *To;               // spectral outputs (analysis)
 	long spec_dist;

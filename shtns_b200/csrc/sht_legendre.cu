@@ -140,6 +140,9 @@ __global__ void __launch_bounds__(256) prep_synth_kernel(PrepParams p)
 		const int k = k0 + kl, fc = fc0 + fl;
 		if (k >= kmax || fc >= nfc) continue;
 		const int type = p.comp_type[fc / p.nf];
+		// fields from neg_from on carry the order -m (complex-field transforms)
+		const int fld = fc - (fc / p.nf) * p.nf;
+		const double emf = (p.neg_from > 0 && fld >= p.neg_from) ? -em : em;
 		double2 q3[3];
 		#pragma unroll
 		for (int r = 0; r < 3; r++) {
@@ -155,9 +158,9 @@ __global__ void __launch_bounds__(256) prep_synth_kernel(PrepParams p)
 				const double2 sm = win[0][fl][i - 1], sp = win[0][fl][i + 1], s0 = win[0][fl][i];
 				const double2 tmn = win[1][fl][i - 1], tp = win[1][fl][i + 1], t0 = win[1][fl][i];
 				if (type == 1)   // V = stdt S + i m T
-					q3[r] = make_double2(lo * sm.x + hi * sp.x - em * t0.y, lo * sm.y + hi * sp.y + em * t0.x);
+					q3[r] = make_double2(lo * sm.x + hi * sp.x - emf * t0.y, lo * sm.y + hi * sp.y + emf * t0.x);
 				else             // W = -stdt T + i m S
-					q3[r] = make_double2(-(lo * tmn.x + hi * tp.x) - em * s0.y, -(lo * tmn.y + hi * tp.y) + em * s0.x);
+					q3[r] = make_double2(-(lo * tmn.x + hi * tp.x) - emf * s0.y, -(lo * tmn.y + hi * tp.y) + emf * s0.x);
 			}
 		}
 		const double* X = p.xs + p.mt.xoff[im] + 3 * k;
@@ -271,8 +274,9 @@ __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 			const double l2 = p.l2[l];
 			const double mxv_r = lo * vm.x + hi * vp.x, mxv_i = lo * vm.y + hi * vp.y;
 			const double mxw_r = lo * wm.x + hi * wp.x, mxw_i = lo * wm.y + hi * wp.y;
-			s = make_double2(-(mxv_r - em * w0.y) * l2, -(mxv_i + em * w0.x) * l2);
-			t = make_double2(-(-em * v0.y - mxw_r) * l2, -(em * v0.x - mxw_i) * l2);
+			const double emf = (p.neg_from > 0 && f >= p.neg_from) ? -em : em;   // order -m fields
+			s = make_double2(-(mxv_r - emf * w0.y) * l2, -(mxv_i + emf * w0.x) * l2);
+			t = make_double2(-(-emf * v0.y - mxw_r) * l2, -(emf * v0.x - mxw_i) * l2);
 			if (m == 0) { s.y = 0.0; t.y = 0.0; }
 		}
 		p.So[o] = s;

@@ -354,3 +354,58 @@ class sht:
 
     def SHqst_to_spat_m(self, Qlm, Slm, Tlm, Vr, Vt, Vp, im):
         self._ml_check(im, [Qlm, Slm, Tlm], [Vr, Vt, Vp]); self._ml("SHqst_to_spat_ml", im, Qlm, Slm, Tlm, Vr, Vt, Vp)
+
+    # ---------------- complex-valued fields (shtns_numpy.i:469-545) ----------------
+    def zidx(self, l, m):
+        """index l(l+1)+m of (l, m) in a complex-field expansion (lmax = mmax)"""
+        l = np.asarray(l)
+        m = np.asarray(m)
+        return l * (l + 1) + m
+
+    def _cplx_ready(self):
+        self._need_grid()
+        if self.lmax != self.mmax or self.mres != 1:
+            raise RuntimeError("complex SH requires lmax=mmax and mres=1.")
+
+    def synth_cplx(self, *arg):
+        """z = synth_cplx(zlm); zt, zp = synth_cplx(slm, tlm); zr, zt, zp =
+        synth_cplx(qlm, slm, tlm): complex-valued spatial fields from
+        (lmax+1)^2 complex coefficients each."""
+        self._cplx_ready()
+        n = len(arg)
+        if n < 1 or n > 3:
+            raise RuntimeError("1,2 or 3 arguments required.")
+        q = []
+        for a in arg:
+            a = np.ascontiguousarray(a)
+            if a.size != (self.lmax + 1) ** 2:
+                raise RuntimeError("spectral array has wrong size.")
+            if a.dtype != np.complex128:
+                raise RuntimeError("spectral array should be dtype=complex.")
+            q.append(a)
+        outs = [np.empty(self.spat_shape, dtype=np.complex128) for _ in range(n)]
+        fn = {1: "SH_to_spat_cplx", 2: "SHsphtor_to_spat_cplx", 3: "SHqst_to_spat_cplx"}[n]
+        getattr(self._lib, fn)(self._cfg, *[x.ctypes.data_as(C.c_void_p) for x in q + outs])
+        capi.check(self._lib)
+        return outs[0] if n == 1 else tuple(outs)
+
+    def analys_cplx(self, *arg):
+        """zlm = analys_cplx(z); slm, tlm = analys_cplx(zt, zp); qlm, slm, tlm =
+        analys_cplx(zr, zt, zp)."""
+        self._cplx_ready()
+        n = len(arg)
+        if n < 1 or n > 3:
+            raise RuntimeError("1,2 or 3 arguments required.")
+        v = []
+        for a in arg:
+            a = np.ascontiguousarray(a)
+            if a.shape != self.spat_shape:
+                raise RuntimeError("spatial array has wrong shape.")
+            if a.dtype != np.complex128:
+                raise RuntimeError("spatial array should be dtype=complex128.")
+            v.append(a)
+        outs = [np.empty((self.lmax + 1) ** 2, dtype=np.complex128) for _ in range(n)]
+        fn = {1: "spat_cplx_to_SH", 2: "spat_cplx_to_SHsphtor", 3: "spat_cplx_to_SHqst"}[n]
+        getattr(self._lib, fn)(self._cfg, *[x.ctypes.data_as(C.c_void_p) for x in v + outs])
+        capi.check(self._lib)
+        return outs[0] if n == 1 else tuple(outs)
