@@ -124,6 +124,29 @@ void shtns_b200_group_analys(shtns_group, double **Vr, cplx **Qlm, const int *nf
  * No counterpart in the reference. */
 void cu_SH_to_spat_noalloc(shtns_cfg, cplx *Qlm, double *Vr, int ltr);
 
+/* Order-split stages: one transform divided over processes (GPUs) by order.
+ * Synthesis: each process runs shtns_b200_legendre_synth for its orders
+ * m0..m1 over every grid row, the processes exchange Fourier rows (an
+ * all-to-all) so that each holds every order of its block of grid rows, and
+ * each runs shtns_b200_fourier_synth on its block.  Analysis runs
+ * shtns_b200_fourier_analys on the block, the exchange backwards, and
+ * shtns_b200_legendre_analys for the orders.  kind: 0 scalar (Q), 1
+ * spheroidal/toroidal (S, T; outputs theta, phi components), 2 Q, S, T.
+ * Fourier buffers (complex): on the Legendre side F[fc][im - m0][row] for the
+ * nlat grid rows; on the Fourier side F[fc][im][r] for im = 0..mmax and the
+ * nrows rows of the block (nrows even), fc = c * howmany + f for component c
+ * of field f (shtns_set_batch).  Spatial blocks hold nrows consecutive grid
+ * rows of each field in the plan's layout with nrows in place of nlat, fields
+ * nphi*nrows doubles apart.  Spectral arrays keep the full layout (field
+ * stride spec_dist); only orders m0..m1 are read or written.  Orders above
+ * ltr are not written on the Fourier side (nor read by the FFT); the Legendre
+ * analysis writes them as zero.  Device pointers; asynchronous on the plan's
+ * compute stream.  No counterpart in SHTns 3.5.2 (single-process only). */
+void shtns_b200_legendre_synth(shtns_cfg, int kind, cplx *Qlm, cplx *Slm, cplx *Tlm, cplx *F, int m0, int m1, int ltr);
+void shtns_b200_fourier_synth(shtns_cfg, int kind, cplx *F, double *V0, double *V1, double *V2, int nrows, int ltr);
+void shtns_b200_fourier_analys(shtns_cfg, int kind, double *V0, double *V1, double *V2, cplx *F, int nrows, int ltr);
+void shtns_b200_legendre_analys(shtns_cfg, int kind, cplx *F, cplx *Qlm, cplx *Slm, cplx *Tlm, int m0, int m1, int ltr);
+
 #ifdef __cplusplus
 }
 #endif

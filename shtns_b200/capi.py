@@ -133,6 +133,10 @@ PROTOTYPES = {
     "shtns_b200_group_set_option": (I, [P, I, I]),
     "shtns_b200_group_synth": (None, [P, P, P, P, I]),
     "shtns_b200_group_analys": (None, [P, P, P, P, I]),
+    "shtns_b200_legendre_synth": (None, [CFG, I, P, P, P, P, I, I, I]),
+    "shtns_b200_fourier_synth": (None, [CFG, I, P, P, P, P, I, I]),
+    "shtns_b200_fourier_analys": (None, [CFG, I, P, P, P, P, I, I]),
+    "shtns_b200_legendre_analys": (None, [CFG, I, P, P, P, P, I, I, I]),
 }
 
 _lib = None

@@ -36,7 +36,8 @@ struct Job {
 	int nf, nfc, ncol, llim, mlim, vec_extra;
 };
 
-bool setup_job(shtns_cfg s, Job& j, int ncomp, const int* types, int ltr)
+// bufs: 1 = coefficient buffer, 2 = Fourier buffer (both by default)
+bool setup_job(shtns_cfg s, Job& j, int ncomp, const int* types, int ltr, unsigned bufs = 3)
 {
 	if (!s || !s->grid_set) { shtb_set_error(1, "transform on a plan without grid"); return false; }
 	if (ltr < 0) { shtb_set_error(1, "negative truncation degree"); return false; }
@@ -53,10 +54,14 @@ bool setup_job(shtns_cfg s, Job& j, int ncomp, const int* types, int ltr)
 	size_t qq_bytes = sizeof(double) * (size_t) s->ktot * j.ncol;
 	size_t F_bytes = sizeof(double2) * (size_t) j.nfc * (s->mmax + 1) * s->nlat;
 	size_t cq = s->qq_cap * sizeof(double), cf = s->F_cap * sizeof(double2);
-	if (!ensure((void**) &s->d_qq, &cq, qq_bytes, "coefficient buffer")) { s->qq_cap = 0; return false; }
-	s->qq_cap = cq / sizeof(double);
-	if (!ensure((void**) &s->d_F, &cf, F_bytes, "Fourier buffer")) { s->F_cap = 0; return false; }
-	s->F_cap = cf / sizeof(double2);
+	if (bufs & 1) {
+		if (!ensure((void**) &s->d_qq, &cq, qq_bytes, "coefficient buffer")) { s->qq_cap = 0; return false; }
+		s->qq_cap = cq / sizeof(double);
+	}
+	if (bufs & 2) {
+		if (!ensure((void**) &s->d_F, &cf, F_bytes, "Fourier buffer")) { s->F_cap = 0; return false; }
+		s->F_cap = cf / sizeof(double2);
+	}
 	return true;
 }
 
@@ -92,8 +97,10 @@ PrepParams prep_params(shtns_cfg s, const Job& j)
 	return p;
 }
 
-FftParams fft_params(shtns_cfg s, const Job& j)
+// nrows: grid rows transformed (the plan's nlat, or a block of them)
+FftParams fft_params(shtns_cfg s, const Job& j, int nrows = 0)
 {
+	if (nrows <= 0) nrows = s->nlat;
 	FftParams p;
 	memset(&p, 0, sizeof(p));
 	p.N = s->nphi; p.nlat = s->nlat; p.mlim = j.mlim;
@@ -119,7 +126,7 @@ FftParams fft_params(shtns_cfg s, const Job& j)
 		while (S > 1 && fft_smem_bytes(s->nphi, S) / (fused ? 2 : 1) > 227 * 1024) S /= 2;
 		if (!fused && S > 4) S = 4;
 	}
-	while (S > 1 && 2 * S > (int) s->nlat) S /= 2;
+	while (S > 1 && 2 * S > nrows) S /= 2;
 	p.S = S;
 	p.tw = s->d_tw; p.F = s->d_F;
 	p.fstride = (long)(s->mmax + 1) * s->nlat;
@@ -1009,3 +1016,139 @@ extern "C" void SHqst_to_spat_cplx(shtns_cfg s, cplx* Qlm, cplx* Slm, cplx* Tlm,
 
 extern "C" void spat_cplx_to_SHqst(shtns_cfg s, cplx* Vr, cplx* Vt, cplx* Vp, cplx* Qlm, cplx* Slm, cplx* Tlm)
 { const cplx* i[3] = {Vr, Vt, Vp}; cplx* o[3] = {Qlm, Slm, Tlm}; cplx_analys(s, 3, T_QST, i, o); }
+
+// ---------------------------------------------------------------------------
+// Order-split stages: one transform divided over processes by order.  The
+// Legendre stages work on a range of orders m0..m1 over every grid row, the
+// Fourier (phi FFT) stages on a block of rows over every order; between them
+// the caller moves Fourier rows so that each process holds what its next stage
+// needs (an all-to-all when the processes are GPUs).  Buffers and pointers are
+// device memory; every call is enqueued on the plan's compute stream.
+//   Legendre-side Fourier buffer:  F[fc][im - m0][row], rows 0..nlat-1
+//   Fourier-side Fourier buffer:   F[fc][im][r], im 0..mmax, r 0..nrows-1
+// with fc = c * howmany + f for component c of field f.  Spatial blocks hold
+// nrows consecutive grid rows of each field in the plan's layout with nrows in
+// place of nlat (fields nphi*nrows doubles apart).  Spectral arrays keep the
+// plan's full layout (field stride spec_dist); only orders m0..m1 are read or
+// written.  Orders above the truncation ltr are not written on the Fourier
+// side and not read by the FFT; the Legendre analysis writes them as zero.
+namespace {
+
+bool kind_types(int kind, int* ncomp, const int** types)
+{
+	switch (kind) {
+		case 0: *ncomp = 1; *types = T_SCAL; return true;
+		case 1: *ncomp = 2; *types = T_VEC; return true;
+		case 2: *ncomp = 3; *types = T_QST; return true;
+		default: shtb_set_error(1, "order-split stage: kind must be 0 (scalar), 1 (sphtor) or 2 (qst)"); return false;
+	}
+}
+
+bool range_ok(shtns_cfg s, int m0, int m1, const void* F)
+{
+	if (m0 < 0 || m1 < m0 || m1 > s->mmax) { shtb_set_error(1, "order-split stage: invalid order range"); return false; }
+	if (!F) { shtb_set_error(1, "order-split stage: null Fourier buffer"); return false; }
+	return true;
+}
+
+bool rows_ok(shtns_cfg s, int nrows, const void* F)
+{
+	if (nrows <= 0 || nrows > (int) s->nlat || (nrows & 1)) {
+		shtb_set_error(1, "order-split stage: row count must be even and in 2..nlat");
+		return false;
+	}
+	if (!F) { shtb_set_error(1, "order-split stage: null Fourier buffer"); return false; }
+	return true;
+}
+
+} // namespace
+
+extern "C" void shtns_b200_legendre_synth(shtns_cfg s, int kind, cplx* Q, cplx* S, cplx* T, cplx* F,
+                                          int m0, int m1, int ltr)
+{
+	int nc; const int* ty;
+	Job j;
+	if (!kind_types(kind, &nc, &ty) || !setup_job(s, j, nc, ty, ltr, 1) || !range_ok(s, m0, m1, F)) return;
+	if (m0 > j.mlim) return;
+	const int mhi = std::min(m1, j.mlim);
+	PrepParams pp = prep_params(s, j);
+	pp.im0 = m0; pp.mlim = mhi;
+	pp.Q = reinterpret_cast<const double2*>(Q);
+	pp.S = reinterpret_cast<const double2*>(S);
+	pp.T = reinterpret_cast<const double2*>(T);
+	shtb_stage_begin(s, 0);
+	launch_prep_synth(pp, s->comp_stream);
+	shtb_stage_end(s);
+	LegParams lp = leg_params(s, j);
+	lp.im0 = m0; lp.mlim = mhi;
+	lp.F = shifted(reinterpret_cast<double2*>(F), (long) m0 * s->nlat);
+	lp.fstride = (long)(m1 - m0 + 1) * s->nlat;
+	shtb_stage_begin(s, 1);
+	launch_leg_synth(lp, s->comp_stream);
+	shtb_stage_end(s);
+	check_launch("order-split Legendre synthesis launch");
+}
+
+extern "C" void shtns_b200_fourier_synth(shtns_cfg s, int kind, cplx* F, double* V0, double* V1, double* V2,
+                                         int nrows, int ltr)
+{
+	int nc; const int* ty;
+	Job j;
+	if (!kind_types(kind, &nc, &ty) || !setup_job(s, j, nc, ty, ltr, 0) || !rows_ok(s, nrows, F)) return;
+	FftParams fp = fft_params(s, j, nrows);
+	fp.nlat = nrows;
+	fp.F = reinterpret_cast<double2*>(F);
+	fp.fstride = (long)(s->mmax + 1) * nrows;
+	fp.spat_dist = (long) s->nphi * nrows;
+	fp.spat[0] = V0; fp.spat[1] = V1; fp.spat[2] = V2;
+	fp.vec2 = aligned16(V0, V1, V2, fp.spat_dist);
+	shtb_stage_begin(s, 2);
+	launch_fft_synth(fp, j.nfc, s->comp_stream);
+	shtb_stage_end(s);
+	check_launch("order-split FFT synthesis launch");
+}
+
+extern "C" void shtns_b200_fourier_analys(shtns_cfg s, int kind, double* V0, double* V1, double* V2, cplx* F,
+                                          int nrows, int ltr)
+{
+	int nc; const int* ty;
+	Job j;
+	if (!kind_types(kind, &nc, &ty) || !setup_job(s, j, nc, ty, ltr, 0) || !rows_ok(s, nrows, F)) return;
+	FftParams fp = fft_params(s, j, nrows);
+	fp.nlat = nrows;
+	fp.F = reinterpret_cast<double2*>(F);
+	fp.fstride = (long)(s->mmax + 1) * nrows;
+	fp.spat_dist = (long) s->nphi * nrows;
+	fp.spat_in[0] = V0; fp.spat_in[1] = V1; fp.spat_in[2] = V2;
+	fp.vec2 = aligned16(V0, V1, V2, fp.spat_dist);
+	shtb_stage_begin(s, 3);
+	launch_fft_analys(fp, j.nfc, s->comp_stream);
+	shtb_stage_end(s);
+	check_launch("order-split FFT analysis launch");
+}
+
+extern "C" void shtns_b200_legendre_analys(shtns_cfg s, int kind, cplx* F, cplx* Q, cplx* S, cplx* T,
+                                           int m0, int m1, int ltr)
+{
+	int nc; const int* ty;
+	Job j;
+	if (!kind_types(kind, &nc, &ty) || !setup_job(s, j, nc, ty, ltr, 1) || !range_ok(s, m0, m1, F)) return;
+	if (m0 <= j.mlim) {
+		LegParams lp = leg_params(s, j);
+		lp.im0 = m0; lp.mlim = std::min(m1, j.mlim);
+		lp.F = shifted(reinterpret_cast<double2*>(F), (long) m0 * s->nlat);
+		lp.fstride = (long)(m1 - m0 + 1) * s->nlat;
+		shtb_stage_begin(s, 4);
+		launch_leg_analys(lp, (j.llim + j.vec_extra - m0 * s->mres) / 2 + 1, s->comp_stream);
+		shtb_stage_end(s);
+	}
+	PrepParams pp = prep_params(s, j);
+	pp.im0 = m0;
+	pp.Qo = reinterpret_cast<double2*>(Q);
+	pp.So = reinterpret_cast<double2*>(S);
+	pp.To = reinterpret_cast<double2*>(T);
+	shtb_stage_begin(s, 5);
+	launch_post_analys_m(pp, m1, s->comp_stream);
+	shtb_stage_end(s);
+	check_launch("order-split Legendre analysis launch");
+}
