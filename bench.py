@@ -625,6 +625,131 @@ def run_highdeg(args):
     print(json.dumps(line), flush=True)
 
 
+def run_ordersplit(args):
+    """One scalar field of lmax=4095 on the 6144 x 12288 grid divided over the
+    ranks by order (shtns_b200.ordersplit): each step is a synthesis and an
+    analysis, each with one all-to-all of Fourier rows (NCCL between GPUs; a
+    copy on one).  The total work is fixed as ranks are added (strong
+    scaling); value = field-pairs/s of the whole job, device-timed, max over
+    ranks."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    import shtns_b200
+    from shtns_b200 import capi
+    from shtns_b200.ordersplit import OrderSplit
+    from tests.common import rand_spec
+    lib = capi.load()
+    nf = args.fields if args.fields != NFIELDS else 1
+    sh = shtns_b200.sht(HD_L)
+    sh.set_grid(HD_NLAT, HD_NPHI, flags=shtns_b200.sht_quick_init | shtns_b200.SHT_THETA_CONTIGUOUS, polar_opt=EPS)
+    q = torch.from_numpy(rand_spec(HD_L, HD_L, 1, 400, power=1.0, nfields=nf)).to(dev)
+    sp = OrderSplit(sh, rank=rank, world=world)
+    out = {}
+
+    def step():
+        v = sp.synth(q)
+        out["q"] = sp.analys(v)
+
+    def sync_all():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    sync_all()
+    steps = max(3, min(args.steps, 20))
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    n0 = lib.shtns_b200_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    e1.synchronize()
+    launches = lib.shtns_b200_launch_count() - n0
+    sync_all()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / steps
+    sl = sp.spec_slice()
+    err = float((out["q"][..., sl] - q[..., sl]).abs().max() / q.abs().max())
+    # stage times of this rank (one more step, timed per stage)
+    lib.shtns_b200_set_timing(sh._cfg, 1)
+    step()
+    torch.cuda.synchronize()
+    st = np.zeros(6)
+    ca = np.zeros(6, dtype=np.int64)
+    lib.shtns_b200_stage_times(sh._cfg, st.ctypes.data_as(C.c_void_p), ca.ctypes.data_as(C.c_void_p))
+    lib.shtns_b200_set_timing(sh._cfg, 0)
+    tm = np.zeros(HD_L + 1, dtype=np.int32)
+    lib.shtns_b200_polar_rows(sh._cfg, tm.ctypes.data_as(C.c_void_p))
+    ims = np.arange(sp.m0, sp.m1 + 1)
+    flops = 8.0 * float(((HD_NLAT // 2 - tm[ims]) * ((HD_L - ims) // 2 + 1)).sum()) * nf
+    whole_ms = None
+    if world == 1:
+        # the same field through the whole-field transform, for the cost of the split
+        v = torch.empty((nf,) + sh.spat_shape, dtype=torch.float64, device=dev)
+        r = torch.empty_like(q)
+        for _ in range(2):
+            sh.synth_into([q], [v])
+            sh.analys_into([v], [r])
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            sh.synth_into([q], [v])
+            sh.analys_into([v], [r])
+        e1.record()
+        e1.synchronize()
+        whole_ms = e0.elapsed_time(e1) / steps
+    if world > 1:
+        t = torch.tensor([ms, err], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, err = float(t[0]), float(t[1])
+    if rank == 0:
+        peak = fp64_gemm_peak(torch, dev)
+        ach = flops / (st[1] * 1e-3) / 1e12
+        fourier_bytes = 16.0 * (HD_L + 1) * HD_NLAT * nf
+        line = {
+            "metric": METRIC, "value": nf / (ms * 1e-3), "unit": HD_UNIT.replace("lmax=4095", "one field, lmax=4095"),
+            "n_gpus": world, "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded N(0,1)/(l+1))",
+            "config": {"workload": "lmax4095_1field_ordersplit", "lmax": HD_L, "nlat": HD_NLAT, "nphi": HD_NPHI,
+                       "fields": nf, "polar_eps": EPS, "layout": "theta-contiguous",
+                       "parallelism": "orders split over %d rank(s), one all-to-all per direction" % world,
+                       "orders_per_rank": [b - a + 1 for a, b in sp.orders],
+                       "exchange_bytes_per_step": 2 * fourier_bytes * (world - 1) / max(world, 1),
+                       "l2": "no flush: per-step working set > 2 GB > 126 MB L2"},
+            "stages_rank0_ms": {"legendre_synthesis": st[1], "fft_synthesis": st[2], "fft_analysis": st[3],
+                                "legendre_analysis": st[4], "prologue": st[0], "epilogue": st[5]},
+            "roofline": {"kernel": "leg_synth_simt_kernel (FP64 FMA: one field), rank 0's orders", "bound": "fp64",
+                         "achieved": ach,
+                         "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+                         "work_per_launch": "8 flop per theta-row x field-component x Ishioka step (the "
+                                            "recurrence's 4 more are not counted)",
+                         "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (the FP64 FMA pipe has "
+                                        "the same nominal rate on B200)"},
+            "roundtrip_relerr": err,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        if whole_ms is not None:
+            line["whole_field_pair_ms"] = whole_ms
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -636,15 +761,18 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-chunks", type=int, default=E2E_CHUNKS,
                     help="field chunks (streams) of the end-to-end step")
-    ap.add_argument("--workload", default="qst", choices=["qst", "uneven", "highdeg"],
+    ap.add_argument("--workload", default="qst", choices=["qst", "uneven", "highdeg", "ordersplit"],
                     help="qst: lmax=511 vector transforms of 64 fields (default); "
                          "uneven: 256 scalar fields of lmax 63..1023 through a plan group; "
-                         "highdeg: lmax=4095, 8 fields, FP64 and split-precision synthesis")
+                         "highdeg: lmax=4095, 8 fields, FP64 and split-precision synthesis; "
+                         "ordersplit: one lmax=4095 field divided over the ranks by order")
     args = ap.parse_args()
     if args.workload == "uneven" and args.impl != "reference":
         run_uneven(args)
     elif args.workload == "highdeg" and args.impl != "reference":
         run_highdeg(args)
+    elif args.workload == "ordersplit" and args.impl != "reference":
+        run_ordersplit(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

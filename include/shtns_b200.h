@@ -79,8 +79,11 @@ int shtns_b200_set_option(shtns_cfg, int option, int value);
 int shtns_b200_get_option(shtns_cfg, int option);
 
 /* Option 5 of shtns_b200_set_option: shape of the FP64 Legendre tiles, warps
- * along the rows: 1 = 32 rows x 128 columns, 2 = 64 x 64, 4 = 128 x 32;
- * 0 (default) picks 128 x 32 for calls with at most 32 GEMM columns (8
+ * along the rows: 1 = 32 rows x 128 columns, 2 = 64 x 64, 4 = 128 x 32,
+ * 8 = SIMT kernels (FP64 FMA, recurrence in registers; calls with 1 to 4
+ * field-components, others fall back to the automatic choice); 0 (default)
+ * picks the SIMT kernels for at most 4 field-components in the synthesis and
+ * 3 in the analysis, 128 x 32 for calls with at most 32 GEMM columns (8
  * field-components) and 64 x 64 otherwise.  Plan groups always use 64 x 64.
  * Option 4 of shtns_b200_set_option: split-precision Legendre synthesis on
  * the FP16 tensor cores with 3, 4 or 5 balanced 8-bit slices per operand

@@ -176,6 +176,9 @@ void launch_post_analys_m(const PrepParams& p, int mmax, cudaStream_t st);
 void launch_leg_synth(const LegParams& p, cudaStream_t st);
 void launch_leg_analys(const LegParams& p, int kmax_all, cudaStream_t st);
 void launch_leg_synth_split(shtns_cfg s, const LegParams& p, cudaStream_t st);
+bool leg_simt_selected(const LegParams& p, bool synth);
+void launch_leg_synth_simt(const LegParams& p, cudaStream_t st);
+void launch_leg_analys_simt(const LegParams& p, int kmax_all, cudaStream_t st);
 void free_split(shtns_cfg s);
 void launch_leg_multi(const LegParams* d_plist, const int4* d_work, int nwork, int* d_counter, int ckseg, bool synth,
                       int nctas, cudaStream_t st);

@@ -687,6 +687,7 @@ static int tile_wm(const LegParams& p)
 
 void launch_leg_synth(const LegParams& p, cudaStream_t st)
 {
+	if (leg_simt_selected(p, true)) { launch_leg_synth_simt(p, st); shtb_count_launch(); return; }
 	switch (tile_wm(p)) {
 		case 1: launch_leg_synth_wm<1>(p, st); break;
 		case 4: launch_leg_synth_wm<4>(p, st); break;
@@ -697,6 +698,7 @@ void launch_leg_synth(const LegParams& p, cudaStream_t st)
 
 void launch_leg_analys(const LegParams& p, int kmax_all, cudaStream_t st)
 {
+	if (leg_simt_selected(p, false)) { launch_leg_analys_simt(p, kmax_all, st); shtb_count_launch(); return; }
 	switch (tile_wm(p)) {
 		case 1: launch_leg_analys_wm<1>(p, kmax_all, st); break;
 		case 4: launch_leg_analys_wm<4>(p, kmax_all, st); break;

@@ -788,8 +788,8 @@ extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
 			if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8) return -1;
 			s->fft_pairs = value;
 			return 0;
-		case 5:   // Legendre tile shape: warps along the rows (0 automatic)
-			if (value != 0 && value != 1 && value != 2 && value != 4) return -1;
+		case 5:   // Legendre tile shape: warps along the rows, 8 = SIMT kernels (0 automatic)
+			if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8) return -1;
 			s->tile_wm = value;
 			return 0;
 		case 4:   // split-precision synthesis: slices per operand (0 = FP64)

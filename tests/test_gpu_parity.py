@@ -263,3 +263,58 @@ def test_legendre_tile_shapes_agree():
     assert lib.shtns_b200_set_option(sh._cfg, 5, 3) == -1
     for v, r in outs[1:]:
         assert torch.equal(v, outs[0][0]) and torch.equal(r, outs[0][1])
+
+
+@pytest.mark.parametrize("case", ["scalar1", "scalar2", "scalar3", "scalar4", "qst_mres2", "sphtor_south_robert",
+                                  "scalar1_l2047"])
+def test_simt_legendre_matches_tensor_tiles(case):
+    """Option 5 = 8 (SIMT kernels, 1-4 field-components) against the tensor-core
+    tiles (option 5 = 2) on the same plan: synthesis, analysis and the scalar
+    adjoints agree to rounding (different summation order)."""
+    import ctypes as C
+    import shtns_b200
+    from shtns_b200 import capi
+    lib = capi.load()
+    dev = torch.device("cuda:0")
+    lmax, mmax, mres, nlat, nphi, nf, kind = 255, 255, 1, 384, 768, 1, 0
+    flags = shtns_b200.sht_quick_init | shtns_b200.SHT_THETA_CONTIGUOUS
+    robert = False
+    if case.startswith("scalar") and case[6:].isdigit():
+        nf = int(case[6:])
+    elif case == "qst_mres2":
+        lmax, mmax, mres, nlat, nphi, nf, kind = 191, 60, 2, 288, 384, 1, 2
+        flags = shtns_b200.sht_quick_init | shtns_b200.SHT_PHI_CONTIGUOUS
+    elif case == "sphtor_south_robert":
+        nf, kind, robert = 2, 1, True
+        flags |= shtns_b200.SHT_SOUTH_POLE_FIRST
+    elif case == "scalar1_l2047":
+        lmax, mmax, nlat, nphi = 2047, 2047, 3072, 6144
+    sh = shtns_b200.sht(lmax, mmax, mres)
+    sh.set_grid(nlat, nphi, flags=flags, polar_opt=1e-10)
+    if robert:
+        sh.robert_form(1)
+    ncomp = {0: 1, 1: 2, 2: 3}[kind]
+    specs = [torch.from_numpy(rand_spec(lmax, mmax, mres, 40 + i, nfields=nf, zero_l0=(kind > 0))).to(dev)
+             for i in range(ncomp)]
+    res = {}
+    for opt in (2, 8):
+        assert lib.shtns_b200_set_option(sh._cfg, 5, opt) == 0
+        v = sh.synth(*specs)
+        v = list(v) if isinstance(v, tuple) else [v]
+        back = sh.analys(*v)
+        back = list(back) if isinstance(back, tuple) else [back]
+        res[opt] = (v, back)
+        if kind == 0 and nf == 1:
+            g = torch.empty_like(specs[0])
+            lib.cu_SH_to_spat_adjoint(sh._cfg, C.c_void_p(v[0].data_ptr()), C.c_void_p(g.data_ptr()), lmax)
+            h = torch.empty_like(v[0])
+            lib.cu_spat_to_SH_adjoint(sh._cfg, C.c_void_p(specs[0].data_ptr()), C.c_void_p(h.data_ptr()), lmax)
+            torch.cuda.synchronize()
+            res[opt] += (g, h)
+    for a, b in zip(res[2][0] + res[2][1], res[8][0] + res[8][1]):
+        assert relerr(a.cpu().numpy(), b.cpu().numpy()) < 1e-13
+    if len(res[2]) > 2:
+        for a, b in zip(res[2][2:], res[8][2:]):
+            assert relerr(a.cpu().numpy(), b.cpu().numpy()) < 1e-13
+    for a, b in zip(specs, res[8][1]):
+        assert relerr(a.cpu().numpy(), b.cpu().numpy()) < 1e-11
