@@ -287,6 +287,155 @@ __global__ void __launch_bounds__(SA_NT) leg_analys_simt_kernel(LegParams p)
 	}
 }
 
+// ---------------------------------------------------------------------------
+// Analysis of one field-component with the partial sums in registers.
+// CTA = (order, block of 16 k), 64 threads; every thread takes north rows
+// tmm + tid, tmm + tid + 64, ... and for each runs the recurrence over the
+// block (from the checkpoint of its segment, advancing to the block start
+// when the block starts inside a segment) and accumulates Y_k G for its rows:
+// 4 x 16 = 64 sums per thread.  They are reduced once per CTA: a butterfly
+// reduce-scatter inside each warp (lane L ends with sums 2L and 2L+1), then
+// across the two warps in shared memory.  Measured on B200 against the
+// shared-memory kernel above: faster for one component when the checkpoints
+// are 16 or 32 apart or the grid has at most 1024 rows (2x at lmax 127, 1.5x at
+// 511, 1.15x at 4095), slower at lmax 1023 (checkpoints 8 apart) and for two
+// components.
+#define SR_NT 64
+#define SR_NV 64                       // partial sums per thread
+
+template <int SEG>
+__global__ void __launch_bounds__(SR_NT) leg_analys_reg_kernel(LegParams p)
+{
+	constexpr int NFC = 1;
+	constexpr int KB = 16;                             // k per block
+	constexpr int NSB = (KB > SEG) ? KB / SEG : 1;     // checkpoints per row and block
+	constexpr int NC = SEG + KB + 2;                   // recurrence constants staged per block
+	__shared__ double2 cs[NC];
+	__shared__ double red[SR_NT / 32][SR_NV];
+	constexpr int nt = SR_NT;
+	const int im = p.im0 + blockIdx.y;
+	const int m = im * p.mres;
+	const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
+	const int kb0 = blockIdx.x * KB;
+	if (kb0 >= nk) return;
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const int tmm = p.mt.tm[im];
+	const int s0 = (kb0 / SEG) * SEG;                  // first segment start of the block
+	const double* cm = p.c + p.mt.coff[im];
+	for (int i = tid; i < NC; i += nt) {
+		const int k = s0 + i;
+		cs[i] = (k >= 2 && k < nk) ? make_double2(__ldg(cm + 2 * k - 2), __ldg(cm + 2 * k - 1)) : make_double2(0.0, 0.0);
+	}
+	__syncthreads();
+	const double2* ckm = p.ck + (long)p.mt.ckoff[im] * p.nlat_2;
+	const double wfac = (m > 0) ? p.mpos_inv : 1.0;
+	double v[SR_NV];
+	#pragma unroll
+	for (int i = 0; i < SR_NV; i++) v[i] = 0.0;
+
+	// the loads of row t + 128 are issued before the work of row t
+	double2 nfn[NFC], nfs[NFC], nck[NSB];
+	double nw = 0.0, nx = 0.0, nx2 = 0.0, nsv = 0.0;
+	auto load_row = [&](int t) {
+		if (t >= p.nlat_2) return;
+		const int rn = p.south_first ? p.nlat - 1 - t : t;
+		const int rs = p.nlat - 1 - rn;
+		#pragma unroll
+		for (int f = 0; f < NFC; f++) {
+			const double2* Ff = p.F + (long)f * p.fstride + (long)im * p.nlat;
+			nfn[f] = __ldg(Ff + rn);
+			nfs[f] = __ldg(Ff + rs);
+		}
+		#pragma unroll
+		for (int b = 0; b < NSB; b++) {
+			const int ks = (NSB > 1) ? kb0 + b * SEG : s0;
+			nck[b] = (ks < nk) ? __ldg(ckm + (long)(ks / SEG) * p.nlat_2 + t) : make_double2(0.0, 0.0);
+		}
+		nw = p.adjoint ? 0.0 : __ldg(p.w + t);
+		nx = __ldg(p.x + t);
+		nx2 = __ldg(p.x2 + t);
+		nsv = __ldg(p.sinv + t);
+	};
+	load_row(tmm + tid);
+	for (int t = tmm + tid; t < p.nlat_2; t += nt) {
+		// G of this row: w (F_N + F_S), w cos (F_N - F_S) per field-component
+		double g[NFC][4];
+		const double x2 = nx2;
+		double2 ckr[NSB];
+		#pragma unroll
+		for (int f = 0; f < NFC; f++) {
+			double w = p.adjoint ? p.nphi * (m > 0 ? 2.0 : 1.0) : nw * wfac;
+			if (p.ctype[f / p.nf] != 0) {
+				double sv = nsv;
+				if (p.robert) sv *= sv;
+				w *= sv;
+			}
+			const double wo = w * nx;
+			const double2 fn = nfn[f], fs = nfs[f];
+			g[f][0] = w * (fn.x + fs.x);  g[f][1] = w * (fn.y + fs.y);
+			g[f][2] = wo * (fn.x - fs.x); g[f][3] = wo * (fn.y - fs.y);
+		}
+		#pragma unroll
+		for (int b = 0; b < NSB; b++) ckr[b] = nck[b];
+		load_row(t + nt);
+		#pragma unroll
+		for (int b = 0; b < NSB; b++) {
+			const int ks = (NSB > 1) ? kb0 + b * SEG : s0;           // segment start
+			if (ks >= nk) break;
+			const double2 ck = ckr[b];
+			double ya = ck.x, yb = ck.y;                               // Y_ks, Y_ks+1
+			int ci = ks - s0 + 2;                                      // constants of Y_{ks+2}
+			if (NSB == 1) {
+				// advance from the segment start to the block start
+				for (int k = ks; k < kb0; k++, ci++) {
+					const double2 c = cs[ci];
+					const double y2 = fma(fma(c.y, x2, c.x), yb, ya);
+					ya = yb; yb = y2;
+				}
+			}
+			constexpr int JN = (NSB > 1) ? SEG : KB;
+			#pragma unroll
+			for (int jj = 0; jj < JN; jj++) {
+				const int j = b * JN + jj;                             // k = kb0 + j
+				#pragma unroll
+				for (int f = 0; f < NFC; f++) {
+					#pragma unroll
+					for (int u = 0; u < 4; u++) v[(j * NFC + f) * 4 + u] = fma(ya, g[f][u], v[(j * NFC + f) * 4 + u]);
+				}
+				if (jj + 1 < JN) {
+					const double2 c = cs[ci + jj];
+					const double y2 = fma(fma(c.y, x2, c.x), yb, ya);
+					ya = yb; yb = y2;
+				}
+			}
+		}
+	}
+	// reduce-scatter over the warp: after the level of stride s, lanes with
+	// bit s set hold the upper half of the remaining sums
+	#pragma unroll
+	for (int s = 16, n = SR_NV / 2; s >= 1; s >>= 1, n >>= 1) {
+		const bool up = (lane & s) != 0;
+		#pragma unroll
+		for (int i = 0; i < n; i++) {
+			const double send = up ? v[i] : v[i + n];
+			const double keep = up ? v[i + n] : v[i];
+			v[i] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+		}
+	}
+	red[warp][2 * lane] = v[0];
+	red[warp][2 * lane + 1] = v[1];
+	__syncthreads();
+	for (int e = tid; e < SR_NV; e += nt) {
+		double sum = 0.0;
+		#pragma unroll
+		for (int w = 0; w < nt / 32; w++) sum += red[w][e];
+		const int j = e / (4 * NFC), f = (e / 4) % NFC, u = e & 3;
+		const int k = kb0 + j;
+		if (k < nk)
+			p.qq[((long)p.mt.koff[im] + k) * p.ncol + 16 * (f >> 2) + 2 * (f & 3) + ((u & 2) ? 8 : 0) + (u & 1)] = sum;
+	}
+}
+
 template <int SEG>
 void synth_seg(const LegParams& p, dim3 grid, int nt, cudaStream_t st)
 {
@@ -334,8 +483,23 @@ void launch_leg_synth_simt(const LegParams& p, cudaStream_t st)
 	}
 }
 
+template <int SEG>
+void analys_reg_seg(const LegParams& p, int kmax_all, cudaStream_t st)
+{
+	dim3 grid((kmax_all + 15) / 16, p.mlim + 1 - p.im0);
+	leg_analys_reg_kernel<SEG><<<grid, SR_NT, 0, st>>>(p);
+}
+
 void launch_leg_analys_simt(const LegParams& p, int kmax_all, cudaStream_t st)
 {
+	if (p.nfc == 1 && (p.ckseg >= 16 || p.nlat_2 <= 512)) {
+		switch (p.ckseg) {
+			case 8: analys_reg_seg<8>(p, kmax_all, st); break;
+			case 16: analys_reg_seg<16>(p, kmax_all, st); break;
+			default: analys_reg_seg<32>(p, kmax_all, st); break;
+		}
+		return;
+	}
 	// block of 2 nt k: the smallest of 32, 64, 128 threads that covers kmax_all
 	int nt = 32;
 	while (nt < SA_NT && 2 * nt < kmax_all) nt *= 2;
