@@ -9,9 +9,9 @@
  * (SH_to_spat, ...) copy their arrays to the GPU, transform there and copy
  * back; the cu_* functions of shtns_cuda.h take device pointers.
  *
- * Functions of the SHTns API that are not on the transform path (rotations,
- * point and latitude evaluation, complex-field transforms, regular grids) are
- * not provided.
+ * Local evaluation (points, one latitude), Legendre arrays, the l+-1
+ * operators and rotations run on the GPU as well (host arrays are copied in
+ * and out).  Regular (non-Gauss) grids are not provided.
  */
 #ifndef SHTNS_B200_SHTNS_H
 #define SHTNS_B200_SHTNS_H
@@ -166,6 +166,33 @@ void spat_to_SHsphtor_l(shtns_cfg, double *Vt, double *Vp, cplx *Slm, cplx *Tlm,
 void spat_to_SHqst_l(shtns_cfg, double *Vr, double *Vt, double *Vp, cplx *Qlm, cplx *Slm, cplx *Tlm, int ltr);
 void SHqst_to_spat_l(shtns_cfg, cplx *Qlm, cplx *Slm, cplx *Tlm, double *Vr, double *Vt, double *Vp, int ltr);
 #define SH_to_grad_spat_l(shtns, S,Gt,Gp,ltr) SHsph_to_spat_l(shtns, S, Gt, Gp, ltr)
+
+/* Local and partial evaluation (shtns.h:349-363); no grid needed.  Points
+ * at cos(theta) = cost and longitude phi; latitudes on nphi equispaced
+ * longitudes phi_j = 2 pi j / nphi, truncated at degree ltr and order mtr. */
+double SH_to_point(shtns_cfg, cplx *Qlm, double cost, double phi);                                  /* shtns.h:352 */
+cplx SH_to_point_cplx(shtns_cfg, cplx *alm, double cost, double phi);                                /* shtns.h:353 */
+void SH_to_grad_point(shtns_cfg, cplx *DrSlm, cplx *Slm,
+                      double cost, double phi, double *vr, double *vt, double *vp);                  /* shtns.h:354 */
+void SHqst_to_point(shtns_cfg, cplx *Qlm, cplx *Slm, cplx *Tlm,
+                    double cost, double phi, double *vr, double *vt, double *vp);                    /* shtns.h:356 */
+void SH_to_lat(shtns_cfg shtns, cplx *Qlm, double cost, double *vr, int nphi, int ltr, int mtr);     /* shtns.h:359 */
+void SHqst_to_lat(shtns_cfg, cplx *Qlm, cplx *Slm, cplx *Tlm, double cost,
+                  double *vr, double *vt, double *vp, int nphi, int ltr, int mtr);                   /* shtns.h:361 */
+
+/* Associated Legendre functions of order im*mres at x = cos(theta), degrees
+ * m..lmax, normalised as the plan's harmonics (shtns.h:232-233); the _deriv
+ * form returns P/sin(theta) (m > 0) and dP/dtheta.  Return the first degree
+ * whose value is not negligible (values below are written as 0). */
+int legendre_sphPlm_array(shtns_cfg shtns, const int lmax, const int im, const double x, double *yl); /* shtns.h:232 */
+int legendre_sphPlm_deriv_array(shtns_cfg shtns, const int lmax, const int im, const double x,
+                                const double sint, double *yl, double *dyl);                         /* shtns.h:233 */
+
+/* Operators coupling degrees l-1 and l+1 (shtns.h:240-245):
+ * Rlm[lm] = mx[2*lm] * Qlm[lm-1] + mx[2*lm+1] * Qlm[lm+1]; mx holds 2*nlm doubles. */
+void mul_ct_matrix(shtns_cfg, double *mx);                                                           /* shtns.h:240 */
+void st_dt_matrix(shtns_cfg, double *mx);                                                            /* shtns.h:243 */
+void SH_mul_mx(shtns_cfg, double *mx, cplx *Qlm, cplx *Rlm);                                         /* shtns.h:245 */
 
 #ifdef __cplusplus
 }

@@ -150,6 +150,15 @@ void shtns_b200_fourier_synth(shtns_cfg, int kind, cplx *F, double *V0, double *
 void shtns_b200_fourier_analys(shtns_cfg, int kind, double *V0, double *V1, double *V2, cplx *F, int nrows, int ltr);
 void shtns_b200_legendre_analys(shtns_cfg, int kind, cplx *F, cplx *Qlm, cplx *Slm, cplx *Tlm, int m0, int m1, int ltr);
 
+/* Batched point evaluation on device arrays: v[i] = the scalar field Qlm at
+ * (cost[i], phi[i]) for i < npts (SHqst form: the three components of
+ * SHqst_to_point).  One CTA per point; asynchronous on the plan's compute
+ * stream; no grid needed.  Single points: SH_to_point / SHqst_to_point
+ * (shtns.h).  No counterpart in SHTns 3.5.2. */
+void shtns_b200_SH_to_points(shtns_cfg, cplx *Qlm, const double *cost, const double *phi, double *v, int npts);
+void shtns_b200_SHqst_to_points(shtns_cfg, cplx *Qlm, cplx *Slm, cplx *Tlm, const double *cost, const double *phi,
+                                double *vr, double *vt, double *vp, int npts);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,6 +37,11 @@ class ShtnsInfo(C.Structure):
     ]
 
 
+class CPLX(C.Structure):
+    """C99 double complex returned by value (two doubles)."""
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
 CFG = C.POINTER(ShtnsInfo)
 P = C.c_void_p
 I = C.c_int
@@ -133,6 +138,19 @@ PROTOTYPES = {
     "shtns_b200_group_set_option": (I, [P, I, I]),
     "shtns_b200_group_synth": (None, [P, P, P, P, I]),
     "shtns_b200_group_analys": (None, [P, P, P, P, I]),
+    "SH_to_point": (D, [CFG, P, D, D]),
+    "SH_to_point_cplx": (CPLX, [CFG, P, D, D]),
+    "SH_to_grad_point": (None, [CFG, P, P, D, D, P, P, P]),
+    "SHqst_to_point": (None, [CFG, P, P, P, D, D, P, P, P]),
+    "SH_to_lat": (None, [CFG, P, D, P, I, I, I]),
+    "SHqst_to_lat": (None, [CFG, P, P, P, D, P, P, P, I, I, I]),
+    "legendre_sphPlm_array": (I, [CFG, I, I, D, P]),
+    "legendre_sphPlm_deriv_array": (I, [CFG, I, I, D, D, P, P]),
+    "mul_ct_matrix": (None, [CFG, P]),
+    "st_dt_matrix": (None, [CFG, P]),
+    "SH_mul_mx": (None, [CFG, P, P, P]),
+    "shtns_b200_SH_to_points": (None, [CFG, P, P, P, P, I]),
+    "shtns_b200_SHqst_to_points": (None, [CFG, P, P, P, P, P, P, P, P, I]),
     "shtns_b200_legendre_synth": (None, [CFG, I, P, P, P, P, I, I, I]),
     "shtns_b200_fourier_synth": (None, [CFG, I, P, P, P, P, I, I]),
     "shtns_b200_fourier_analys": (None, [CFG, I, P, P, P, P, I, I]),

@@ -106,6 +106,10 @@ struct shtns_info {
 	void *d_bsl; size_t bsl_cap;         // coefficient slices
 	int *d_bexp; size_t bexp_cap;        // column exponents [im][column]
 	int *d_split_err;                    // set by the kernel when a wait gives up
+	// local evaluation (points, latitudes, operators): classic-recurrence
+	// tables on the device, allocated on first use (no grid needed), and staging
+	double *d_alm; long *d_almoff;
+	void *d_loc; size_t loc_cap;
 	cudaStream_t comp_stream, xfer_stream;
 	int own_xfer;
 	int is_clone;

@@ -153,6 +153,29 @@ static inline double alm_b(shtns_cfg s, int im, int l)   // l >= m+2
 	return s->alm[s->alm_off[im] + 2 * (l - m - 1)];
 }
 
+// Coefficients of cos(theta) x Q coupling degrees l-1 and l+1 (mul_ct_matrix,
+// sht_func.c:395-458): mx[2 lm] multiplies Q_{l-1}, mx[2 lm + 1] Q_{l+1};
+// zero for l = m (below) and l = lmax (above).  st_dt_matrix scales them by
+// (l - 1) and -(l + 2) for sin(theta) d/dtheta (sht_func.c:460-469).
+static void ct_coefficients(shtns_cfg s, double* mx, int stdt)
+{
+	long lm = 0;
+	for (int im = 0; im <= s->mmax; im++) {
+		const int m = im * s->mres;
+		for (int l = m; l <= s->lmax; l++, lm++) {
+			double lo = (l > m) ? 1.0 / alm_a(s, im, l) : 0.0, hi = 0.0;
+			if (l < s->lmax)
+				hi = (s->base_norm == sht_schmidt) ? -alm_b(s, im, l + 2) / alm_a(s, im, l + 2) : 1.0 / alm_a(s, im, l + 1);
+			if (stdt) { lo *= (l - 1); hi *= -(l + 2); }
+			mx[2 * lm] = lo;
+			mx[2 * lm + 1] = hi;
+		}
+	}
+}
+
+extern "C" void mul_ct_matrix(shtns_cfg s, double* mx) { if (s && mx) ct_coefficients(s, mx, 0); }
+extern "C" void st_dt_matrix(shtns_cfg s, double* mx) { if (s && mx) ct_coefficients(s, mx, 1); }
+
 // Ishioka recurrence (sht_legendre.c:673-734): per order, the two-term
 // coefficients c (2 per k) and the basis change x (3 per k), padded so that
 // kernels may read whole 32-step segments.
@@ -344,6 +367,9 @@ static void free_device(shtns_cfg s)
 		for (void* p : ptrs) if (p) cudaFree(p);
 	}
 	free_split(s);
+	if (s->d_alm) cudaFree(s->d_alm);
+	if (s->d_loc) cudaFree(s->d_loc);
+	s->d_alm = nullptr; s->d_almoff = nullptr; s->d_loc = nullptr; s->loc_cap = 0;
 	if (s->d_qq) cudaFree(s->d_qq);
 	if (s->d_F) cudaFree(s->d_F);
 	if (s->d_stage) cudaFree(s->d_stage);
@@ -675,6 +701,7 @@ extern "C" shtns_cfg cushtns_clone(shtns_cfg b, cudaStream_t compute_stream, cud
 	s->base->nclones++;
 	s->d_qq = nullptr; s->qq_cap = 0; s->d_F = nullptr; s->F_cap = 0;
 	s->d_stage = nullptr; s->stage_cap = 0;
+	s->d_alm = nullptr; s->d_almoff = nullptr; s->d_loc = nullptr; s->loc_cap = 0;
 	s->d_yexp = nullptr; s->d_boff = nullptr; s->split_chunks = 0; s->split_kc = 0;
 	s->d_bsl = nullptr; s->bsl_cap = 0; s->d_bexp = nullptr; s->bexp_cap = 0; s->d_split_err = nullptr;
 	s->xfer_stream = nullptr; s->own_xfer = 0;

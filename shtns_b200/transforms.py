@@ -409,3 +409,94 @@ class sht:
         getattr(self._lib, fn)(self._cfg, *[x.ctypes.data_as(C.c_void_p) for x in v + outs])
         capi.check(self._lib)
         return outs[0] if n == 1 else tuple(outs)
+
+    # ---------------- local evaluation (shtns_numpy.i:566-606) ----------------
+    def _spec(self, a, n=None):
+        a = np.ascontiguousarray(a, dtype=np.complex128)
+        if a.size != (self.nlm if n is None else n):
+            raise RuntimeError("spectral array has wrong size.")
+        return a
+
+    def SH_to_point(self, Qlm, cost, phi):
+        """Value of the real scalar field Qlm at cos(theta) = cost, longitude phi."""
+        q = self._spec(Qlm)
+        v = self._lib.SH_to_point(self._cfg, q.ctypes.data_as(C.c_void_p), float(cost), float(phi))
+        capi.check(self._lib)
+        return v
+
+    def SH_to_point_cplx(self, alm, cost, phi):
+        """Value of the complex field alm (LM_cplx layout) at (cost, phi)."""
+        a = self._spec(alm, (self.lmax + 1) ** 2)
+        z = self._lib.SH_to_point_cplx(self._cfg, a.ctypes.data_as(C.c_void_p), float(cost), float(phi))
+        capi.check(self._lib)
+        return complex(z.re, z.im)
+
+    def _point3(self, fn, arrs, cost, phi):
+        out = [C.c_double() for _ in range(3)]
+        getattr(self._lib, fn)(self._cfg, *[a.ctypes.data_as(C.c_void_p) for a in arrs], float(cost), float(phi),
+                               *[C.byref(o) for o in out])
+        capi.check(self._lib)
+        return tuple(o.value for o in out)
+
+    def SH_to_grad_point(self, DrSlm, Slm, cost, phi):
+        """(vr, vt, vp): vr from DrSlm, (vt, vp) the gradient of Slm."""
+        return self._point3("SH_to_grad_point", [self._spec(DrSlm), self._spec(Slm)], cost, phi)
+
+    def SHqst_to_point(self, Qlm, Slm, Tlm, cost, phi):
+        """(vr, vt, vp) of the vector field (Qlm, Slm, Tlm) at (cost, phi)."""
+        return self._point3("SHqst_to_point", [self._spec(Qlm), self._spec(Slm), self._spec(Tlm)], cost, phi)
+
+    def SH_to_lat(self, Qlm, cost, Vr, ltr=None, mtr=None):
+        """Fill Vr (nphi doubles) with the field on latitude cost at phi_j = 2 pi j / nphi."""
+        q = self._spec(Qlm)
+        if Vr.dtype != np.float64 or not Vr.flags.c_contiguous:
+            raise RuntimeError("Vr must be a contiguous float64 array.")
+        self._lib.SH_to_lat(self._cfg, q.ctypes.data_as(C.c_void_p), float(cost), Vr.ctypes.data_as(C.c_void_p),
+                            int(Vr.size), self.lmax if ltr is None else int(ltr), self.mmax if mtr is None else int(mtr))
+        capi.check(self._lib)
+
+    def SHqst_to_lat(self, Qlm, Slm, Tlm, cost, Vr, Vt, Vp, ltr=None, mtr=None):
+        n = Vr.size
+        for v in (Vr, Vt, Vp):
+            if v.dtype != np.float64 or not v.flags.c_contiguous or v.size != n:
+                raise RuntimeError("Vr, Vt, Vp must be contiguous float64 arrays of one size.")
+        arrs = [self._spec(a) for a in (Qlm, Slm, Tlm)]
+        self._lib.SHqst_to_lat(self._cfg, *[a.ctypes.data_as(C.c_void_p) for a in arrs], float(cost),
+                               *[v.ctypes.data_as(C.c_void_p) for v in (Vr, Vt, Vp)], int(n),
+                               self.lmax if ltr is None else int(ltr), self.mmax if mtr is None else int(mtr))
+        capi.check(self._lib)
+
+    def points(self, Qlm, cost, phi):
+        """Values of the scalar field Qlm (CUDA complex128, nlm) at the points
+        (cost[i], phi[i]) (CUDA float64 tensors), one CUDA launch."""
+        if not (_is_torch(Qlm) and Qlm.is_cuda):
+            raise RuntimeError("points() takes CUDA tensors")
+        q = Qlm.contiguous()
+        ct, ph = cost.contiguous().double(), phi.contiguous().double()
+        v = torch.empty_like(ct)
+        self._stream()
+        self._lib.shtns_b200_SH_to_points(self._cfg, C.c_void_p(q.data_ptr()), C.c_void_p(ct.data_ptr()),
+                                          C.c_void_p(ph.data_ptr()), C.c_void_p(v.data_ptr()), int(ct.numel()))
+        capi.check(self._lib)
+        return v
+
+    def mul_ct_matrix(self):
+        mx = np.zeros(2 * self.nlm)
+        self._lib.mul_ct_matrix(self._cfg, mx.ctypes.data_as(C.c_void_p))
+        return mx
+
+    def st_dt_matrix(self):
+        mx = np.zeros(2 * self.nlm)
+        self._lib.st_dt_matrix(self._cfg, mx.ctypes.data_as(C.c_void_p))
+        return mx
+
+    def SH_mul_mx(self, mx, Qlm):
+        m = np.ascontiguousarray(mx, dtype=np.float64)
+        if m.size != 2 * self.nlm:
+            raise RuntimeError("matrix has wrong size.")
+        q = self._spec(Qlm)
+        r = np.empty_like(q)
+        self._lib.SH_mul_mx(self._cfg, m.ctypes.data_as(C.c_void_p), q.ctypes.data_as(C.c_void_p),
+                            r.ctypes.data_as(C.c_void_p))
+        capi.check(self._lib)
+        return r
