@@ -38,6 +38,9 @@ extern "C" {
 /* plan handle (shtns.h:42) */
 typedef struct shtns_info* shtns_cfg;
 
+/* rotation handle (shtns.h:43-44) */
+typedef struct shtns_rot_* shtns_rot;
+
 /* normalisations (shtns.h:48-55) */
 enum shtns_norm {
 	sht_orthonormal,
@@ -187,6 +190,25 @@ void SHqst_to_lat(shtns_cfg, cplx *Qlm, cplx *Slm, cplx *Tlm, double cost,
 int legendre_sphPlm_array(shtns_cfg shtns, const int lmax, const int im, const double x, double *yl); /* shtns.h:232 */
 int legendre_sphPlm_deriv_array(shtns_cfg shtns, const int lmax, const int im, const double x,
                                 const double sint, double *yl, double *dyl);                         /* shtns.h:233 */
+
+/* Rotations (shtns.h:186-218).  SH_Zrotate rotates about the z axis by alpha
+ * (Rlm = Qlm e^{-i m alpha}); SH_Yrotate, SH_Yrotate90 and SH_Xrotate90 need
+ * mres = 1 and mmax = lmax.  Rotation objects take Euler angles (intrinsic
+ * ZYZ or ZXZ) or an angle and an axis and apply the rotation to orthonormal
+ * expansions of real (LM layout) or complex (LM_cplx layout) fields; Rlm may
+ * be Qlm.  All rotations are active rotations of the field. */
+void SH_Zrotate(shtns_cfg, cplx *Qlm, double alpha, cplx *Rlm);                                      /* shtns.h:192 */
+void SH_Yrotate(shtns_cfg, cplx *Qlm, double alpha, cplx *Rlm);                                      /* shtns.h:194 */
+void SH_Yrotate90(shtns_cfg, cplx *Qlm, cplx *Rlm);                                                  /* shtns.h:196 */
+void SH_Xrotate90(shtns_cfg, cplx *Qlm, cplx *Rlm);                                                  /* shtns.h:198 */
+shtns_rot shtns_rotation_create(const int lmax, const int mmax, int norm);                           /* shtns.h:202 */
+void shtns_rotation_destroy(shtns_rot r);                                                            /* shtns.h:204 */
+void shtns_rotation_set_angles_ZYZ(shtns_rot r, double alpha, double beta, double gamma);            /* shtns.h:206 */
+void shtns_rotation_set_angles_ZXZ(shtns_rot r, double alpha, double beta, double gamma);            /* shtns.h:208 */
+void shtns_rotation_set_angle_axis(shtns_rot r, double theta, double Vx, double Vy, double Vz);      /* shtns.h:210 */
+int shtns_rotation_wigner_d_matrix(shtns_rot r, const int l, double *mx);                            /* shtns.h:214 */
+void shtns_rotation_apply_cplx(shtns_rot r, cplx *Zlm, cplx *Rlm);                                   /* shtns.h:216 */
+void shtns_rotation_apply_real(shtns_rot r, cplx *Qlm, cplx *Rlm);                                   /* shtns.h:218 */
 
 /* Operators coupling degrees l-1 and l+1 (shtns.h:240-245):
  * Rlm[lm] = mx[2*lm] * Qlm[lm-1] + mx[2*lm+1] * Qlm[lm+1]; mx holds 2*nlm doubles. */

@@ -10,6 +10,6 @@ from .capi import (sht_orthonormal, sht_fourpi, sht_schmidt, SHT_NO_CS_PHASE, SH
                    SHT_NATIVE_LAYOUT, SHT_THETA_CONTIGUOUS, SHT_PHI_CONTIGUOUS, SHT_SOUTH_POLE_FIRST,
                    SHT_SCALAR_ONLY, SHT_ALLOW_GPU, SHTError)
 
-from .transforms import sht  # noqa: F401  (the CUDA library loads when a plan is created)
+from .transforms import sht, rotation  # noqa: F401  (the CUDA library loads when a plan is created)
 
 __version__ = "0.1.0"

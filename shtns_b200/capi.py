@@ -149,6 +149,18 @@ PROTOTYPES = {
     "mul_ct_matrix": (None, [CFG, P]),
     "st_dt_matrix": (None, [CFG, P]),
     "SH_mul_mx": (None, [CFG, P, P, P]),
+    "SH_Zrotate": (None, [CFG, P, D, P]),
+    "SH_Yrotate": (None, [CFG, P, D, P]),
+    "SH_Yrotate90": (None, [CFG, P, P]),
+    "SH_Xrotate90": (None, [CFG, P, P]),
+    "shtns_rotation_create": (P, [I, I, I]),
+    "shtns_rotation_destroy": (None, [P]),
+    "shtns_rotation_set_angles_ZYZ": (None, [P, D, D, D]),
+    "shtns_rotation_set_angles_ZXZ": (None, [P, D, D, D]),
+    "shtns_rotation_set_angle_axis": (None, [P, D, D, D, D]),
+    "shtns_rotation_wigner_d_matrix": (I, [P, I, P]),
+    "shtns_rotation_apply_cplx": (None, [P, P, P]),
+    "shtns_rotation_apply_real": (None, [P, P, P]),
     "shtns_b200_SH_to_points": (None, [CFG, P, P, P, P, I]),
     "shtns_b200_SHqst_to_points": (None, [CFG, P, P, P, P, P, P, P, P, I]),
     "shtns_b200_legendre_synth": (None, [CFG, I, P, P, P, P, I, I, I]),

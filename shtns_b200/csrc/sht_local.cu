@@ -253,6 +253,20 @@ __global__ void __launch_bounds__(PT_THREADS) point_kernel(LocalParams p, const 
 	}
 }
 
+// associated Legendre values of every order im <= mmax at x, for degrees
+// m..lmax, into out[ofs(m) + l - m], ofs(m) = m (lmax + 2) - m (m + 1) / 2
+__global__ void plm_table_kernel(LocalParams p, double x, double st, double* out)
+{
+	const int im = blockIdx.x * blockDim.x + threadIdx.x;
+	if (im > p.mmax) return;
+	const int m = im * p.mres;
+	LocalParams q = p;
+	q.yl = out + (long) m * (p.lmax + 2) - (long) m * (m + 1) / 2;
+	q.dyl = nullptr;
+	q.lnz = nullptr;
+	order_sums(q, im, x, st, 0);
+}
+
 __global__ void legendre_array_kernel(LocalParams p, int im, double x, double st, int deriv)
 {
 	if (threadIdx.x == 0 && blockIdx.x == 0) order_sums(p, im, x, st, deriv);
@@ -414,6 +428,17 @@ int legendre_host(shtns_cfg s, int lmax, int im, double x, double sint, double* 
 }
 
 } // namespace
+
+// Legendre values of all orders of plan s (mres = 1) at x = cos(theta), for
+// the rotation tables (enqueued on stream st_)
+void launch_plm_table(shtns_cfg s, double x, double st, double* out, cudaStream_t st_)
+{
+	if (!loc_check(s)) return;
+	LocalParams p = loc_params(s);
+	plm_table_kernel<<<(s->mmax + 1 + 127) / 128, 128, 0, st_>>>(p, x, st, out);
+	shtb_count_launch();
+	shtb_cuda_ok(cudaGetLastError(), "Legendre table launch");
+}
 
 // ---- points (sht_func.c:516-730) ----
 extern "C" double SH_to_point(shtns_cfg s, cplx* Qlm, double cost, double phi)

@@ -500,3 +500,87 @@ class sht:
                             r.ctypes.data_as(C.c_void_p))
         capi.check(self._lib)
         return r
+
+    # ---------------- rotations (shtns_numpy.i:608-649) ----------------
+    def _rot(self, fn, Qlm, *args):
+        q = self._spec(Qlm)
+        r = np.empty_like(q)
+        getattr(self._lib, fn)(self._cfg, q.ctypes.data_as(C.c_void_p), *args, r.ctypes.data_as(C.c_void_p))
+        capi.check(self._lib)
+        return r
+
+    def Zrotate(self, Qlm, alpha):
+        """Rotation about the z axis by alpha (Rlm = Qlm e^{-i m alpha})."""
+        return self._rot("SH_Zrotate", Qlm, float(alpha))
+
+    def Yrotate(self, Qlm, alpha):
+        """Rotation about the y axis by alpha (mres = 1, mmax = lmax)."""
+        return self._rot("SH_Yrotate", Qlm, float(alpha))
+
+    def Yrotate90(self, Qlm):
+        return self._rot("SH_Yrotate90", Qlm)
+
+    def Xrotate90(self, Qlm):
+        return self._rot("SH_Xrotate90", Qlm)
+
+
+class rotation:
+    """Rotation of spherical-harmonic expansions (shtns_numpy.i:717-771):
+    rotation(lmax, mmax=-1, norm=0), then set_angles_ZYZ / set_angles_ZXZ /
+    set_angle_axis and apply_real / apply_cplx (orthonormal expansions of
+    real fields, LM layout, or complex fields, LM_cplx layout)."""
+
+    def __init__(self, lmax, mmax=-1, norm=0):
+        self._lib = capi.load()
+        if mmax < 0:
+            mmax = lmax
+        self._r = self._lib.shtns_rotation_create(int(lmax), int(mmax), int(norm))
+        if not self._r:
+            raise SHTError(self._lib.shtns_b200_last_error().decode())
+        self.lmax, self.mmax = lmax, mmax
+        self.nlm = int(self._lib.nlm_calc(lmax, mmax, 1))
+        self.nlm_cplx = int(self._lib.nlm_cplx_calc(lmax, mmax, 1))
+
+    def __del__(self):
+        try:
+            if getattr(self, "_r", None):
+                self._lib.shtns_rotation_destroy(self._r)
+                self._r = None
+        except Exception:
+            pass
+
+    def set_angles_ZYZ(self, alpha, beta, gamma):
+        self._lib.shtns_rotation_set_angles_ZYZ(self._r, float(alpha), float(beta), float(gamma))
+        capi.check(self._lib)
+
+    def set_angles_ZXZ(self, alpha, beta, gamma):
+        self._lib.shtns_rotation_set_angles_ZXZ(self._r, float(alpha), float(beta), float(gamma))
+        capi.check(self._lib)
+
+    def set_angle_axis(self, theta, Vx, Vy, Vz):
+        self._lib.shtns_rotation_set_angle_axis(self._r, float(theta), float(Vx), float(Vy), float(Vz))
+        capi.check(self._lib)
+
+    def wigner_d_matrix(self, l):
+        """(2l+1, 2l+1) Wigner d-matrix of the y rotation by beta, entry [m'+l, m+l]."""
+        mx = np.zeros((2 * l + 1, 2 * l + 1))
+        n = self._lib.shtns_rotation_wigner_d_matrix(self._r, int(l), mx.ctypes.data_as(C.c_void_p))
+        capi.check(self._lib)
+        if n == 0:
+            raise ValueError("0 <= l <= lmax not satisfied")
+        return mx
+
+    def _apply(self, fn, a, n):
+        q = np.ascontiguousarray(a, dtype=np.complex128)
+        if q.size != n:
+            raise RuntimeError("spectral array has wrong size.")
+        r = np.empty_like(q)
+        getattr(self._lib, fn)(self._r, q.ctypes.data_as(C.c_void_p), r.ctypes.data_as(C.c_void_p))
+        capi.check(self._lib)
+        return r
+
+    def apply_real(self, Qlm):
+        return self._apply("shtns_rotation_apply_real", Qlm, self.nlm)
+
+    def apply_cplx(self, Zlm):
+        return self._apply("shtns_rotation_apply_cplx", Zlm, self.nlm_cplx)
