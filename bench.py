@@ -750,6 +750,109 @@ def run_ordersplit(args):
         dist.destroy_process_group()
 
 
+def run_local(args):
+    """Rotations, batched point evaluation and latitude evaluation: the GPU
+    forms beside the reference library's own CPU functions on the same inputs
+    (host cores, all threads for the rotation).  value = rotations/s of one
+    lmax=1023 real field through shtns_rotation_apply_real (host arrays, as the
+    reference's API); the other rows are in "rows"."""
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    import shtns_b200
+    from shtns_b200 import capi
+    from tests.common import rand_spec
+    lib = capi.load()
+    rows = {}
+    clocks = ClockSampler(0)
+    clocks.start()
+
+    def wall(fn, reps):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        return (time.perf_counter() - t0) / reps
+
+    # rotation, lmax 1023, host arrays in and out
+    LR = 1023
+    q = rand_spec(LR, LR, 1, 5)
+    rot = shtns_b200.rotation(LR)
+    rot.set_angles_ZYZ(0.4, 1.9, -1.2)
+    n0 = lib.shtns_b200_launch_count()
+    t_rot = wall(lambda: rot.apply_real(q), 10)
+    launches = (lib.shtns_b200_launch_count() - n0) // 11
+    rows["rotation_lmax1023"] = {"gpu_ms": t_rot * 1e3, "form": "shtns_rotation_apply_real, host arrays"}
+    # batched points, lmax 255, 2^20 points on the device
+    LP, NPTS = 255, 1 << 20
+    sh = shtns_b200.sht(LP)
+    qp = rand_spec(LP, LP, 1, 6)
+    rng = np.random.default_rng(1)
+    ct = torch.from_numpy(rng.uniform(-1, 1, NPTS)).to(dev)
+    ph = torch.from_numpy(rng.uniform(0, 2 * np.pi, NPTS)).to(dev)
+    qd = torch.from_numpy(qp).to(dev)
+    sh.points(qd, ct, ph)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        sh.points(qd, ct, ph)
+    e1.record()
+    e1.synchronize()
+    t_pts = e0.elapsed_time(e1) / 5 * 1e-3
+    rows["points_lmax255"] = {"gpu_points_per_s": NPTS / t_pts, "form": "shtns_b200_SH_to_points, device arrays, 2^20 points"}
+    # one latitude, lmax 1023, 2048 longitudes, host arrays
+    sl = shtns_b200.sht(LR)
+    vl = np.zeros(2048)
+    t_lat = wall(lambda: sl.SH_to_lat(q, 0.3, vl), 20)
+    rows["latitude_lmax1023"] = {"gpu_ms": t_lat * 1e3, "form": "SH_to_lat, host arrays, nphi 2048"}
+    clk = clocks.stop()
+    cpu = None
+    if not args.no_cpu:
+        from oracle import shtns_ref as R
+        L = R.lib()
+        P = lambda a: a.ctypes.data_as(C.c_void_p)
+        L.shtns_rotation_create.restype = C.c_void_p
+        L.shtns_rotation_create.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.shtns_rotation_set_angles_ZYZ.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+        L.shtns_rotation_apply_real.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.shtns_use_threads(0)
+        rr = L.shtns_rotation_create(LR, LR, 0)
+        L.shtns_rotation_set_angles_ZYZ(rr, 0.4, 1.9, -1.2)
+        out = np.zeros_like(q)
+        c_rot = wall(lambda: L.shtns_rotation_apply_real(rr, P(q), P(out)), 3)
+        with quiet_stdout():
+            ref = R.RefSHT(LP, LP, 1, 0, 384, 768, flags=R.sht_gauss | R.SHT_THETA_CONTIGUOUS, eps=0.0, nthreads=1)
+        ctn, phn = ct[:2000].cpu().numpy(), ph[:2000].cpu().numpy()
+        t0 = time.perf_counter()
+        for a, b in zip(ctn, phn):
+            L.SH_to_point(ref.cfg, P(qp), float(a), float(b))
+        c_pts = 2000 / (time.perf_counter() - t0)
+        ref.close()
+        L.SH_to_lat.argtypes = [L.shtns_create.restype, C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_int,
+                                C.c_int]
+        with quiet_stdout():
+            ref = R.RefSHT(LR, LR, 1, 0, 1030, 2060, flags=R.sht_gauss | R.SHT_THETA_CONTIGUOUS, eps=0.0, nthreads=1)
+        xs = iter(np.linspace(-0.9, 0.9, 1000))    # a new latitude each call (the reference caches its last one)
+        c_lat = wall(lambda: L.SH_to_lat(ref.cfg, P(q), float(next(xs)), P(vl), 2048, LR, LR), 10)
+        ref.close()
+        rows["rotation_lmax1023"].update({"cpu_ms": c_rot * 1e3, "cpu_threads": os.cpu_count(), "speedup": c_rot / t_rot})
+        rows["points_lmax255"].update({"cpu_points_per_s": c_pts, "cpu_threads": 1,
+                                       "speedup": rows["points_lmax255"]["gpu_points_per_s"] / c_pts})
+        rows["latitude_lmax1023"].update({"cpu_ms": c_lat * 1e3, "cpu_threads": 1, "speedup": c_lat / t_lat})
+        cpu = {"value": 1.0 / c_rot, "unit": "rotations/s (lmax=1023, one real field)", "cores": os.cpu_count(),
+               "kind": "reference", "sample": "3 rotations of one lmax=1023 field (reference shtns_rotation_apply_real, OpenMP)"}
+    line = {
+        "metric": "rotations/s, points/s and latitudes/s against the reference CPU functions",
+        "value": 1.0 / t_rot, "unit": "rotations/s (lmax=1023, one real field, host arrays)", "n_gpus": 1,
+        "steps": 10, "warmup": 1, "ms_per_step": t_rot * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1)/(l+1))",
+        "config": {"workload": "local_evaluation_and_rotation", "l2": "not flushed (host-array API, wall clock)"},
+        "rows": rows, "gpu_launches": int(launches), "cpu_baseline": cpu, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -761,11 +864,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-chunks", type=int, default=E2E_CHUNKS,
                     help="field chunks (streams) of the end-to-end step")
-    ap.add_argument("--workload", default="qst", choices=["qst", "uneven", "highdeg", "ordersplit"],
+    ap.add_argument("--workload", default="qst", choices=["qst", "uneven", "highdeg", "ordersplit", "local"],
                     help="qst: lmax=511 vector transforms of 64 fields (default); "
                          "uneven: 256 scalar fields of lmax 63..1023 through a plan group; "
                          "highdeg: lmax=4095, 8 fields, FP64 and split-precision synthesis; "
-                         "ordersplit: one lmax=4095 field divided over the ranks by order")
+                         "ordersplit: one lmax=4095 field divided over the ranks by order; "
+                         "local: rotations, points and latitudes against the reference functions")
     args = ap.parse_args()
     if args.workload == "uneven" and args.impl != "reference":
         run_uneven(args)
@@ -773,6 +877,8 @@ def main():
         run_highdeg(args)
     elif args.workload == "ordersplit" and args.impl != "reference":
         run_ordersplit(args)
+    elif args.workload == "local" and args.impl != "reference":
+        run_local(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
