@@ -584,3 +584,58 @@ class rotation:
 
     def apply_cplx(self, Zlm):
         return self._apply("shtns_rotation_apply_cplx", Zlm, self.nlm_cplx)
+
+
+def _inplace(fn, kinds):
+    """Method writing into caller arrays, as the reference's in-place
+    transforms (shtns_numpy.i:319-395): one field, sizes checked."""
+    def method(self, *arrs):
+        self._need_grid()
+        if len(arrs) != len(kinds):
+            raise RuntimeError("%d arrays required." % len(kinds))
+        sizes = {"q": (np.complex128, self.nlm), "v": (np.float64, self.nspat),
+                 "a": (np.complex128, (self.lmax + 1) ** 2), "z": (np.complex128, self.nspat)}
+        ptrs = []
+        for a, k in zip(arrs, kinds):
+            dt, n = sizes[k]
+            if not isinstance(a, np.ndarray) or not a.flags.c_contiguous or a.dtype != dt or a.size != n:
+                raise RuntimeError("array must be a contiguous %s array of %d elements." % (np.dtype(dt).name, n))
+            ptrs.append(a.ctypes.data_as(C.c_void_p))
+        self._batch(1)
+        getattr(self._lib, fn)(self._cfg, *ptrs)
+        capi.check(self._lib)
+    method.__name__ = fn
+    method.__doc__ = "%s(%s) in place (shtns_numpy.i:319-395)." % (fn, ", ".join(kinds))
+    return method
+
+
+for _fn, _k in (("spat_to_SH", "vq"), ("SH_to_spat", "qv"), ("spat_cplx_to_SH", "za"), ("SH_to_spat_cplx", "az"),
+                ("spat_to_SHsphtor", "vvqq"), ("SHsphtor_to_spat", "qqvv"), ("SHsph_to_spat", "qvv"),
+                ("SHtor_to_spat", "qvv"), ("spat_cplx_to_SHsphtor", "zzaa"), ("SHsphtor_to_spat_cplx", "aazz"),
+                ("spat_to_SHqst", "vvvqqq"), ("SHqst_to_spat", "qqqvvv"), ("spat_cplx_to_SHqst", "zzzaaa"),
+                ("SHqst_to_spat_cplx", "aaazzz")):
+    setattr(sht, _fn, _inplace(_fn, _k))
+
+
+def _zlm(self, idx):
+    """(l, m) of index idx in the complex expansion (shtns_numpy.i:545-553)."""
+    idx = np.asarray(idx)
+    if (idx >= (self.lmax + 1) ** 2).any() or (idx < 0).any():
+        raise RuntimeError("invalid range for l,m")
+    l = np.sqrt(idx).astype(int)
+    return l, idx - l * (l + 1)
+
+
+def _spec_array_cplx(self):
+    return np.zeros((self.lmax + 1) ** 2, dtype=complex)
+
+
+def _spat_array_cplx(self):
+    if self.nlat == 0:
+        raise RuntimeError("Grid not set. Call .set_grid() method.")
+    return np.zeros(self.spat_shape, dtype="complex128")
+
+
+sht.zlm = _zlm
+sht.spec_array_cplx = _spec_array_cplx
+sht.spat_array_cplx = _spat_array_cplx
