@@ -388,6 +388,17 @@ def run_gpu(args):
             roof = {"kernel": names[dom], "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
                     "frac": ach / hbm, "traffic": TRAFFIC_PER_FIELD[names[dom]] * nf, "traffic_source": TRAFFIC_SOURCE,
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
+        # the reference's own work count for a transform direction
+        # (time_SHT.c:297): W = nlat (4 nlm + 2 (mmax+1) + mmax log2(mmax+1) + 5 nphi log2 nphi)
+        # per scalar component; a qst pair counts 2 directions x 3 components
+        w1 = NLAT * (4.0 * sh.nlm + 2 * (LMAX + 1) + LMAX * np.log2(LMAX + 1) + 5.0 * NPHI * np.log2(NPHI))
+        w_step = 2 * 3 * w1 * nf * world
+        roof["reference_work_count"] = {
+            "flop_per_step": w_step, "tflops": w_step / (ms_step * 1e-3) / 1e12,
+            "frac_of_fp64_peak": w_step / (ms_step * 1e-3) / 1e12 / peak_fp64,
+            "note": "whole step (all GPUs) in the reference's operation count (4 flop per degree, order and "
+                    "latitude in the Legendre sums); the even/odd folded Ishioka contraction does half of "
+                    "those Legendre flops, so this figure is above the kernels' own count"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
