@@ -150,6 +150,31 @@ void shtns_b200_fourier_synth(shtns_cfg, int kind, cplx *F, double *V0, double *
 void shtns_b200_fourier_analys(shtns_cfg, int kind, double *V0, double *V1, double *V2, cplx *F, int nrows, int ltr);
 void shtns_b200_legendre_analys(shtns_cfg, int kind, cplx *F, cplx *Qlm, cplx *Slm, cplx *Tlm, int m0, int m1, int ltr);
 
+/* The order-split Legendre stages with the exchange fused in: the synthesis
+ * stores Fourier row `row` of order im and field-component fc into the buffer
+ * F[b] of the block b with lat0[b] <= row < lat0[b+1], at
+ * (fc * (mmax+1) + im) * (lat0[b+1] - lat0[b]) + row - lat0[b] (the Fourier
+ * side of shtns_b200_fourier_synth for that block); the analysis loads the
+ * rows from there.  lat0[0] = 0, lat0[nblk] = nlat, 1 <= nblk <= 16.  The
+ * buffers may be other GPUs' memory mapped with shtns_b200_ipc_open: the
+ * rows then cross NVLink inside the Legendre kernels.  The caller orders
+ * the stages across processes (a barrier between a rank's Legendre stage and
+ * the FFT stages that read or write the same buffers).  No counterpart in
+ * SHTns 3.5.2. */
+void shtns_b200_legendre_synth_rows(shtns_cfg, int kind, cplx *Qlm, cplx *Slm, cplx *Tlm, int m0, int m1, int ltr,
+                                    int nblk, const int *lat0, cplx **F);
+void shtns_b200_legendre_analys_rows(shtns_cfg, int kind, int nblk, const int *lat0, cplx **F,
+                                     cplx *Qlm, cplx *Slm, cplx *Tlm, int m0, int m1, int ltr);
+/* Buffers for those stages: device allocations of their own (so that an IPC
+ * handle maps exactly the buffer), the 64-byte CUDA IPC handle of such an
+ * allocation (returns 0 or -1), the mapping of another process's handle
+ * (NULL on error) and its release. */
+void *shtns_b200_alloc(size_t bytes);
+void shtns_b200_free(void *ptr);
+int shtns_b200_ipc_handle(void *dev_ptr, void *handle64);
+void *shtns_b200_ipc_open(const void *handle64);
+void shtns_b200_ipc_close(void *ptr);
+
 /* Batched point evaluation on device arrays: v[i] = the scalar field Qlm at
  * (cost[i], phi[i]) for i < npts (SHqst form: the three components of
  * SHqst_to_point).  One CTA per point; asynchronous on the plan's compute

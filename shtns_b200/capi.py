@@ -163,6 +163,13 @@ PROTOTYPES = {
     "shtns_rotation_apply_real": (None, [P, P, P]),
     "shtns_b200_SH_to_points": (None, [CFG, P, P, P, P, I]),
     "shtns_b200_SHqst_to_points": (None, [CFG, P, P, P, P, P, P, P, P, I]),
+    "shtns_b200_legendre_synth_rows": (None, [CFG, I, P, P, P, I, I, I, I, P, P]),
+    "shtns_b200_legendre_analys_rows": (None, [CFG, I, I, P, P, P, P, P, I, I, I]),
+    "shtns_b200_alloc": (P, [C.c_size_t]),
+    "shtns_b200_free": (None, [P]),
+    "shtns_b200_ipc_handle": (I, [P, P]),
+    "shtns_b200_ipc_open": (P, [P]),
+    "shtns_b200_ipc_close": (None, [P]),
     "shtns_b200_legendre_synth": (None, [CFG, I, P, P, P, P, I, I, I]),
     "shtns_b200_fourier_synth": (None, [CFG, I, P, P, P, P, I, I]),
     "shtns_b200_fourier_analys": (None, [CFG, I, P, P, P, P, I, I]),

@@ -1152,3 +1152,124 @@ extern "C" void shtns_b200_legendre_analys(shtns_cfg s, int kind, cplx* F, cplx*
 	shtb_stage_end(s);
 	check_launch("order-split Legendre analysis launch");
 }
+
+// ---------------------------------------------------------------------------
+// Order-split stages with the exchange fused into the Legendre kernels: the
+// synthesis stores each Fourier row straight into the buffer of the block of
+// grid rows that owns it (blocks lat0[b] .. lat0[b+1]-1, buffer F[b] laid out
+// as the Fourier side of shtns_b200_fourier_synth), and the analysis loads
+// the rows from there.  When the buffers are other GPUs' memory mapped into
+// this process (shtns_b200_ipc_open), the stores and loads go over NVLink
+// inside the Legendre kernels and no separate all-to-all remains.
+namespace {
+
+bool row_blocks(shtns_cfg s, int nblk, const int* lat0, cplx* const* F, RowBlocks& rb)
+{
+	if (nblk < 1 || nblk > SHTB_MAX_BLOCKS || !lat0 || !F) {
+		shtb_set_error(1, "order-split rows: 1 to 16 blocks with row bounds and buffers required");
+		return false;
+	}
+	memset(&rb, 0, sizeof(rb));
+	rb.n = nblk;
+	rb.mstride = s->mmax + 1;
+	for (int b = 0; b <= nblk; b++) rb.lat0[b] = lat0[b];
+	if (rb.lat0[0] != 0 || rb.lat0[nblk] != (int) s->nlat) {
+		shtb_set_error(1, "order-split rows: blocks must cover rows 0..nlat-1");
+		return false;
+	}
+	for (int b = 0; b < nblk; b++) {
+		if (rb.lat0[b + 1] <= rb.lat0[b] || !F[b]) { shtb_set_error(1, "order-split rows: empty block or null buffer"); return false; }
+		rb.base[b] = reinterpret_cast<double2*>(F[b]);
+	}
+	return true;
+}
+
+} // namespace
+
+extern "C" void shtns_b200_legendre_synth_rows(shtns_cfg s, int kind, cplx* Q, cplx* S, cplx* T, int m0, int m1, int ltr,
+                                               int nblk, const int* lat0, cplx** F)
+{
+	int nc; const int* ty;
+	Job j;
+	RowBlocks rb;
+	if (!kind_types(kind, &nc, &ty) || !setup_job(s, j, nc, ty, ltr, 1)) return;
+	if (m0 < 0 || m1 < m0 || m1 > s->mmax) { shtb_set_error(1, "order-split stage: invalid order range"); return; }
+	if (!row_blocks(s, nblk, lat0, F, rb)) return;
+	if (m0 > j.mlim) return;
+	const int mhi = std::min(m1, j.mlim);
+	PrepParams pp = prep_params(s, j);
+	pp.im0 = m0; pp.mlim = mhi;
+	pp.Q = reinterpret_cast<const double2*>(Q);
+	pp.S = reinterpret_cast<const double2*>(S);
+	pp.T = reinterpret_cast<const double2*>(T);
+	launch_prep_synth(pp, s->comp_stream);
+	LegParams lp = leg_params(s, j);
+	lp.im0 = m0; lp.mlim = mhi;
+	lp.rb = rb;
+	launch_leg_synth(lp, s->comp_stream);
+	check_launch("order-split Legendre synthesis launch");
+}
+
+extern "C" void shtns_b200_legendre_analys_rows(shtns_cfg s, int kind, int nblk, const int* lat0, cplx** F,
+                                                cplx* Q, cplx* S, cplx* T, int m0, int m1, int ltr)
+{
+	int nc; const int* ty;
+	Job j;
+	RowBlocks rb;
+	if (!kind_types(kind, &nc, &ty) || !setup_job(s, j, nc, ty, ltr, 1)) return;
+	if (m0 < 0 || m1 < m0 || m1 > s->mmax) { shtb_set_error(1, "order-split stage: invalid order range"); return; }
+	if (!row_blocks(s, nblk, lat0, F, rb)) return;
+	if (m0 <= j.mlim) {
+		LegParams lp = leg_params(s, j);
+		lp.im0 = m0; lp.mlim = std::min(m1, j.mlim);
+		lp.rb = rb;
+		launch_leg_analys(lp, (j.llim + j.vec_extra - m0 * s->mres) / 2 + 1, s->comp_stream);
+	}
+	PrepParams pp = prep_params(s, j);
+	pp.im0 = m0;
+	pp.Qo = reinterpret_cast<double2*>(Q);
+	pp.So = reinterpret_cast<double2*>(S);
+	pp.To = reinterpret_cast<double2*>(T);
+	launch_post_analys_m(pp, m1, s->comp_stream);
+	check_launch("order-split Legendre analysis launch");
+}
+
+// Device allocations of their own (an IPC handle maps a whole allocation).
+extern "C" void* shtns_b200_alloc(size_t bytes)
+{
+	void* p = nullptr;
+	if (!shtb_cuda_ok(cudaMalloc(&p, bytes), "device buffer")) return nullptr;
+	return p;
+}
+
+extern "C" void shtns_b200_free(void* p)
+{
+	if (p) cudaFree(p);
+}
+
+// CUDA IPC: the 64-byte handle of a device allocation made in this process,
+// and the mapping of another process's handle (peer access enabled lazily).
+extern "C" int shtns_b200_ipc_handle(void* dev_ptr, void* handle64)
+{
+	cudaIpcMemHandle_t h;
+	if (!dev_ptr || !handle64) { shtb_set_error(1, "ipc handle: null argument"); return -1; }
+	if (!shtb_cuda_ok(cudaIpcGetMemHandle(&h, dev_ptr), "cudaIpcGetMemHandle")) return -1;
+	static_assert(sizeof(h) == 64, "CUDA IPC handles are 64 bytes");
+	memcpy(handle64, &h, sizeof(h));
+	return 0;
+}
+
+extern "C" void* shtns_b200_ipc_open(const void* handle64)
+{
+	cudaIpcMemHandle_t h;
+	void* p = nullptr;
+	if (!handle64) { shtb_set_error(1, "ipc open: null handle"); return nullptr; }
+	memcpy(&h, handle64, sizeof(h));
+	if (!shtb_cuda_ok(cudaIpcOpenMemHandle(&p, h, cudaIpcMemLazyEnablePeerAccess), "cudaIpcOpenMemHandle")) return nullptr;
+	return p;
+}
+
+extern "C" void shtns_b200_ipc_close(void* ptr)
+{
+	if (ptr) shtb_cuda_ok(cudaIpcCloseMemHandle(ptr), "cudaIpcCloseMemHandle");
+}

@@ -125,6 +125,18 @@ struct shtns_info {
 };
 
 // ---- kernel parameter blocks ----
+// Fourier rows split over several buffers by blocks of grid rows (the
+// order-split transform with its exchange fused into the Legendre kernels):
+// block b holds rows lat0[b] .. lat0[b+1]-1 as [fc][im][row - lat0[b]] with
+// mstride orders per field-component.  n = 0: the plain buffer F.
+#define SHTB_MAX_BLOCKS 16
+struct RowBlocks {
+	int n;
+	int mstride;
+	int lat0[SHTB_MAX_BLOCKS + 1];
+	double2* base[SHTB_MAX_BLOCKS];
+};
+
 struct LegParams {
 	int nlat, nlat_2, llim, mlim, mres, vec_extra;
 	int im0;                             // first order of the launch (orders im0..mlim; 0 for whole transforms)
@@ -143,7 +155,36 @@ struct LegParams {
 	double *qq;                          // coefficient buffer
 	double2 *F;                          // Fourier buffer
 	long fstride;                        // complex elements between field-components in F
+	RowBlocks rb;                        // rows in per-block buffers instead of F (rb.n > 0)
 };
+
+// address of Fourier row `row` of field-component fc, order im (block-split
+// layouts go through the out-of-line forms below, so that the plain layout
+// keeps its registers)
+__device__ __forceinline__ double2* fourier_row(const LegParams& p, int fc, int im, int row)
+{
+	if (p.rb.n == 0) return p.F + (long)fc * p.fstride + (long)im * p.nlat + row;
+	int b = 0;
+	while (b + 1 < p.rb.n && row >= p.rb.lat0[b + 1]) b++;
+	const int r0 = p.rb.lat0[b];
+	return p.rb.base[b] + ((long)fc * p.rb.mstride + im) * (p.rb.lat0[b + 1] - r0) + (row - r0);
+}
+
+static __device__ __noinline__ void fourier_row_store2(const LegParams& p, int fc, int im, int rn, int rs, double2 vn, double2 vs)
+{
+	*fourier_row(p, fc, im, rn) = vn;
+	*fourier_row(p, fc, im, rs) = vs;
+}
+
+struct RowPair { double2 n, s; };
+
+static __device__ __noinline__ RowPair fourier_row_load2(const LegParams& p, int fc, int im, int rn, int rs)
+{
+	RowPair r;
+	r.n = __ldg(fourier_row(p, fc, im, rn));
+	r.s = __ldg(fourier_row(p, fc, im, rs));
+	return r;
+}
 
 struct PrepParams {
 	int lmax, llim, mlim, mres, nf, ncomp, ncol, comp_type[3];   // comp_type: 0 scalar Q, 1 V (from S,T), 2 W (from S,T)

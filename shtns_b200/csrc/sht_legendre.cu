@@ -410,7 +410,7 @@ __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int t
 	const int fc = ((c0 + wn * 16) >> 4) * 4 + (lane & 3);
 	if (fc >= p.nfc) return;
 	const bool vec = (p.ctype[fc / p.nf] != 0) && !p.robert;
-	double2* Ff = p.F + (long)fc * p.fstride + (long)im * p.nlat;
+	double2* Ff = p.F + (long)fc * p.fstride + (long)im * p.nlat;     // plain layout (p.rb.n == 0)
 	#pragma unroll
 	for (int i = 0; i < 4; i++) {
 		const int t = t0 + wm * 32 + i * 8 + (lane >> 2);
@@ -427,8 +427,12 @@ __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int t
 		}
 		const int rn = p.south_first ? p.nlat - 1 - t : t;
 		const int rs = p.nlat - 1 - rn;
-		Ff[rn] = make_double2(nr, ni);
-		Ff[rs] = make_double2(sr, si);
+		if (p.rb.n == 0) {
+			Ff[rn] = make_double2(nr, ni);
+			Ff[rs] = make_double2(sr, si);
+		} else {
+			fourier_row_store2(p, fc, im, rn, rs, make_double2(nr, ni), make_double2(sr, si));
+		}
 	}
 }
 
@@ -492,9 +496,15 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 			if (t < p.nlat_2 && t >= tmm && fc < p.nfc) {
 				const int rn = p.south_first ? p.nlat - 1 - t : t;
 				const int rs = p.nlat - 1 - rn;
-				const double2* Ff = p.F + (long)fc * p.fstride + (long)im * p.nlat;
-				fnn[u] = __ldg(Ff + rn);
-				fsn[u] = __ldg(Ff + rs);
+				if (p.rb.n == 0) {
+					const double2* Ff = p.F + (long)fc * p.fstride + (long)im * p.nlat;
+					fnn[u] = __ldg(Ff + rn);
+					fsn[u] = __ldg(Ff + rs);
+				} else {
+					const RowPair r = fourier_row_load2(p, fc, im, rn, rs);
+					fnn[u] = r.n;
+					fsn[u] = r.s;
+				}
 			}
 		}
 		const int t = tt0 + gtt;
@@ -592,14 +602,14 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 
 // Single-plan kernels: blockIdx.y = order - p.im0, blockIdx.x = (row tile, column tile).
 template <int SEG, int WM>
-__global__ void __launch_bounds__(LG_THREADS, WM == 1 ? 2 : 3) leg_synth_kernel(LegParams p)
+__global__ void __launch_bounds__(LG_THREADS, WM == 1 ? 2 : 3) leg_synth_kernel(const __grid_constant__ LegParams p)
 {
 	const int ntb = (p.nlat_2 + 32 * WM - 1) / (32 * WM);
 	leg_synth_tile<SEG, WM>(p, p.im0 + blockIdx.y, blockIdx.x % ntb, blockIdx.x / ntb);
 }
 
 template <int SEG, int WM>
-__global__ void __launch_bounds__(LG_THREADS, WM == 1 ? 2 : 3) leg_analys_kernel(LegParams p, int nkb)
+__global__ void __launch_bounds__(LG_THREADS, WM == 1 ? 2 : 3) leg_analys_kernel(const __grid_constant__ LegParams p, int nkb)
 {
 	leg_analys_tile<SEG, WM>(p, p.im0 + blockIdx.y, blockIdx.x % nkb, blockIdx.x / nkb);
 }

@@ -61,9 +61,8 @@ __device__ __forceinline__ void simt_synth_store(const LegParams& p, int im, int
 			const double s = p.w[t] * (m > 0 ? p.mpos_inv : 1.0) / (p.nphi * (m > 0 ? 2.0 : 1.0));
 			nr *= s; ni *= s; sr *= s; si *= s;
 		}
-		double2* Ff = p.F + (long)f * p.fstride + (long)im * p.nlat;
-		Ff[rn] = make_double2(nr, ni);
-		Ff[rs] = make_double2(sr, si);
+		*fourier_row(p, f, im, rn) = make_double2(nr, ni);
+		*fourier_row(p, f, im, rs) = make_double2(sr, si);
 	}
 }
 
@@ -199,9 +198,8 @@ __global__ void __launch_bounds__(SA_NT) leg_analys_simt_kernel(LegParams p)
 			if (gf < NFC && tg < p.nlat_2 && tg >= tmm) {
 				const int rn = p.south_first ? p.nlat - 1 - tg : tg;
 				const int rs = p.nlat - 1 - rn;
-				const double2* Ff = p.F + (long)gf * p.fstride + (long)im * p.nlat;
-				fn[i] = __ldg(Ff + rn);
-				fs[i] = __ldg(Ff + rs);
+				fn[i] = __ldg(fourier_row(p, gf, im, rn));
+				fs[i] = __ldg(fourier_row(p, gf, im, rs));
 			}
 		}
 	};
@@ -342,9 +340,8 @@ __global__ void __launch_bounds__(SR_NT) leg_analys_reg_kernel(LegParams p)
 		const int rs = p.nlat - 1 - rn;
 		#pragma unroll
 		for (int f = 0; f < NFC; f++) {
-			const double2* Ff = p.F + (long)f * p.fstride + (long)im * p.nlat;
-			nfn[f] = __ldg(Ff + rn);
-			nfs[f] = __ldg(Ff + rs);
+			nfn[f] = __ldg(fourier_row(p, f, im, rn));
+			nfs[f] = __ldg(fourier_row(p, f, im, rs));
 		}
 		#pragma unroll
 		for (int b = 0; b < NSB; b++) {

@@ -659,6 +659,7 @@ static bool split_tables(shtns_cfg s, int kc, cudaStream_t st)
 
 void launch_leg_synth_split(shtns_cfg s, const LegParams& p, cudaStream_t st)
 {
+	if (p.rb.n) { shtb_set_error(1, "split-precision synthesis writes the plain Fourier buffer only"); return; }
 	const int ns = s->split_ns;
 	const int nc = ns <= 5 ? 32 : 16;             // accumulators: nc ns (ns + 1) / 2 <= 512 columns
 	const int kc = ns <= 6 ? 64 : 32;             // staged steps: two A buffers fit 227 KB

@@ -322,3 +322,169 @@ class OrderSplit:
         """Full spatial arrays on every rank from each rank's block of rows."""
         sizes = [b - a for (a, b) in self.rows]
         return self._gather_padded(v.contiguous(), sizes, v.dim() - (2 if self.phi_contiguous else 1))
+
+
+class RowBuffer:
+    """A device allocation of its own holding one rank's Fourier rows
+    [fc][order][row] (complex128), visible to torch through
+    __cuda_array_interface__ without a copy."""
+
+    def __init__(self, lib, shape):
+        self.lib = lib
+        self.shape = tuple(int(x) for x in shape)
+        nbytes = 16 * int(np.prod(self.shape))
+        self.ptr = lib.shtns_b200_alloc(nbytes)
+        if not self.ptr:
+            capi.check(lib)
+            raise MemoryError("device buffer of %d bytes" % nbytes)
+        self.__cuda_array_interface__ = {"shape": self.shape, "typestr": "<c16", "data": (self.ptr, False),
+                                         "version": 3, "strides": None}
+
+    def tensor(self):
+        return torch.as_tensor(self, device=torch.device("cuda", torch.cuda.current_device()))
+
+    def free(self):
+        if self.ptr:
+            self.lib.shtns_b200_free(C.c_void_p(self.ptr))
+            self.ptr = None
+
+
+class FusedOrderSplit(OrderSplit):
+    """OrderSplit with the all-to-all fused into the Legendre kernels: the
+    synthesis stores every Fourier row straight into the row buffer of the
+    rank that owns the row (another GPU's memory mapped by CUDA IPC, over
+    NVLink), the analysis loads rows from there, and the FFT stages work on
+    the rank's own buffer.  Each direction runs
+        barrier, Legendre stage into / from the buffers, barrier, FFT stage
+    (synthesis), or FFT, barrier, Legendre, barrier (analysis): the barriers
+    order the writes of one rank's kernels before the reads of another's.
+    Buffers are allocated and mapped by prepare(nfc), a collective call."""
+
+    def __init__(self, plan, group=None, rank=None, world=None, costs=None, barrier=None):
+        super().__init__(plan, group=group, rank=rank, world=world, costs=costs)
+        self.lib = plan._lib
+        self.buf = None
+        self.ptrs = None
+        self._mapped = []
+        self._barrier = barrier
+
+    def barrier(self):
+        if self._barrier is not None:
+            self._barrier()
+        elif self.world > 1:
+            import torch.distributed as dist
+            dist.barrier(group=self.group)
+
+    def release(self):
+        for p in self._mapped:
+            self.lib.shtns_b200_ipc_close(C.c_void_p(p))
+        self._mapped = []
+        if self.buf is not None:
+            self.buf.free()
+            self.buf = None
+        self.ptrs = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    def prepare(self, nfc):
+        """Row buffer for nfc field-components on every rank, mapped into
+        every rank (collective; nothing to do when the buffers are large enough)."""
+        if self.buf is not None and self.buf.shape[0] >= nfc:
+            return
+        self.allocate(nfc)
+        if self.world == 1:
+            self.set_row_buffers([self.buf.ptr])
+            return
+        import torch.distributed as dist
+        h = (C.c_char * 64)()
+        if self.lib.shtns_b200_ipc_handle(C.c_void_p(self.buf.ptr), h) != 0:
+            capi.check(self.lib)
+        hs = [None] * self.world
+        dist.all_gather_object(hs, bytes(h), group=self.group)
+        ptrs = []
+        for r, hb in enumerate(hs):
+            if r == self.rank:
+                ptrs.append(self.buf.ptr)
+                continue
+            p = self.lib.shtns_b200_ipc_open(C.c_char_p(hb))
+            if not p:
+                capi.check(self.lib)
+            self._mapped.append(p)
+            ptrs.append(p)
+        self.set_row_buffers(ptrs)
+
+    def allocate(self, nfc):
+        """This rank's row buffer only (no mapping): [nfc][mmax+1][nrows]."""
+        self.release()
+        self.buf = RowBuffer(self.lib, (nfc, self.plan.mmax + 1, self.nrows))
+
+    def set_row_buffers(self, ptrs):
+        """Device addresses of every rank's row buffer, in rank order."""
+        self.ptrs = (C.c_void_p * self.world)(*[C.c_void_p(int(p)) for p in ptrs])
+        self.bounds = (C.c_int * (self.world + 1))(*([a for a, _ in self.rows] + [self.plan.nlat]))
+
+    def _spec_ptrs(self, kind, arrs):
+        return CudaStages._ptrs(kind, arrs)
+
+    # ---------------- phases (public for callers that order the ranks themselves) ----------------
+    def synth_rows(self, *specs, ltr=None):
+        """Legendre stage of this rank's orders, rows stored into their owners' buffers."""
+        kind = self._kind(len(specs))
+        specs = [s.contiguous() for s in specs]
+        nf = specs[0].numel() // self.plan.nlm
+        self.plan._batch(nf)
+        self.plan._stream()
+        q = self._spec_ptrs(kind, specs)
+        self.lib.shtns_b200_legendre_synth_rows(self.plan._cfg, kind, q[0], q[1], q[2], self.m0, self.m1,
+                                                self._ltr(ltr), self.world, self.bounds, self.ptrs)
+        capi.check(self.lib)
+
+    def analys_rows(self, n, lead, device, ltr=None):
+        """Legendre stage of this rank's orders from the owners' buffers."""
+        kind = self._kind(n)
+        nf = int(np.prod(lead)) if len(lead) else 1
+        outs = [torch.zeros(tuple(lead) + (self.plan.nlm,), dtype=torch.complex128, device=device) for _ in range(n)]
+        self.plan._batch(nf)
+        self.plan._stream()
+        q = self._spec_ptrs(kind, outs)
+        self.lib.shtns_b200_legendre_analys_rows(self.plan._cfg, kind, self.world, self.bounds, self.ptrs,
+                                                 q[0], q[1], q[2], self.m0, self.m1, self._ltr(ltr))
+        capi.check(self.lib)
+        return outs
+
+    def own_rows(self, nfc):
+        return self.buf.tensor()[:nfc]
+
+    def analys_fourier_rows(self, *blocks, ltr=None):
+        """FFT of this rank's blocks into its own row buffer."""
+        kind = self._kind(len(blocks))
+        blocks = [b.contiguous() for b in blocks]
+        bs = self.block_shape()
+        nf = blocks[0].numel() // (bs[0] * bs[1])
+        self.stages.fourier_analys(kind, blocks, self.own_rows(len(blocks) * nf), self.nrows, self._ltr(ltr), nf)
+
+    # ---------------- whole directions ----------------
+    def synth(self, *specs, ltr=None):
+        nf = specs[0].numel() // self.plan.nlm
+        nfc = len(specs) * nf
+        self.prepare(nfc)
+        self.barrier()
+        self.synth_rows(*specs, ltr=ltr)
+        self.barrier()
+        outs = self.synth_fourier(self.own_rows(nfc), specs[0].shape[:-1], len(specs), ltr)
+        return outs[0] if len(outs) == 1 else tuple(outs)
+
+    def analys(self, *blocks, ltr=None):
+        bs = self.block_shape()
+        nf = blocks[0].numel() // (bs[0] * bs[1])
+        nfc = len(blocks) * nf
+        self.prepare(nfc)
+        self.barrier()
+        self.analys_fourier_rows(*blocks, ltr=ltr)
+        self.barrier()
+        outs = self.analys_rows(len(blocks), blocks[0].shape[:-2], blocks[0].device, ltr)
+        return outs[0] if len(outs) == 1 else tuple(outs)

@@ -122,3 +122,62 @@ def test_order_split_rejects_bad_ranges():
     with pytest.raises(SHTError):
         st.fourier_synth(0, F, [torch.zeros(3, 64, dtype=torch.float64, device="cuda")], 3, 31, 1)  # odd rows
     assert np.isfinite(F.cpu().numpy()).all()
+
+
+def _fused_splits(s, world, nfc):
+    from shtns_b200.ordersplit import FusedOrderSplit
+    splits = [FusedOrderSplit(s, rank=r, world=world, barrier=lambda: None) for r in range(world)]
+    for sp in splits:
+        sp.allocate(nfc)
+    ptrs = [sp.buf.ptr for sp in splits]
+    for sp in splits:
+        sp.set_row_buffers(ptrs)
+    return splits
+
+
+@pytest.mark.parametrize("world,layout,kind,nf", [(2, SHT_PHI_CONTIGUOUS, 1, 2), (3, SHT_THETA_CONTIGUOUS, 3, 2),
+                                                  (4, SHT_PHI_CONTIGUOUS, 2, 2), (2, SHT_THETA_CONTIGUOUS, 1, 1)])
+def test_fused_order_split_emulated_ranks(world, layout, kind, nf):
+    """The exchange fused into the Legendre kernels: every emulated rank's
+    synthesis stores its rows into all ranks' row buffers (local buffers
+    here), each rank's FFT then reads its own; the analysis runs backwards.
+    Same kernels as the whole transform: equal to rounding."""
+    s = make_plan(127, 127, 1, 192, 256, layout)
+    specs = [torch.from_numpy(rand_spec(127, 127, 1, 60 + i, nfields=nf, zero_l0=(kind > 1))).cuda()
+             for i in range(kind)]
+    if kind == 2:
+        specs = specs[:2]
+    n = len(specs)
+    splits = _fused_splits(s, world, n * nf)
+    for sp in splits:
+        sp.synth_rows(*specs)
+    blocks = [sp.synth_fourier(sp.own_rows(n * nf), specs[0].shape[:-1], n) for sp in splits]
+    axis = -2 if splits[0].phi_contiguous else -1
+    got = [torch.cat([b[c] for b in blocks], dim=axis) for c in range(n)]
+    ref = s.synth(*specs)
+    ref = list(ref) if isinstance(ref, tuple) else [ref]
+    for a, b in zip(ref, got):
+        assert relerr(a.cpu().numpy(), b.cpu().numpy()) < 1e-14
+    for sp in splits:
+        sp.analys_fourier_rows(*[sp.local_rows(v) for v in ref])
+    parts = [sp.analys_rows(n, specs[0].shape[:-1], specs[0].device) for sp in splits]
+    back = s.analys(*ref)
+    back = list(back) if isinstance(back, tuple) else [back]
+    for c in range(n):
+        q = torch.zeros_like(back[c])
+        for sp, p in zip(splits, parts):
+            q[..., sp.spec_slice()] = p[c][..., sp.spec_slice()]
+        assert relerr(back[c].cpu().numpy(), q.cpu().numpy()) < 1e-14
+    for sp in splits:
+        sp.release()
+
+
+def test_fused_order_split_single_process_call():
+    from shtns_b200.ordersplit import FusedOrderSplit
+    s = make_plan(95, 95, 1, 144, 192, SHT_PHI_CONTIGUOUS)
+    q = torch.from_numpy(rand_spec(95, 95, 1, 70, nfields=3)).cuda()
+    sp = FusedOrderSplit(s, rank=0, world=1)
+    v = sp.synth(q)
+    assert relerr(s.synth(q).cpu().numpy(), v.cpu().numpy()) < 1e-14
+    assert relerr(q.cpu().numpy(), sp.analys(v).cpu().numpy()) < 1e-11
+    sp.release()
