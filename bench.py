@@ -655,14 +655,14 @@ def run_ordersplit(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
     import shtns_b200
     from shtns_b200 import capi
-    from shtns_b200.ordersplit import OrderSplit
+    from shtns_b200.ordersplit import OrderSplit, FusedOrderSplit
     from tests.common import rand_spec
     lib = capi.load()
     nf = args.fields if args.fields != NFIELDS else 1
     sh = shtns_b200.sht(HD_L)
     sh.set_grid(HD_NLAT, HD_NPHI, flags=shtns_b200.sht_quick_init | shtns_b200.SHT_THETA_CONTIGUOUS, polar_opt=EPS)
     q = torch.from_numpy(rand_spec(HD_L, HD_L, 1, 400, power=1.0, nfields=nf)).to(dev)
-    sp = OrderSplit(sh, rank=rank, world=world)
+    sp = (FusedOrderSplit if args.exchange == "fused" else OrderSplit)(sh, rank=rank, world=world)
     out = {}
 
     def step():
@@ -737,7 +737,9 @@ def run_ordersplit(args):
             "data": "synthetic (seeded N(0,1)/(l+1))",
             "config": {"workload": "lmax4095_1field_ordersplit", "lmax": HD_L, "nlat": HD_NLAT, "nphi": HD_NPHI,
                        "fields": nf, "polar_eps": EPS, "layout": "theta-contiguous",
-                       "parallelism": "orders split over %d rank(s), one all-to-all per direction" % world,
+                       "parallelism": "orders split over %d rank(s), %s" % (world, (
+                           "exchange fused into the Legendre kernels (peer row buffers)" if args.exchange == "fused"
+                           else "one all-to-all per direction")),
                        "orders_per_rank": [b - a + 1 for a, b in sp.orders],
                        "exchange_bytes_per_step": 2 * fourier_bytes * (world - 1) / max(world, 1),
                        "l2": "no flush: per-step working set > 2 GB > 126 MB L2"},
@@ -875,6 +877,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-chunks", type=int, default=E2E_CHUNKS,
                     help="field chunks (streams) of the end-to-end step")
+    ap.add_argument("--exchange", default="nccl", choices=["nccl", "fused"],
+                    help="ordersplit: NCCL all_to_all_single, or rows stored into peers' buffers by the Legendre kernels")
     ap.add_argument("--workload", default="qst", choices=["qst", "uneven", "highdeg", "ordersplit", "local"],
                     help="qst: lmax=511 vector transforms of 64 fields (default); "
                          "uneven: 256 scalar fields of lmax 63..1023 through a plan group; "
