@@ -728,7 +728,7 @@ def run_ordersplit(args):
         ms, err = float(t[0]), float(t[1])
     if rank == 0:
         peak = fp64_gemm_peak(torch, dev)
-        ach = flops / (st[1] * 1e-3) / 1e12
+        ach = flops / (st[1] * 1e-3) / 1e12 if st[1] > 0 else None
         fourier_bytes = 16.0 * (HD_L + 1) * HD_NLAT * nf
         line = {
             "metric": METRIC, "value": nf / (ms * 1e-3), "unit": HD_UNIT.replace("lmax=4095", "one field, lmax=4095"),
@@ -747,7 +747,7 @@ def run_ordersplit(args):
                                 "legendre_analysis": st[4], "prologue": st[0], "epilogue": st[5]},
             "roofline": {"kernel": "leg_synth_simt_kernel (FP64 FMA: one field), rank 0's orders", "bound": "fp64",
                          "achieved": ach,
-                         "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+                         "peak": peak, "unit": "TFLOP/s", "frac": ach / peak if ach else None, "traffic": None,
                          "work_per_launch": "8 flop per theta-row x field-component x Ishioka step (the "
                                             "recurrence's 4 more are not counted)",
                          "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (the FP64 FMA pipe has "

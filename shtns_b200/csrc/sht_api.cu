@@ -1202,11 +1202,15 @@ extern "C" void shtns_b200_legendre_synth_rows(shtns_cfg s, int kind, cplx* Q, c
 	pp.Q = reinterpret_cast<const double2*>(Q);
 	pp.S = reinterpret_cast<const double2*>(S);
 	pp.T = reinterpret_cast<const double2*>(T);
+	shtb_stage_begin(s, 0);
 	launch_prep_synth(pp, s->comp_stream);
+	shtb_stage_end(s);
 	LegParams lp = leg_params(s, j);
 	lp.im0 = m0; lp.mlim = mhi;
 	lp.rb = rb;
+	shtb_stage_begin(s, 1);
 	launch_leg_synth(lp, s->comp_stream);
+	shtb_stage_end(s);
 	check_launch("order-split Legendre synthesis launch");
 }
 
@@ -1223,14 +1227,18 @@ extern "C" void shtns_b200_legendre_analys_rows(shtns_cfg s, int kind, int nblk,
 		LegParams lp = leg_params(s, j);
 		lp.im0 = m0; lp.mlim = std::min(m1, j.mlim);
 		lp.rb = rb;
+		shtb_stage_begin(s, 4);
 		launch_leg_analys(lp, (j.llim + j.vec_extra - m0 * s->mres) / 2 + 1, s->comp_stream);
+		shtb_stage_end(s);
 	}
 	PrepParams pp = prep_params(s, j);
 	pp.im0 = m0;
 	pp.Qo = reinterpret_cast<double2*>(Q);
 	pp.So = reinterpret_cast<double2*>(S);
 	pp.To = reinterpret_cast<double2*>(T);
+	shtb_stage_begin(s, 5);
 	launch_post_analys_m(pp, m1, s->comp_stream);
+	shtb_stage_end(s);
 	check_launch("order-split Legendre analysis launch");
 }
 

@@ -158,9 +158,9 @@ struct LegParams {
 	RowBlocks rb;                        // rows in per-block buffers instead of F (rb.n > 0)
 };
 
-// address of Fourier row `row` of field-component fc, order im (block-split
-// layouts go through the out-of-line forms below, so that the plain layout
-// keeps its registers)
+// address of Fourier row `row` of field-component fc, order im (the
+// tensor-core tiles are compiled separately for the block-split layout, so
+// that the plain one keeps its registers)
 __device__ __forceinline__ double2* fourier_row(const LegParams& p, int fc, int im, int row)
 {
 	if (p.rb.n == 0) return p.F + (long)fc * p.fstride + (long)im * p.nlat + row;
@@ -168,22 +168,6 @@ __device__ __forceinline__ double2* fourier_row(const LegParams& p, int fc, int 
 	while (b + 1 < p.rb.n && row >= p.rb.lat0[b + 1]) b++;
 	const int r0 = p.rb.lat0[b];
 	return p.rb.base[b] + ((long)fc * p.rb.mstride + im) * (p.rb.lat0[b + 1] - r0) + (row - r0);
-}
-
-static __device__ __noinline__ void fourier_row_store2(const LegParams& p, int fc, int im, int rn, int rs, double2 vn, double2 vs)
-{
-	*fourier_row(p, fc, im, rn) = vn;
-	*fourier_row(p, fc, im, rs) = vs;
-}
-
-struct RowPair { double2 n, s; };
-
-static __device__ __noinline__ RowPair fourier_row_load2(const LegParams& p, int fc, int im, int rn, int rs)
-{
-	RowPair r;
-	r.n = __ldg(fourier_row(p, fc, im, rn));
-	r.s = __ldg(fourier_row(p, fc, im, rs));
-	return r;
 }
 
 struct PrepParams {

@@ -300,7 +300,8 @@ __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 
 // WM = warps along the rows (2: 64 rows x 64 columns per CTA; 4: 128 rows x
 // 32 columns, for calls with at most 8 field-components).
-template <int SEG, int WM>
+// RB: Fourier rows in per-block buffers (p.rb) instead of the plain F
+template <int SEG, int WM, bool RB = false>
 __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int tb, int nb)
 {
 	constexpr int WN = 8 / WM, BM = 32 * WM, BN = 16 * WN;
@@ -427,11 +428,12 @@ __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int t
 		}
 		const int rn = p.south_first ? p.nlat - 1 - t : t;
 		const int rs = p.nlat - 1 - rn;
-		if (p.rb.n == 0) {
+		if constexpr (!RB) {
 			Ff[rn] = make_double2(nr, ni);
 			Ff[rs] = make_double2(sr, si);
 		} else {
-			fourier_row_store2(p, fc, im, rn, rs, make_double2(nr, ni), make_double2(sr, si));
+			*fourier_row(p, fc, im, rn) = make_double2(nr, ni);
+			*fourier_row(p, fc, im, rs) = make_double2(sr, si);
 		}
 	}
 }
@@ -446,7 +448,7 @@ __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int t
 
 // WM = warps along the k rows (2: 64 k x 64 columns per CTA; 4: 128 k x 32
 // columns, for calls with at most 8 field-components).
-template <int SEG, int WM>
+template <int SEG, int WM, bool RB = false>
 __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int kb, int nb)
 {
 	constexpr int WN = 8 / WM, BM = 32 * WM, BN = 16 * WN;
@@ -496,14 +498,13 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 			if (t < p.nlat_2 && t >= tmm && fc < p.nfc) {
 				const int rn = p.south_first ? p.nlat - 1 - t : t;
 				const int rs = p.nlat - 1 - rn;
-				if (p.rb.n == 0) {
+				if constexpr (!RB) {
 					const double2* Ff = p.F + (long)fc * p.fstride + (long)im * p.nlat;
 					fnn[u] = __ldg(Ff + rn);
 					fsn[u] = __ldg(Ff + rs);
 				} else {
-					const RowPair r = fourier_row_load2(p, fc, im, rn, rs);
-					fnn[u] = r.n;
-					fsn[u] = r.s;
+					fnn[u] = __ldg(fourier_row(p, fc, im, rn));
+					fsn[u] = __ldg(fourier_row(p, fc, im, rs));
 				}
 			}
 		}
@@ -601,17 +602,17 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 }
 
 // Single-plan kernels: blockIdx.y = order - p.im0, blockIdx.x = (row tile, column tile).
-template <int SEG, int WM>
-__global__ void __launch_bounds__(LG_THREADS, WM == 1 ? 2 : 3) leg_synth_kernel(const __grid_constant__ LegParams p)
+template <int SEG, int WM, bool RB>
+__global__ void __launch_bounds__(LG_THREADS, WM == 1 ? 2 : 3) leg_synth_kernel(LegParams p)
 {
 	const int ntb = (p.nlat_2 + 32 * WM - 1) / (32 * WM);
-	leg_synth_tile<SEG, WM>(p, p.im0 + blockIdx.y, blockIdx.x % ntb, blockIdx.x / ntb);
+	leg_synth_tile<SEG, WM, RB>(p, p.im0 + blockIdx.y, blockIdx.x % ntb, blockIdx.x / ntb);
 }
 
-template <int SEG, int WM>
-__global__ void __launch_bounds__(LG_THREADS, WM == 1 ? 2 : 3) leg_analys_kernel(const __grid_constant__ LegParams p, int nkb)
+template <int SEG, int WM, bool RB>
+__global__ void __launch_bounds__(LG_THREADS, WM == 1 ? 2 : 3) leg_analys_kernel(LegParams p, int nkb)
 {
-	leg_analys_tile<SEG, WM>(p, p.im0 + blockIdx.y, blockIdx.x % nkb, blockIdx.x / nkb);
+	leg_analys_tile<SEG, WM, RB>(p, p.im0 + blockIdx.y, blockIdx.x % nkb, blockIdx.x / nkb);
 }
 
 // Persistent multi-plan kernels: CTAs (one wave) take work items (plan,
@@ -671,9 +672,12 @@ void launch_leg_synth_wm(const LegParams& p, cudaStream_t st)
 	const int nnb = (p.ncol + BN - 1) / BN;
 	dim3 grid(ntb * nnb, p.mlim + 1 - p.im0);
 	switch (p.ckseg) {
-		case 8: leg_synth_kernel<8, WM><<<grid, LG_THREADS, 0, st>>>(p); break;
-		case 16: leg_synth_kernel<16, WM><<<grid, LG_THREADS, 0, st>>>(p); break;
-		default: leg_synth_kernel<32, WM><<<grid, LG_THREADS, 0, st>>>(p); break;
+		case 8: if (p.rb.n) leg_synth_kernel<8, WM, true><<<grid, LG_THREADS, 0, st>>>(p);
+		        else leg_synth_kernel<8, WM, false><<<grid, LG_THREADS, 0, st>>>(p); break;
+		case 16: if (p.rb.n) leg_synth_kernel<16, WM, true><<<grid, LG_THREADS, 0, st>>>(p);
+		         else leg_synth_kernel<16, WM, false><<<grid, LG_THREADS, 0, st>>>(p); break;
+		default: if (p.rb.n) leg_synth_kernel<32, WM, true><<<grid, LG_THREADS, 0, st>>>(p);
+		         else leg_synth_kernel<32, WM, false><<<grid, LG_THREADS, 0, st>>>(p); break;
 	}
 }
 
@@ -685,9 +689,12 @@ void launch_leg_analys_wm(const LegParams& p, int kmax_all, cudaStream_t st)
 	const int nnb = (p.ncol + BN - 1) / BN;
 	dim3 grid(nkb * nnb, p.mlim + 1 - p.im0);
 	switch (p.ckseg) {
-		case 8: leg_analys_kernel<8, WM><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
-		case 16: leg_analys_kernel<16, WM><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
-		default: leg_analys_kernel<32, WM><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
+		case 8: if (p.rb.n) leg_analys_kernel<8, WM, true><<<grid, LG_THREADS, 0, st>>>(p, nkb);
+		        else leg_analys_kernel<8, WM, false><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
+		case 16: if (p.rb.n) leg_analys_kernel<16, WM, true><<<grid, LG_THREADS, 0, st>>>(p, nkb);
+		         else leg_analys_kernel<16, WM, false><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
+		default: if (p.rb.n) leg_analys_kernel<32, WM, true><<<grid, LG_THREADS, 0, st>>>(p, nkb);
+		         else leg_analys_kernel<32, WM, false><<<grid, LG_THREADS, 0, st>>>(p, nkb); break;
 	}
 }
 

@@ -25,6 +25,14 @@ namespace {
 // time (broadcast loads).
 #define SS_KC 64                       // k per staged chunk (a multiple of every SEG)
 
+// address of a Fourier row: plain layout, or per-block buffers when RB
+template <bool RB>
+__device__ __forceinline__ double2* simt_row(const LegParams& p, int fc, int im, int row)
+{
+	if constexpr (RB) return fourier_row(p, fc, im, row);
+	else return p.F + (long)fc * p.fstride + (long)im * p.nlat + row;
+}
+
 template <int NFC>
 __device__ __forceinline__ void simt_acc(double (&a)[NFC][4], const double* cs, double y)
 {
@@ -40,7 +48,7 @@ __device__ __forceinline__ void simt_acc(double (&a)[NFC][4], const double* cs, 
 }
 
 // fold hemispheres, scale, store the two Fourier rows of north row t
-template <int NFC>
+template <int NFC, bool RB>
 __device__ __forceinline__ void simt_synth_store(const LegParams& p, int im, int tmm, int t, const double (&a)[NFC][4])
 {
 	if (t >= p.nlat_2) return;
@@ -61,12 +69,12 @@ __device__ __forceinline__ void simt_synth_store(const LegParams& p, int im, int
 			const double s = p.w[t] * (m > 0 ? p.mpos_inv : 1.0) / (p.nphi * (m > 0 ? 2.0 : 1.0));
 			nr *= s; ni *= s; sr *= s; si *= s;
 		}
-		*fourier_row(p, f, im, rn) = make_double2(nr, ni);
-		*fourier_row(p, f, im, rs) = make_double2(sr, si);
+		*simt_row<RB>(p, f, im, rn) = make_double2(nr, ni);
+		*simt_row<RB>(p, f, im, rs) = make_double2(sr, si);
 	}
 }
 
-template <int SEG, int NFC>
+template <int SEG, int NFC, bool RB>
 __global__ void __launch_bounds__(128) leg_synth_simt_kernel(LegParams p)
 {
 	constexpr int W = 2 + 4 * NFC;     // staged doubles per k: (c_{2k-2}, c_{2k-1}), then per fc E re, E im, O re, O im
@@ -136,8 +144,8 @@ __global__ void __launch_bounds__(128) leg_synth_simt_kernel(LegParams p)
 			}
 		}
 	}
-	simt_synth_store<NFC>(p, im, tmm, ta, aa);
-	simt_synth_store<NFC>(p, im, tmm, tc, ac);
+	simt_synth_store<NFC, RB>(p, im, tmm, ta, aa);
+	simt_synth_store<NFC, RB>(p, im, tmm, tc, ac);
 }
 
 // ---------------------------------------------------------------------------
@@ -150,7 +158,7 @@ __global__ void __launch_bounds__(128) leg_synth_simt_kernel(LegParams p)
 #define SA_TB 16                       // north rows per chunk
 #define SA_NT 128                      // largest block
 
-template <int SEG, int NFC>
+template <int SEG, int NFC, bool RB>
 __global__ void __launch_bounds__(SA_NT) leg_analys_simt_kernel(LegParams p)
 {
 	constexpr int SPT = 32 / SEG;      // segments per generator thread: (2 nt / SEG) / (nt / 16)
@@ -198,8 +206,8 @@ __global__ void __launch_bounds__(SA_NT) leg_analys_simt_kernel(LegParams p)
 			if (gf < NFC && tg < p.nlat_2 && tg >= tmm) {
 				const int rn = p.south_first ? p.nlat - 1 - tg : tg;
 				const int rs = p.nlat - 1 - rn;
-				fn[i] = __ldg(fourier_row(p, gf, im, rn));
-				fs[i] = __ldg(fourier_row(p, gf, im, rs));
+				fn[i] = __ldg(simt_row<RB>(p, gf, im, rn));
+				fs[i] = __ldg(simt_row<RB>(p, gf, im, rs));
 			}
 		}
 	};
@@ -301,7 +309,7 @@ __global__ void __launch_bounds__(SA_NT) leg_analys_simt_kernel(LegParams p)
 #define SR_NT 64
 #define SR_NV 64                       // partial sums per thread
 
-template <int SEG>
+template <int SEG, bool RB>
 __global__ void __launch_bounds__(SR_NT) leg_analys_reg_kernel(LegParams p)
 {
 	constexpr int NFC = 1;
@@ -340,8 +348,8 @@ __global__ void __launch_bounds__(SR_NT) leg_analys_reg_kernel(LegParams p)
 		const int rs = p.nlat - 1 - rn;
 		#pragma unroll
 		for (int f = 0; f < NFC; f++) {
-			nfn[f] = __ldg(fourier_row(p, f, im, rn));
-			nfs[f] = __ldg(fourier_row(p, f, im, rs));
+			nfn[f] = __ldg(simt_row<RB>(p, f, im, rn));
+			nfs[f] = __ldg(simt_row<RB>(p, f, im, rs));
 		}
 		#pragma unroll
 		for (int b = 0; b < NSB; b++) {
@@ -433,26 +441,40 @@ __global__ void __launch_bounds__(SR_NT) leg_analys_reg_kernel(LegParams p)
 	}
 }
 
+template <int SEG, bool RB>
+void synth_seg_rb(const LegParams& p, dim3 grid, int nt, cudaStream_t st)
+{
+	switch (p.nfc) {
+		case 1: leg_synth_simt_kernel<SEG, 1, RB><<<grid, nt, 0, st>>>(p); break;
+		case 2: leg_synth_simt_kernel<SEG, 2, RB><<<grid, nt, 0, st>>>(p); break;
+		case 3: leg_synth_simt_kernel<SEG, 3, RB><<<grid, nt, 0, st>>>(p); break;
+		default: leg_synth_simt_kernel<SEG, 4, RB><<<grid, nt, 0, st>>>(p); break;
+	}
+}
+
 template <int SEG>
 void synth_seg(const LegParams& p, dim3 grid, int nt, cudaStream_t st)
 {
+	if (p.rb.n) synth_seg_rb<SEG, true>(p, grid, nt, st);
+	else synth_seg_rb<SEG, false>(p, grid, nt, st);
+}
+
+template <int SEG, bool RB>
+void analys_seg_rb(const LegParams& p, dim3 grid, int nt, cudaStream_t st)
+{
 	switch (p.nfc) {
-		case 1: leg_synth_simt_kernel<SEG, 1><<<grid, nt, 0, st>>>(p); break;
-		case 2: leg_synth_simt_kernel<SEG, 2><<<grid, nt, 0, st>>>(p); break;
-		case 3: leg_synth_simt_kernel<SEG, 3><<<grid, nt, 0, st>>>(p); break;
-		default: leg_synth_simt_kernel<SEG, 4><<<grid, nt, 0, st>>>(p); break;
+		case 1: leg_analys_simt_kernel<SEG, 1, RB><<<grid, nt, 0, st>>>(p); break;
+		case 2: leg_analys_simt_kernel<SEG, 2, RB><<<grid, nt, 0, st>>>(p); break;
+		case 3: leg_analys_simt_kernel<SEG, 3, RB><<<grid, nt, 0, st>>>(p); break;
+		default: leg_analys_simt_kernel<SEG, 4, RB><<<grid, nt, 0, st>>>(p); break;
 	}
 }
 
 template <int SEG>
 void analys_seg(const LegParams& p, dim3 grid, int nt, cudaStream_t st)
 {
-	switch (p.nfc) {
-		case 1: leg_analys_simt_kernel<SEG, 1><<<grid, nt, 0, st>>>(p); break;
-		case 2: leg_analys_simt_kernel<SEG, 2><<<grid, nt, 0, st>>>(p); break;
-		case 3: leg_analys_simt_kernel<SEG, 3><<<grid, nt, 0, st>>>(p); break;
-		default: leg_analys_simt_kernel<SEG, 4><<<grid, nt, 0, st>>>(p); break;
-	}
+	if (p.rb.n) analys_seg_rb<SEG, true>(p, grid, nt, st);
+	else analys_seg_rb<SEG, false>(p, grid, nt, st);
 }
 
 } // namespace
@@ -484,7 +506,8 @@ template <int SEG>
 void analys_reg_seg(const LegParams& p, int kmax_all, cudaStream_t st)
 {
 	dim3 grid((kmax_all + 15) / 16, p.mlim + 1 - p.im0);
-	leg_analys_reg_kernel<SEG><<<grid, SR_NT, 0, st>>>(p);
+	if (p.rb.n) leg_analys_reg_kernel<SEG, true><<<grid, SR_NT, 0, st>>>(p);
+	else leg_analys_reg_kernel<SEG, false><<<grid, SR_NT, 0, st>>>(p);
 }
 
 void launch_leg_analys_simt(const LegParams& p, int kmax_all, cudaStream_t st)
