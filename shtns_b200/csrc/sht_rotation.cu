@@ -25,6 +25,8 @@
 #include <cstring>
 #include <vector>
 
+#define ROT_STREAMS_DECL 4
+
 struct shtns_rot_ {
 	int lmax, mmax;
 	int norm;
@@ -37,6 +39,8 @@ struct shtns_rot_ {
 	double2* d_e;            // e^{-i m alpha} (m <= lmax), then e^{-i m gamma}
 	void* d_buf; size_t buf_cap;
 	int ready;               // angles set
+	cudaStream_t side[ROT_STREAMS_DECL];   // degree groups run concurrently on these
+	cudaEvent_t ev[ROT_STREAMS_DECL + 1];
 };
 
 void launch_plm_table(shtns_cfg s, double x, double st, double* out, cudaStream_t st_);
@@ -85,8 +89,8 @@ __device__ double2 qin(const RotParams& p, int l, int m)
 }
 
 // quarter element x = d(a, b), b >= |a|: row-type sums (R_a, R_-a), column sums (R_b, R_-b)
-#define ROT_NT 512                 // threads per CTA at most
-#define ROT_LMAX 2047              // 4 columns per thread at most
+#define ROT_NT 256                 // threads per CTA at most (two CTAs per SM at 128 registers)
+#define ROT_LMAX 2047              // 8 columns per thread at most
 
 template <int KC>
 __device__ __forceinline__ void apply_elem(int a, int b, int k, double x, double2 qa, double2 qma, const double2 (&qp)[KC],
@@ -147,7 +151,7 @@ __device__ __forceinline__ void store_row_sums(const double* red, int nw, int la
 }
 
 template <int KC>
-__global__ void __launch_bounds__(ROT_NT) rot_kernel(RotParams p)
+__global__ void __launch_bounds__(ROT_NT, KC <= 4 ? 2 : 1) rot_kernel(RotParams p)
 {
 	extern __shared__ double sm[];
 	const int l = p.l1 - blockIdx.x;                 // largest degrees first
@@ -334,21 +338,38 @@ void launch_rot(const RotParams& p, int nt, size_t smem, cudaStream_t st)
 	rot_kernel<KC><<<p.l1 - p.l0 + 1, nt, smem, st>>>(p);
 }
 
-// all degrees 1..lmax, grouped by size (threads and shared memory per group)
-bool run_rotation(RotParams p, int lmin, int lmax, cudaStream_t st)
+void launch_rot_group(RotParams p, int l0, int l1, cudaStream_t st)
 {
+	const int nt = std::min(ROT_NT, (l1 + 1 + 31) / 32 * 32);
+	const int kc = (l1 + 1 + nt - 1) / nt;
+	const size_t smem = sizeof(double) * (4 * (size_t)(l1 + 2) + 256);
+	p.l0 = l0; p.l1 = l1;
+	if (kc <= 1) launch_rot<1>(p, nt, smem, st);
+	else if (kc <= 2) launch_rot<2>(p, nt, smem, st);
+	else if (kc <= 4) launch_rot<4>(p, nt, smem, st);
+	else launch_rot<8>(p, nt, smem, st);
+	shtb_count_launch();
+}
+
+// all degrees 1..lmax, grouped by size (threads and shared memory per
+// group); the groups are independent and run concurrently on the side
+// streams, largest first, joined back into st
+bool run_rotation(shtns_rot r, RotParams p, int lmin, int lmax, cudaStream_t st)
+{
+	std::vector<std::pair<int, int>> groups;
 	for (int l0 = lmin; l0 <= lmax;) {
 		int l1 = (l0 < 32) ? 31 : 2 * l0 - 1;
 		if (l1 > lmax) l1 = lmax;
-		const int nt = std::min(ROT_NT, (l1 + 1 + 31) / 32 * 32);
-		const int kc = (l1 + 1 + nt - 1) / nt;
-		const size_t smem = sizeof(double) * (4 * (size_t)(l1 + 2) + 256);
-		p.l0 = l0; p.l1 = l1;
-		if (kc <= 1) launch_rot<1>(p, nt, smem, st);
-		else if (kc <= 2) launch_rot<2>(p, nt, smem, st);
-		else launch_rot<4>(p, nt, smem, st);
-		shtb_count_launch();
+		groups.push_back({l0, l1});
 		l0 = l1 + 1;
+	}
+	cudaEventRecord(r->ev[ROT_STREAMS_DECL], st);
+	for (int i = 0; i < ROT_STREAMS_DECL; i++) cudaStreamWaitEvent(r->side[i], r->ev[ROT_STREAMS_DECL], 0);
+	for (size_t g = groups.size(); g-- > 0;)
+		launch_rot_group(p, groups[g].first, groups[g].second, r->side[(groups.size() - 1 - g) % ROT_STREAMS_DECL]);
+	for (int i = 0; i < ROT_STREAMS_DECL; i++) {
+		cudaEventRecord(r->ev[i], r->side[i]);
+		cudaStreamWaitEvent(st, r->ev[i], 0);
 	}
 	return shtb_cuda_ok(cudaGetLastError(), "rotation launch");
 }
@@ -386,7 +407,7 @@ void rot_apply(shtns_rot r, const cplx* Qh, cplx* Rh, int cplx_field)
 	} else {
 		rot_z_kernel<<<1, 32, 0, st>>>(p, 1);               // degree 0 is invariant
 		shtb_count_launch();
-		if (!run_rotation(p, 1, r->lmax, st)) return;
+		if (!run_rotation(r, p, 1, r->lmax, st)) return;
 	}
 	if (!shtb_cuda_ok(cudaGetLastError(), "rotation launch")) return;
 	cudaMemcpyAsync(Rh, out, sizeof(double2) * n, cudaMemcpyDeviceToHost, st);
@@ -417,12 +438,16 @@ extern "C" shtns_rot shtns_rotation_create(const int lmax, const int mmax, int n
 	}
 	r->d_plm = static_cast<double*>(d);
 	r->d_e = reinterpret_cast<double2*>(static_cast<char*>(d) + plm_bytes);
+	for (int i = 0; i < ROT_STREAMS_DECL; i++) cudaStreamCreateWithFlags(&r->side[i], cudaStreamNonBlocking);
+	for (int i = 0; i <= ROT_STREAMS_DECL; i++) cudaEventCreateWithFlags(&r->ev[i], cudaEventDisableTiming);
 	return r;
 }
 
 extern "C" void shtns_rotation_destroy(shtns_rot r)
 {
 	if (!r) return;
+	for (int i = 0; i < ROT_STREAMS_DECL; i++) if (r->side[i]) cudaStreamDestroy(r->side[i]);
+	for (int i = 0; i <= ROT_STREAMS_DECL; i++) if (r->ev[i]) cudaEventDestroy(r->ev[i]);
 	if (r->d_plm) cudaFree(r->d_plm);
 	if (r->d_buf) cudaFree(r->d_buf);
 	if (r->leg) shtns_destroy(r->leg);
@@ -504,7 +529,8 @@ extern "C" int shtns_rotation_wigner_d_matrix(shtns_rot r, const int l, double* 
 	const size_t smem = sizeof(double) * (4 * (size_t)(l + 2) + 256);
 	if (kc <= 1) launch_rot<1>(p, nt, smem, st);
 	else if (kc <= 2) launch_rot<2>(p, nt, smem, st);
-	else launch_rot<4>(p, nt, smem, st);
+	else if (kc <= 4) launch_rot<4>(p, nt, smem, st);
+	else launch_rot<8>(p, nt, smem, st);
 	shtb_count_launch();
 	if (!shtb_cuda_ok(cudaGetLastError(), "Wigner matrix launch")) return 0;
 	cudaMemcpyAsync(mx, p.wig, sizeof(double) * w * w, cudaMemcpyDeviceToHost, st);
