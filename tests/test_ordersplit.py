@@ -161,3 +161,83 @@ def test_order_split_exchange_matches_single_process(world, layout):
     assert relerr(sh.analys(v_ref), qa) < 1e-14
     assert relerr(q, qa) < 1e-12                      # round trip
     assert relerr(sh.synth(q, ltr=20), vt) < 1e-14
+
+
+class FakeLib:
+    """Stand-in for the CUDA library's buffer and IPC entry points: pointers
+    are integers, a handle encodes (rank, pointer), opening a peer's handle
+    returns a pointer tagged with that peer."""
+
+    def __init__(self, rank):
+        self.rank = rank
+        self.next = 0x1000 * (rank + 1)
+        self.opened, self.closed, self.freed = [], [], []
+
+    def shtns_b200_alloc(self, nbytes):
+        self.next += 0x100
+        return self.next
+
+    def shtns_b200_free(self, p):
+        self.freed.append(p.value)
+
+    def shtns_b200_ipc_handle(self, p, h):
+        data = ("%d:%d" % (self.rank, p.value)).encode().ljust(64, b"\0")
+        for i, b in enumerate(data):
+            h[i] = bytes([b])
+        return 0
+
+    def shtns_b200_ipc_open(self, h):
+        r, ptr = h.value.decode().split(":")
+        p = 0x7000000 + 0x1000 * int(r) + int(ptr)
+        self.opened.append(p)
+        return p
+
+    def shtns_b200_ipc_close(self, p):
+        self.closed.append(p.value)
+
+    def shtns_b200_status(self):
+        return 0
+
+
+def _fused_worker(rank, world, port, out):
+    import torch.distributed as dist
+    from shtns_b200.ordersplit import FusedOrderSplit
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        lib = FakeLib(rank)
+        plan = SimpleNamespace(lmax=LMAX, mmax=LMAX, mres=1, nlm=528, nlat=NLAT, nphi=NPHI, layout=512, _lib=lib)
+        sp = FusedOrderSplit(plan, costs=np.arange(LMAX + 1, 0, -1))
+        sp.prepare(3)
+        ptrs = list(sp.ptrs)
+        bounds = list(sp.bounds)
+        own = sp.buf.ptr
+        sp.prepare(2)                      # large enough already: no new exchange
+        again = list(sp.ptrs)
+        sp.release()
+        out.put((rank, own, ptrs, again, bounds, lib.opened, lib.closed, lib.freed))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_fused_split_maps_every_ranks_buffer_in_rank_order():
+    world = 3
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_fused_worker, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(out.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    owns = [r[1] for r in res]
+    for rank, own, ptrs, again, bounds, opened, closed, freed in res:
+        assert ptrs == again
+        assert bounds[0] == 0 and bounds[-1] == NLAT and len(bounds) == world + 1
+        for r, p in enumerate(ptrs):
+            assert p == (own if r == rank else 0x7000000 + 0x1000 * r + owns[r])
+        assert sorted(opened) == sorted(closed) and len(opened) == world - 1
+        assert freed == [own]
