@@ -109,9 +109,11 @@ __global__ void ck_kernel(int nlat_2, int mres, int seg, const double* __restric
 #define PT_F 16
 #define PT_W 69          // window length (68 needed), odd stride in 16-byte units
 
-__global__ void __launch_bounds__(256) prep_synth_kernel(PrepParams p)
+__global__ void __launch_bounds__(256, 6) prep_synth_kernel(PrepParams p)
 {
+	constexpr int NE = 2 * PT_F * PT_W, NU = (NE + 255) / 256;
 	__shared__ double2 win[2][PT_F][PT_W];
+	__shared__ int s_comp[PT_F], s_f[PT_F];
 	const int im = p.im0 + blockIdx.z;
 	if (im > p.mlim) return;
 	const int m = im * p.mres;
@@ -124,20 +126,37 @@ __global__ void __launch_bounds__(256) prep_synth_kernel(PrepParams p)
 	const int lrel_max = p.llim - m;
 	const long off = (long)im * (2 * p.lmax + 2 - (im + 1) * p.mres) / 2 + m;   // LM(m, m)
 	const int d0 = 2 * k0 - 1;
-	for (int e = threadIdx.x; e < 2 * PT_F * PT_W; e += blockDim.x) {
+	if (threadIdx.x < PT_F) {
+		const int fc = fc0 + threadIdx.x;
+		const int comp = fc / p.nf;
+		s_comp[threadIdx.x] = (fc < nfc) ? comp : -1;
+		s_f[threadIdx.x] = fc - comp * p.nf;
+	}
+	__syncthreads();
+	// all window loads of a thread are issued before the first is stored
+	double2 v[NU];
+	#pragma unroll
+	for (int u = 0; u < NU; u++) {
+		const int e = threadIdx.x + 256 * u;
 		const int a = e / (PT_F * PT_W), r = e - a * PT_F * PT_W;
 		const int fl = r / PT_W, i = r - fl * PT_W;
-		const int fc = fc0 + fl, d = d0 + i;
-		double2 v = make_double2(0.0, 0.0);
-		if (fc < nfc && d >= 0 && d <= lrel_max) {
-			const int comp = fc / p.nf, f = fc - comp * p.nf;
+		const int d = d0 + i;
+		v[u] = make_double2(0.0, 0.0);
+		const int comp = (e < NE) ? s_comp[fl] : -1;
+		if (comp >= 0 && d >= 0 && d <= lrel_max) {
 			const double2* base = (p.comp_type[comp] == 0) ? (a == 0 ? p.Q : nullptr) : (a == 0 ? p.S : p.T);
-			if (base) {
-				v = base[off + (long)f * p.spec_dist + d];
-				if (m0) v.y = 0.0;
-			}
+			if (base) v[u] = base[off + (long)s_f[fl] * p.spec_dist + d];
 		}
-		win[a][fl][i] = v;
+	}
+	#pragma unroll
+	for (int u = 0; u < NU; u++) {
+		const int e = threadIdx.x + 256 * u;
+		if (e < NE) {
+			const int a = e / (PT_F * PT_W), r = e - a * PT_F * PT_W;
+			const int fl = r / PT_W, i = r - fl * PT_W;
+			if (m0) v[u].y = 0.0;
+			win[a][fl][i] = v[u];
+		}
 	}
 	__syncthreads();
 	const int voff = p.mt.voff[im];
@@ -146,9 +165,9 @@ __global__ void __launch_bounds__(256) prep_synth_kernel(PrepParams p)
 		const int kl = e / PT_F, fl = e - kl * PT_F;
 		const int k = k0 + kl, fc = fc0 + fl;
 		if (k >= kmax || fc >= nfc) continue;
-		const int type = p.comp_type[fc / p.nf];
+		const int type = p.comp_type[s_comp[fl]];
 		// fields from neg_from on carry the order -m (complex-field transforms)
-		const int fld = fc - (fc / p.nf) * p.nf;
+		const int fld = s_f[fl];
 		const double emf = (p.neg_from > 0 && fld >= p.neg_from) ? -em : em;
 		double2 q3[3];
 		#pragma unroll
@@ -193,30 +212,37 @@ __global__ void __launch_bounds__(256) prep_synth_kernel(PrepParams p)
 #define PE_J 64
 #define PE_F 16
 #define PE_R 36          // staged k rows: j0/2-2 .. j0/2+33
+#define PE_S (2 * PE_F + 2)   // row stride in double2: 32 mod 128 bytes, so the 4 rows read by 8 lanes use distinct banks
 
-__device__ __forceinline__ double2 ish_inv_s(const double2 (*E)[PE_F][2], const double* X, int kb, int fl, int j)
+// E[row][2 fl + 0] = even pair (re, im), [2 fl + 1] = odd pair, row = k - kb;
+// Xs[3 row + c] = basis-change coefficients of k
+__device__ __forceinline__ double2 ish_inv_s(const double2 (*E)[PE_S], const double* Xs, int kb, int fl, int j)
 {
-	// E[row][field][0] = even pair (re, im), [1] = odd pair, row = k - kb
 	if (j < 0) return make_double2(0.0, 0.0);
-	const int k = j >> 1;
+	const int r = (j >> 1) - kb;
 	if ((j & 1) == 0) {
-		const double2 e = E[k - kb][fl][0];
-		double2 r = make_double2(X[3 * k] * e.x, X[3 * k] * e.y);
-		if (k > 0) {
-			const double2 e1 = E[k - 1 - kb][fl][0];
-			r.x = fma(X[3 * (k - 1) + 1], e1.x, r.x);
-			r.y = fma(X[3 * (k - 1) + 1], e1.y, r.y);
+		const double2 e = E[r][2 * fl];
+		const double x = Xs[3 * r];
+		double2 q = make_double2(x * e.x, x * e.y);
+		if (j > 1) {
+			const double2 e1 = E[r - 1][2 * fl];
+			const double x1 = Xs[3 * (r - 1) + 1];
+			q.x = fma(x1, e1.x, q.x);
+			q.y = fma(x1, e1.y, q.y);
 		}
-		return r;
+		return q;
 	}
-	const double2 o = E[k - kb][fl][1];
-	return make_double2(X[3 * k + 2] * o.x, X[3 * k + 2] * o.y);
+	const double2 o = E[r][2 * fl + 1];
+	const double x2 = Xs[3 * r + 2];
+	return make_double2(x2 * o.x, x2 * o.y);
 }
 
 __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 {
-	__shared__ double2 sv[PE_R][PE_F][2];     // first component of the group (Q, or V)
-	__shared__ double2 sw[PE_R][PE_F][2];     // second component (W) for the vector group
+	constexpr int NE = PE_R * PE_F * 2, NU = (NE + 255) / 256;
+	__shared__ double2 sv[PE_R][PE_S];     // first component of the group (Q, or V)
+	__shared__ double2 sw[PE_R][PE_S];     // second component (W) for the vector group
+	__shared__ double xs[3 * PE_R];
 	const int im = p.im0 + blockIdx.z;
 	const int m = im * p.mres;
 	const int nl = p.lmax - m + 1;
@@ -234,26 +260,44 @@ __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 	if (!zero_m) {
 		const int cv = scalar_group ? 0 : (has_q ? 1 : 0);
 		const long r0 = p.mt.koff[im];
-		for (int e = threadIdx.x; e < PE_R * PE_F * 2; e += blockDim.x) {
+		// all row loads of a thread are issued before the first is stored
+		double2 v[NU], w[NU];
+		#pragma unroll
+		for (int u = 0; u < NU; u++) {
+			const int e = threadIdx.x + 256 * u;
 			const int r = e / (PE_F * 2), rem = e - r * PE_F * 2;
 			const int fl = rem >> 1, eo = rem & 1;
 			const int k = kb + r, f = f0 + fl;
-			double2 v = make_double2(0.0, 0.0), w = make_double2(0.0, 0.0);
-			if (k >= 0 && k < nk && f < p.nf) {
+			v[u] = make_double2(0.0, 0.0);
+			w[u] = make_double2(0.0, 0.0);
+			if (e < NE && k >= 0 && k < nk && f < p.nf) {
 				const double* row = p.qq + (r0 + k) * p.ncol;
 				const int fcv = cv * p.nf + f;
-				v = *reinterpret_cast<const double2*>(row + 16 * (fcv >> 2) + 2 * (fcv & 3) + 8 * eo);
+				v[u] = *reinterpret_cast<const double2*>(row + 16 * (fcv >> 2) + 2 * (fcv & 3) + 8 * eo);
 				if (!scalar_group) {
 					const int fcw = (cv + 1) * p.nf + f;
-					w = *reinterpret_cast<const double2*>(row + 16 * (fcw >> 2) + 2 * (fcw & 3) + 8 * eo);
+					w[u] = *reinterpret_cast<const double2*>(row + 16 * (fcw >> 2) + 2 * (fcw & 3) + 8 * eo);
 				}
 			}
-			sv[r][fl][eo] = v;
-			sw[r][fl][eo] = w;
+		}
+		// basis-change coefficients of the staged rows (3 (kmax + 1) entries per order)
+		const int kx = (p.lmax + 1 - m) / 2 + 1;
+		const double* X = p.xa + p.mt.xoff[im];
+		for (int e = threadIdx.x; e < 3 * PE_R; e += blockDim.x) {
+			const int k = kb + e / 3;
+			xs[e] = (k >= 0 && k <= kx) ? X[3 * kb + e] : 0.0;
+		}
+		#pragma unroll
+		for (int u = 0; u < NU; u++) {
+			const int e = threadIdx.x + 256 * u;
+			if (e < NE) {
+				const int r = e / (PE_F * 2), c = e - r * PE_F * 2;
+				sv[r][c] = v[u];
+				sw[r][c] = w[u];
+			}
 		}
 	}
 	__syncthreads();
-	const double* X = p.xa + p.mt.xoff[im];
 	const int voff = p.mt.voff[im];
 	const double em = (p.msign < 0) ? -(double) m : (double) m;   // signed m (negative orders of the _ml transforms)
 	for (int e = threadIdx.x; e < PE_J * PE_F; e += blockDim.x) {
@@ -266,7 +310,7 @@ __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 		if (scalar_group) {
 			double2 q = make_double2(0.0, 0.0);
 			if (!zero) {
-				q = ish_inv_s(sv, X, kb, fl, j);
+				q = ish_inv_s(sv, xs, kb, fl, j);
 				if (m == 0) q.y = 0.0;
 			}
 			p.Qo[o] = q;
@@ -274,8 +318,8 @@ __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 		}
 		double2 s = make_double2(0.0, 0.0), t = make_double2(0.0, 0.0);
 		if (!zero) {
-			const double2 vm = ish_inv_s(sv, X, kb, fl, j - 1), v0 = ish_inv_s(sv, X, kb, fl, j), vp = ish_inv_s(sv, X, kb, fl, j + 1);
-			const double2 wm = ish_inv_s(sw, X, kb, fl, j - 1), w0 = ish_inv_s(sw, X, kb, fl, j), wp = ish_inv_s(sw, X, kb, fl, j + 1);
+			const double2 vm = ish_inv_s(sv, xs, kb, fl, j - 1), v0 = ish_inv_s(sv, xs, kb, fl, j), vp = ish_inv_s(sv, xs, kb, fl, j + 1);
+			const double2 wm = ish_inv_s(sw, xs, kb, fl, j - 1), w0 = ish_inv_s(sw, xs, kb, fl, j), wp = ish_inv_s(sw, xs, kb, fl, j + 1);
 			const double lo = (j > 0) ? p.van_lo[voff + j] : 0.0;
 			const double hi = p.van_hi[voff + j];
 			const double l2 = p.l2[l];
