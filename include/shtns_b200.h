@@ -73,7 +73,10 @@ void cu_spat_to_SH_adjoint(shtns_cfg, cplx *Qg, double *Vg, int ltr);
 /* Tuning options of a plan.  option 1: latitude pairs per FFT CTA (1, 2, 4,
  * 8 where the fused chain's buffer fits; 0 = automatic); option 2: recurrence checkpoint spacing (8, 16, 32; rebuilds
  * the checkpoint table; not for clones or plans that have clones); option 3:
- * 1 = always use the generic mixed-radix FFT kernels.  Return 0 or -1.
+ * FFT kernels, 0 = automatic (for nphi = 3 * 2^k up to 6144: persistent CTAs
+ * that prefetch their next latitude tile with tensor copies while the current
+ * one is transformed), 1 = always the generic mixed-radix kernels, 2 = the
+ * fused kernels without prefetch.  Return 0 or -1.
  * No counterpart in SHTns 3.5.2. */
 int shtns_b200_set_option(shtns_cfg, int option, int value);
 int shtns_b200_get_option(shtns_cfg, int option);
@@ -89,8 +92,9 @@ int shtns_b200_get_option(shtns_cfg, int option);
  * the FP16 tensor cores with 3, 4 or 5 balanced 8-bit slices per operand
  * (about 24, 32, 40 bits; products summed exactly in FP32 over windows of 256
  * steps and in FP64 across them); 0 (default) keeps the FP64 contraction.
- * Waits for the plan's stream; returns 1 (and clears it) if a bounded wait of
- * the split-precision kernel gave up since the last call, else 0.
+ * Waits for the device; returns 1 (and clears it) if a bounded wait of the
+ * split-precision kernel or of the prefetching FFT kernels gave up since the
+ * last call, else 0.
  * No counterpart in SHTns 3.5.2. */
 int shtns_b200_kernel_errors(shtns_cfg);
 

@@ -121,7 +121,7 @@ FftParams fft_params(shtns_cfg s, const Job& j, int nrows = 0)
 	if (const char* e = getenv("SHTNS_B200_FFT_PAIRS")) want = atoi(e);
 	if (want == 1 || want == 2 || want == 4 || want == 8) {
 		// fused chains keep one buffer, the generic kernels two
-		const bool fused = fft_fused_available(s->nphi) && !s->fft_generic;
+		const bool fused = fft_fused_available(s->nphi) && s->fft_generic != 1;
 		S = want;
 		while (S > 1 && fft_smem_bytes(s->nphi, S) / (fused ? 2 : 1) > 227 * 1024) S /= 2;
 		if (!fused && S > 4) S = 4;
@@ -132,7 +132,8 @@ FftParams fft_params(shtns_cfg s, const Job& j, int nrows = 0)
 	p.fstride = (long)(s->mmax + 1) * s->nlat;
 	p.nf = j.nf; p.spat_dist = s->spat_dist;
 	p.phi_contiguous = s->phi_contiguous;
-	p.generic = s->fft_generic && fft_smem_bytes(s->nphi, 1) <= 227 * 1024;   // generic kernels need two buffers
+	// generic kernels need two buffers
+	p.generic = (s->fft_generic == 1) ? (fft_smem_bytes(s->nphi, 1) <= 227 * 1024 ? 1 : 0) : s->fft_generic;
 	return p;
 }
 

@@ -16,6 +16,11 @@
 // phi-contiguous (v[theta*nphi + j]).
 #include "sht_internal.h"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <algorithm>
+#include <cstdint>
+
 namespace {
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b)
@@ -380,7 +385,7 @@ __device__ __forceinline__ void twiddle(double2* u, const double2* __restrict__ 
 
 // One middle pass (in place in X).  P = product of earlier radices.
 template <int N, int S, int R, int P>
-__device__ __forceinline__ void mid_pass(double2* X, const double2* __restrict__ tw, int sign)
+__device__ __forceinline__ void mid_pass(double2* X, const double2* __restrict__ tw, int sign, int tid)
 {
 	using G = Geo<N, S>;
 	constexpr int NBF = N / R, TOT = S * NBF, NB = (TOT + G::T - 1) / G::T, TSTEP = N / (P * R);
@@ -388,7 +393,7 @@ __device__ __forceinline__ void mid_pass(double2* X, const double2* __restrict__
 	int dst[NB], ss[NB];
 	#pragma unroll
 	for (int i = 0; i < NB; i++) {
-		const int g = threadIdx.x + i * G::T;
+		const int g = tid + i * G::T;
 		dst[i] = -1;
 		if (g < TOT) {
 			const int s = g % S, b = g / S, k = b % P;
@@ -415,7 +420,7 @@ __device__ __forceinline__ void mid_pass(double2* X, const double2* __restrict__
 template <int N, int S, int P, bool TO_GLOBAL, int R, int... Rest>
 struct Chain {
 	template <class Store>
-	static __device__ __forceinline__ void run(double2* X, const double2* tw, int sign, Store& st)
+	static __device__ __forceinline__ void run(double2* X, const double2* tw, int sign, Store& st, int tid)
 	{
 		if constexpr (sizeof...(Rest) == 0) {
 			if constexpr (TO_GLOBAL) {
@@ -424,7 +429,7 @@ struct Chain {
 				constexpr int NBF = N / R, TOT = S * NBF, NB = (TOT + G::T - 1) / G::T, TSTEP = N / (P * R);
 				#pragma unroll
 				for (int i = 0; i < NB; i++) {
-					const int g = threadIdx.x + i * G::T;
+					const int g = tid + i * G::T;
 					if (g < TOT) {
 						const int s = g % S, b = g / S;
 						double2 u[R];
@@ -437,17 +442,22 @@ struct Chain {
 					}
 				}
 			} else {
-				mid_pass<N, S, R, P>(X, tw, sign);
+				mid_pass<N, S, R, P>(X, tw, sign, tid);
 			}
 		} else {
-			mid_pass<N, S, R, P>(X, tw, sign);
-			Chain<N, S, P * R, TO_GLOBAL, Rest...>::run(X, tw, sign, st);
+			mid_pass<N, S, R, P>(X, tw, sign, tid);
+			Chain<N, S, P * R, TO_GLOBAL, Rest...>::run(X, tw, sign, st, tid);
 		}
 	}
 };
 
-template <int N, int S, bool TO_GLOBAL, class Load, class Store, int R0, int... Rest>
-__device__ __forceinline__ void fused_fft(double2* X, const double2* tw, int sign, Load& ld, Store& st, RadixList<R0, Rest...>)
+struct NoHook { __device__ __forceinline__ void operator()() const {} };
+
+// after_first() runs once the first pass has written X and the block has
+// synchronised (the input is no longer read)
+template <int N, int S, bool TO_GLOBAL, class Load, class Store, class Hook, int R0, int... Rest>
+__device__ __forceinline__ void fused_fft(double2* X, const double2* tw, int sign, Load& ld, Store& st, const Hook& after_first,
+                                          int tid, RadixList<R0, Rest...>)
 {
 	// first pass: butterfly b reads elements b + q*N/R0 from global, no twiddles
 	using G = Geo<N, S>;
@@ -455,7 +465,7 @@ __device__ __forceinline__ void fused_fft(double2* X, const double2* tw, int sig
 	double2 u[NB][R0];
 	#pragma unroll
 	for (int i = 0; i < NB; i++) {
-		const int g = threadIdx.x + i * G::T;
+		const int g = tid + i * G::T;
 		if (g < TOT) {
 			const int s = g % S, b = g / S;
 			#pragma unroll
@@ -464,7 +474,7 @@ __device__ __forceinline__ void fused_fft(double2* X, const double2* tw, int sig
 	}
 	#pragma unroll
 	for (int i = 0; i < NB; i++) {
-		const int g = threadIdx.x + i * G::T;
+		const int g = tid + i * G::T;
 		if (g < TOT) {
 			const int s = g % S, b = g / S;
 			Dft<R0>::run(u[i], sign);
@@ -473,7 +483,8 @@ __device__ __forceinline__ void fused_fft(double2* X, const double2* tw, int sig
 		}
 	}
 	__syncthreads();
-	Chain<N, S, R0, TO_GLOBAL, Rest...>::run(X, tw, sign, st);
+	after_first();
+	Chain<N, S, R0, TO_GLOBAL, Rest...>::run(X, tw, sign, st, tid);
 }
 
 template <int N, int S>
@@ -507,7 +518,7 @@ __global__ void __launch_bounds__(Geo<N, S>::T) fft3_synth_kernel(FftParams p)
 			out[(long)(row + 1) * N + j] = z.y;
 		}
 	};
-	fused_fft<N, S, true>(smem, p.tw, +1, ld, st, typename NphiPlan<N>::L{});
+	fused_fft<N, S, true>(smem, p.tw, +1, ld, st, NoHook{}, threadIdx.x, typename NphiPlan<N>::L{});
 }
 
 template <int N, int S>
@@ -532,7 +543,7 @@ __global__ void __launch_bounds__(Geo<N, S>::T) fft3_analys_kernel(FftParams p)
 	};
 	int dummy = 0;
 	auto st = [&](int, int, double2) { dummy++; };
-	fused_fft<N, S, false>(smem, p.tw, -1, ld, st, typename NphiPlan<N>::L{});
+	fused_fft<N, S, false>(smem, p.tw, -1, ld, st, NoHook{}, threadIdx.x, typename NphiPlan<N>::L{});
 	double2* Ff = p.F + (long)fc * p.fstride;
 	const double sc = 0.5 / N;
 	for (int e = threadIdx.x; e < (p.mlim + 1) * S; e += G::T) {
@@ -545,6 +556,311 @@ __global__ void __launch_bounds__(Geo<N, S>::T) fft3_analys_kernel(FftParams p)
 			Ff[(long)k * nlat + ra + 1] = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
 		}
 	}
+}
+
+// ---------------------------------------------------------------------------
+// Prefetched fused kernels.  A persistent CTA walks over tiles (2 S latitudes
+// of one field-component, tile t = fc * nlg + latitude group) and keeps the
+// input of its next tile in flight while the current one is transformed: one
+// thread issues tensor copies (TMA, no multicast) of the next tile into a
+// shared staging buffer right after the first pass has moved the current
+// tile from there into the FFT buffer, and the copies complete on an
+// mbarrier that the CTA waits on (bounded) before the next first pass.
+//   synthesis input   F[fc][k][theta]: box (2 S latitudes x 2 doubles, <= 256 k)
+//   analysis input    theta-contiguous v[f][j][theta]: box (2 S latitudes, 256 or 192 j)
+// Outputs are written as by the direct kernels above.
+// j rows per box of the analysis input: 256, or nphi for 192, 192 for 384
+__host__ __device__ constexpr int box_j(int N) { return (N % 256 == 0) ? 256 : (N <= 256 ? N : 192); }
+
+struct TmaTiles {
+	int nlg;          // latitude groups (tiles per field-component)
+	int ntiles;
+	int ncopy;        // box copies per tile
+	int box;          // rows (k or j) per box
+	unsigned bytes;   // bytes per tile (all boxes, out-of-range parts included)
+	int stage_off;    // staging buffer offset in the dynamic shared memory (bytes)
+};
+
+constexpr uint64_t FT_WAIT_NS = 1000000000ull;   // time limit of every mbarrier wait
+
+__device__ int g_fft_wait_err;                    // set when a bounded wait gave up
+
+__device__ __forceinline__ uint32_t su32(const void* ptr) { return static_cast<uint32_t>(__cvta_generic_to_shared(ptr)); }
+
+__device__ __forceinline__ uint64_t gtimer()
+{
+	uint64_t t;
+	asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+	return t;
+}
+
+__device__ __forceinline__ bool fbar_wait(uint64_t* bar, uint32_t parity)
+{
+	const uint32_t a = su32(bar);
+	const uint64_t t0 = gtimer();
+	for (int it = 0;; it++) {
+		if ((it & 1023) == 1023 && gtimer() - t0 > FT_WAIT_NS) return false;
+		uint32_t done;
+		asm volatile("{\n\t.reg .pred p;\n\t"
+		             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+		             "selp.u32 %0, 1, 0, p;\n\t}"
+		             : "=r"(done) : "r"(a), "r"(parity) : "memory");
+		if (done) return true;
+	}
+}
+
+__device__ __forceinline__ void tma_tile3(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar)
+{
+	asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+	             :: "r"(su32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(su32(bar))
+	             : "memory");
+}
+
+// One thread: announce the bytes of a tile, then issue its box copies
+// (latitude coordinate c0, rows c * box, field c2).
+__device__ __forceinline__ void fetch_tile(uint64_t* bar, const CUtensorMap* map, char* stage, const TmaTiles& tt,
+                                           int c0, int c2, int box_bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(su32(bar)), "r"(tt.bytes) : "memory");
+	for (int c = 0; c < tt.ncopy; c++)
+		tma_tile3(stage + (size_t) c * box_bytes, map, c0, c * tt.box, c2, bar);
+}
+
+// Wait for the staged tile; false (uniformly in the CTA) if the wait gave up,
+// after recording it and waiting once more (bounded) for the copies in flight.
+__device__ __forceinline__ bool stage_ready(uint64_t* bar, uint32_t parity)
+{
+	const bool ok = fbar_wait(bar, parity);
+	if (__syncthreads_or(!ok)) {
+		if (threadIdx.x == 0) {
+			atomicExch(&g_fft_wait_err, 1);
+			fbar_wait(bar, parity);
+		}
+		return false;
+	}
+	return true;
+}
+
+__device__ __forceinline__ void stage_init(uint64_t* bar)
+{
+	if (threadIdx.x == 0) {
+		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(su32(bar)) : "memory");
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	__syncthreads();
+}
+
+template <int N, int S>
+__global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_synth_kernel(const __grid_constant__ CUtensorMap fmap, FftParams p,
+                                                                   TmaTiles tt)
+{
+	extern __shared__ __align__(128) char fsm[];
+	__shared__ __align__(8) uint64_t bar;
+	char* base = fsm + ((128u - (su32(fsm) & 127u)) & 127u);   // tensor copies land on 128-byte boundaries
+	double2* X = reinterpret_cast<double2*>(base);
+	char* stage = base + tt.stage_off;
+	const double2* stg = reinterpret_cast<const double2*>(stage);
+	const int ml = p.mlim, nlat = p.nlat;
+	const int box_bytes = tt.box * 2 * S * 16;
+	stage_init(&bar);
+	int tile = blockIdx.x;
+	if (threadIdx.x == 0) {
+		const int fc = tile / tt.nlg;
+		fetch_tile(&bar, &fmap, stage, tt, 4 * S * (tile - fc * tt.nlg), fc, box_bytes);
+	}
+	for (uint32_t parity = 0; tile < tt.ntiles; tile += gridDim.x, parity ^= 1) {
+		if (!stage_ready(&bar, parity)) return;
+		const int fc = tile / tt.nlg;
+		const int lat0 = (tile - fc * tt.nlg) * 2 * S;
+		// ml opaque per tile: the first pass's shared addresses and predicates
+		// are recomputed per tile instead of held in registers across tiles
+		int mlo = ml;
+		asm volatile("" : "+r"(mlo));
+		auto ld = [&](int s, int j) -> double2 {
+			const int k = (j <= mlo) ? j : ((j >= N - mlo) ? N - j : -1);
+			if (k < 0) return make_double2(0.0, 0.0);
+			// the two latitudes of sequence s, read in an order that alternates
+			// with the row so that the 8 lanes of a shared-memory phase (4 rows)
+			// hit distinct banks; swapped back in registers
+			const int f = (k >> (S == 1 ? 2 : (S == 2 ? 1 : 0))) & 1;
+			const double2 u0 = stg[k * 2 * S + 2 * s + f], u1 = stg[k * 2 * S + 2 * s + 1 - f];
+			double2 a = f ? u1 : u0, b = f ? u0 : u1;
+			if (k == 0) { a.y = 0.0; b.y = 0.0; }
+			return (j <= mlo) ? make_double2(a.x - b.y, a.y + b.x) : make_double2(a.x + b.y, b.x - a.y);
+		};
+		const int c = fc / p.nf;
+		double* out = (c == 0 ? p.spat[0] : c == 1 ? p.spat[1] : p.spat[2]) + (long)(fc - c * p.nf) * p.spat_dist;
+		const bool phi = p.phi_contiguous, v2 = p.vec2;
+		auto st = [&](int s, int j, double2 z) {
+			const int row = lat0 + 2 * s;
+			if (row >= nlat) return;
+			if (!phi) {
+				double* o = out + (long)j * nlat + row;
+				if (v2) *reinterpret_cast<double2*>(o) = z;
+				else { o[0] = z.x; o[1] = z.y; }
+			} else {
+				out[(long)row * N + j] = z.x;
+				out[(long)(row + 1) * N + j] = z.y;
+			}
+		};
+		const int next = tile + gridDim.x;
+		auto prefetch = [&]() {
+			if (threadIdx.x == 0 && next < tt.ntiles) {
+				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+				const int nfc = next / tt.nlg;
+				fetch_tile(&bar, &fmap, stage, tt, 4 * S * (next - nfc * tt.nlg), nfc, box_bytes);
+			}
+		};
+		// thread index and twiddle pointer opaque per tile: the per-thread
+		// addresses of the passes are recomputed instead of held across tiles
+		fused_fft<N, S, true>(X, p.tw, +1, ld, st, prefetch, threadIdx.x, typename NphiPlan<N>::L{});
+	}
+}
+
+template <int N, int S>
+__global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_analys_kernel(const __grid_constant__ CUtensorMap m0,
+                                                                    const __grid_constant__ CUtensorMap m1,
+                                                                    const __grid_constant__ CUtensorMap m2, FftParams p,
+                                                                    TmaTiles tt)
+{
+	using G = Geo<N, S>;
+	extern __shared__ __align__(128) char fsm[];
+	__shared__ __align__(8) uint64_t bar;
+	char* base = fsm + ((128u - (su32(fsm) & 127u)) & 127u);   // tensor copies land on 128-byte boundaries
+	double2* X = reinterpret_cast<double2*>(base);
+	char* stage = base + tt.stage_off;
+	const double* stg = reinterpret_cast<const double*>(stage);
+	const int nlat = p.nlat, nf = p.nf;
+	const int box_bytes = box_j(N) * 2 * S * 8;
+	auto issue = [&](int t) {
+		const int fc = t / tt.nlg, c = fc / nf;
+		const CUtensorMap* m = (c == 0) ? &m0 : (c == 1 ? &m1 : &m2);
+		fetch_tile(&bar, m, stage, tt, 2 * S * (t - fc * tt.nlg), fc - c * nf, box_bytes);
+	};
+	stage_init(&bar);
+	int tile = blockIdx.x;
+	if (threadIdx.x == 0) issue(tile);
+	for (uint32_t parity = 0; tile < tt.ntiles; tile += gridDim.x, parity ^= 1) {
+		if (!stage_ready(&bar, parity)) return;
+		const int fc = tile / tt.nlg;
+		const int lat0 = (tile - fc * tt.nlg) * 2 * S;
+		int rs = 2 * S;                         // opaque per tile, as mlim in the synthesis
+		asm volatile("" : "+r"(rs));
+		auto ld = [&](int s, int j) -> double2 { return *reinterpret_cast<const double2*>(stg + j * rs + 2 * s); };
+		int dummy = 0;
+		auto st = [&](int, int, double2) { dummy++; };
+		const int next = tile + gridDim.x;
+		auto prefetch = [&]() {
+			if (threadIdx.x == 0 && next < tt.ntiles) {
+				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+				issue(next);
+			}
+		};
+		fused_fft<N, S, false>(X, p.tw, -1, ld, st, prefetch, threadIdx.x, typename NphiPlan<N>::L{});
+		double2* Ff = p.F + (long)fc * p.fstride;
+		const double sc = 0.5 / N;
+		int ne = (p.mlim + 1) * S;
+		asm volatile("" : "+r"(ne));             // opaque per tile, as the first pass's values
+		for (int e = threadIdx.x; e < ne; e += G::T) {
+			const int k = e / S, s = e - k * S;
+			const int ra = lat0 + 2 * s;
+			const double2 z = X[G::at(s, k)];
+			const double2 w = X[G::at(s, k ? N - k : 0)];
+			if (ra < nlat) {
+				Ff[(long)k * nlat + ra] = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
+				Ff[(long)k * nlat + ra + 1] = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
+			}
+		}
+	}
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	static bool tried = false;
+	if (!tried) {
+		tried = true;
+		void* f = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+		    q == cudaDriverEntryPointSuccess)
+			fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+		else
+			cudaGetLastError();
+	}
+	return fn;
+}
+
+// 3-d FP64 tensor map, dims / byte strides of dims 1 and 2 / box, no swizzle,
+// zero fill out of range
+bool encode3(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint64_t s1, uint64_t s2,
+             uint32_t b0, uint32_t b1)
+{
+	PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+	if (!enc || ((uintptr_t) base & 15) || (s1 & 15) || (s2 & 15) || ((b0 * 8) & 15)) return false;
+	const cuuint64_t dims[3] = {d0, d1, d2};
+	const cuuint64_t strides[2] = {s1, s2};
+	const cuuint32_t box[3] = {b0, b1, 1};
+	const cuuint32_t es[3] = {1, 1, 1};
+	return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(base), dims, strides, box, es,
+	           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+	           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int sm_count()
+{
+	static int n = 0;
+	if (!n) {
+		int dev = 0;
+		cudaGetDevice(&dev);
+		if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) { cudaGetLastError(); n = 148; }
+	}
+	return n;
+}
+
+template <int N, int S>
+bool launch_fft4(const FftParams& p, int nfc, cudaStream_t st, bool synth)
+{
+	using G = Geo<N, S>;
+	alignas(64) CUtensorMap maps[3];
+	TmaTiles tt;
+	tt.nlg = (p.nlat + 2 * S - 1) / (2 * S);
+	tt.ntiles = tt.nlg * nfc;
+	size_t stage_bytes;
+	if (synth) {
+		const int rows = p.mlim + 1;
+		tt.box = rows < 256 ? rows : 256;
+		tt.ncopy = (rows + tt.box - 1) / tt.box;
+		stage_bytes = (size_t) tt.ncopy * tt.box * 2 * S * 16;
+		if (!encode3(&maps[0], p.F, 2 * (uint64_t) p.nlat, rows, nfc, 16 * (uint64_t) p.nlat, 16 * (uint64_t) p.fstride, 4 * S, tt.box))
+			return false;
+	} else {
+		// theta-contiguous grids only (phi-contiguous rows are read faster
+		// straight from global memory by the direct kernel)
+		if (!p.vec2 || p.phi_contiguous || (p.nlat & 1)) return false;
+		tt.box = box_j(N);
+		if (N % tt.box) return false;
+		tt.ncopy = N / tt.box;
+		stage_bytes = (size_t) N * 2 * S * 8;
+		const int ncomp = (nfc + p.nf - 1) / p.nf;
+		for (int c = 0; c < 3; c++) {
+			const double* base = p.spat_in[c < ncomp ? c : 0];
+			if (!encode3(&maps[c], base, p.nlat, N, p.nf, 8 * (uint64_t) p.nlat, 8 * (uint64_t) p.spat_dist, 2 * S, tt.box))
+				return false;
+		}
+	}
+	tt.bytes = (unsigned) stage_bytes;
+	tt.stage_off = (int)(((size_t) S * G::SEQ * sizeof(double2) + 127) / 128 * 128);
+	const size_t smem = tt.stage_off + stage_bytes + 128;
+	if (smem > 226 * 1024) return false;
+	int per_sm = 0;
+	cudaError_t e = synth ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft4_synth_kernel<N, S>, G::T, smem)
+	                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft4_analys_kernel<N, S>, G::T, smem);
+	if (e != cudaSuccess || per_sm <= 0) { cudaGetLastError(); return false; }
+	const int grid = std::min(tt.ntiles, per_sm * sm_count());
+	if (synth) fft4_synth_kernel<N, S><<<grid, G::T, smem, st>>>(maps[0], p, tt);
+	else fft4_analys_kernel<N, S><<<grid, G::T, smem, st>>>(maps[0], maps[1], maps[2], p, tt);
+	return true;
 }
 
 template <int N, int S>
@@ -570,8 +886,42 @@ bool launch_fft3_n(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 	return launch_fft3<N, 1>(p, nfc, st, synth);
 }
 
+} // namespace
+
+static int g_last_fft_path = -1;
+static bool g_fft4_ran = false;
+
+namespace {
+
+// prefetched kernels for the automatic choice (p.generic == 0); false where
+// they do not apply (layout, alignment, shared memory), for the direct ones
+template <int N>
+bool launch_fft4_n(const FftParams& p, int nfc, cudaStream_t st, bool synth)
+{
+	if constexpr (N + (N >> 3) + 8 > 6400) return false;     // FFT buffer above 100 KB
+	else {
+		if (p.S == 1) return launch_fft4<N, 1>(p, nfc, st, synth);
+		if constexpr (2 * N / 8 <= 768) if (p.S == 2) return launch_fft4<N, 2>(p, nfc, st, synth);
+		if constexpr (4 * N / 8 <= 768) if (p.S == 4) return launch_fft4<N, 4>(p, nfc, st, synth);
+		return false;
+	}
+}
+
 bool launch_fused(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 {
+	if (p.generic == 0) {
+		bool done = false;
+		switch (p.N) {
+			case 192: done = launch_fft4_n<192>(p, nfc, st, synth); break;
+			case 384: done = launch_fft4_n<384>(p, nfc, st, synth); break;
+			case 768: done = launch_fft4_n<768>(p, nfc, st, synth); break;
+			case 1536: done = launch_fft4_n<1536>(p, nfc, st, synth); break;
+			case 3072: done = launch_fft4_n<3072>(p, nfc, st, synth); break;
+			case 6144: done = launch_fft4_n<6144>(p, nfc, st, synth); break;
+			default: break;
+		}
+		if (done) { g_fft4_ran = true; return true; }
+	}
 	switch (p.N) {
 		case 192: return launch_fft3_n<192>(p, nfc, st, synth);
 		case 384: return launch_fft3_n<384>(p, nfc, st, synth);
@@ -588,6 +938,20 @@ template <int N>
 void set_fused_limits()
 {
 	const int lim = 227 * 1024;
+	if constexpr (N + (N >> 3) + 8 <= 6400) {
+		// the prefetching kernels also hold an mbarrier in static shared memory
+		const int lim4 = 226 * 1024;
+		cudaFuncSetAttribute(fft4_synth_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim4);
+		cudaFuncSetAttribute(fft4_analys_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim4);
+		if constexpr (2 * N / 8 <= 768) {
+			cudaFuncSetAttribute(fft4_synth_kernel<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim4);
+			cudaFuncSetAttribute(fft4_analys_kernel<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim4);
+		}
+		if constexpr (4 * N / 8 <= 768) {
+			cudaFuncSetAttribute(fft4_synth_kernel<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim4);
+			cudaFuncSetAttribute(fft4_analys_kernel<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim4);
+		}
+	}
 	cudaFuncSetAttribute(fft3_synth_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 	cudaFuncSetAttribute(fft3_analys_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 	if constexpr (2 * N / 8 <= 768) {
@@ -632,9 +996,15 @@ bool fft_fused_available(int N)
 	}
 }
 
+// kernel family of the last FFT launch (host side): 0 generic, 1 fused
+// direct loads, 2 fused with prefetched tiles
+int fft_last_path() { return g_last_fft_path; }
+
 void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st)
 {
-	if (!p.generic && launch_fused(p, nfc, st, true)) { shtb_count_launch(); return; }
+	g_fft4_ran = false;
+	if (p.generic != 1 && launch_fused(p, nfc, st, true)) { g_last_fft_path = g_fft4_ran ? 2 : 1; shtb_count_launch(); return; }
+	g_last_fft_path = 0;
 	const int T = fft_threads(p.N, p.S, p.rcode, p.nradix);
 	const size_t smem = fft_smem_bytes(p.N, p.S);
 	dim3 grid((p.nlat + 2 * p.S - 1) / (2 * p.S), nfc);
@@ -648,7 +1018,9 @@ void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st)
 
 void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st)
 {
-	if (!p.generic && launch_fused(p, nfc, st, false)) { shtb_count_launch(); return; }
+	g_fft4_ran = false;
+	if (p.generic != 1 && launch_fused(p, nfc, st, false)) { g_last_fft_path = g_fft4_ran ? 2 : 1; shtb_count_launch(); return; }
+	g_last_fft_path = 0;
 	const int T = fft_threads(p.N, p.S, p.rcode, p.nradix);
 	const size_t smem = fft_smem_bytes(p.N, p.S);
 	dim3 grid((p.nlat + 2 * p.S - 1) / (2 * p.S), nfc);
@@ -662,6 +1034,8 @@ void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st)
 
 void fft_set_smem_limits()
 {
+	tensor_map_encoder();    // resolved here, outside any stream capture
+	sm_count();
 	set_fused_limits<192>(); set_fused_limits<384>(); set_fused_limits<768>();
 	set_fused_limits<1536>(); set_fused_limits<3072>(); set_fused_limits<6144>(); set_fused_limits<12288>();
 	const int lim = 227 * 1024;
@@ -671,4 +1045,18 @@ void fft_set_smem_limits()
 	cudaFuncSetAttribute(fft_analys_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 	cudaFuncSetAttribute(fft_analys_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 	cudaFuncSetAttribute(fft_analys_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+}
+
+// Returns (and clears) the flag that a bounded wait of the prefetched FFT
+// kernels gave up; waits for the device.
+int fft_take_wait_error()
+{
+	int e = 0;
+	cudaDeviceSynchronize();
+	if (cudaMemcpyFromSymbol(&e, g_fft_wait_err, sizeof(int)) != cudaSuccess) { cudaGetLastError(); return 0; }
+	if (e) {
+		const int z = 0;
+		cudaMemcpyToSymbol(g_fft_wait_err, &z, sizeof(int));
+	}
+	return e;
 }

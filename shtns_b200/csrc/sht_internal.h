@@ -77,7 +77,7 @@ struct shtns_info {
 	long ktot, ctot, xtot, vtot, segtot;
 	int ckseg;                           // checkpoint spacing in k
 	int fft_pairs;                       // latitude pairs per FFT CTA (0: automatic)
-	int fft_generic;                     // 1: always use the generic mixed-radix FFT kernels
+	int fft_generic;                     // FFT kernels: 0 automatic, 1 generic mixed-radix, 2 fused without prefetch
 	int tile_wm;                         // Legendre tile shape option (0 automatic)
 	std::vector<int> fft_radix;          // factorisation of nphi
 	double Y00_1, Y10_ct, Y11_st;
@@ -195,7 +195,7 @@ struct FftParams {
 	long spat_dist;
 	int phi_contiguous;
 	int vec2;                            // spatial pointers 16-byte aligned: latitude pairs moved as double2
-	int generic;                         // 1: force the generic mixed-radix kernels
+	int generic;                         // 0 automatic, 1 generic mixed-radix kernels, 2 fused kernels without prefetch
 };
 
 // ---- launchers (sht_legendre.cu / sht_fft.cu) ----
@@ -216,6 +216,8 @@ bool fft_fused_available(int N);
 size_t fft_smem_bytes(int N, int S);
 void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st);
 void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st);
+int fft_take_wait_error();
+int fft_last_path();
 
 // ---- error reporting (sht_plan.cu) ----
 void shtb_set_error(int code, const std::string& msg);

@@ -847,8 +847,9 @@ extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
 			launch_checkpoints(s, 0);
 			return shtb_cuda_ok(cudaDeviceSynchronize(), "checkpoint rebuild") ? 0 : -1;
 		}
-		case 3:   // force the generic FFT kernels
-			s->fft_generic = value ? 1 : 0;
+		case 3:   // FFT kernels: 0 automatic, 1 generic mixed-radix, 2 fused without prefetch
+			if (value < 0 || value > 2) return -1;
+			s->fft_generic = value;
 			return 0;
 		default:
 			return -1;
@@ -864,6 +865,7 @@ extern "C" int shtns_b200_get_option(shtns_cfg s, int option)
 		case 3: return s->fft_generic;
 		case 4: return s->split_ns;
 		case 5: return s->tile_wm;
+		case 6: return fft_last_path();   // FFT kernels of the last launch in this process
 		default: return -1;
 	}
 }

@@ -686,14 +686,17 @@ void free_split(shtns_cfg s)
 	s->d_bsl = nullptr; s->bsl_cap = 0; s->d_bexp = nullptr; s->bexp_cap = 0; s->d_split_err = nullptr;
 }
 
-// Waits for the plan's stream and returns (and clears) the flag that the
-// split-precision kernel sets when one of its bounded waits gave up.
+// Waits for the device and returns (and clears) the flags that the
+// split-precision kernel and the prefetched FFT kernels set when one of their
+// bounded waits gave up.
 extern "C" int shtns_b200_kernel_errors(shtns_cfg s)
 {
-	if (!s || !s->d_split_err) return 0;
+	if (!s) return 0;
+	int e = fft_take_wait_error();
+	if (!s->d_split_err) return e;
 	cudaStreamSynchronize(s->comp_stream);
-	int e = 0;
-	cudaMemcpy(&e, s->d_split_err, sizeof(int), cudaMemcpyDeviceToHost);
-	if (e) cudaMemset(s->d_split_err, 0, sizeof(int));
-	return e;
+	int f = 0;
+	cudaMemcpy(&f, s->d_split_err, sizeof(int), cudaMemcpyDeviceToHost);
+	if (f) cudaMemset(s->d_split_err, 0, sizeof(int));
+	return e | f;
 }

@@ -318,3 +318,48 @@ def test_simt_legendre_matches_tensor_tiles(case):
             assert relerr(a.cpu().numpy(), b.cpu().numpy()) < 1e-13
     for a, b in zip(specs, res[8][1]):
         assert relerr(a.cpu().numpy(), b.cpu().numpy()) < 1e-11
+
+
+@pytest.mark.parametrize("case", ["l511_theta_qst", "l1023_theta", "l255_phi_qst", "l100_ragged", "l63_theta",
+                                  "l511_nlat770_ltr"])
+def test_prefetched_fft_matches_direct(case):
+    """Option 3 (FFT kernels): the automatic choice, persistent CTAs that fetch
+    their next latitude tile with tensor copies (option 6 reports 2), computes
+    the same passes as the direct-load fused kernels (option 3 = 2): results
+    agree bit for bit, and with the generic mixed-radix kernels to rounding."""
+    import shtns_b200
+    from shtns_b200 import capi
+    lib = capi.load()
+    dev = torch.device("cuda:0")
+    L, nlat, nphi, nf, ncomp, phi, ltr = {
+        "l511_theta_qst": (511, 768, 1536, 8, 3, False, None),
+        "l1023_theta": (1023, 1536, 3072, 2, 1, False, None),
+        "l255_phi_qst": (255, 384, 768, 4, 3, True, None),
+        "l100_ragged": (100, 150, 384, 3, 1, False, None),
+        "l63_theta": (63, 96, 192, 16, 1, False, None),
+        "l511_nlat770_ltr": (511, 770, 1536, 2, 3, False, 300),
+    }[case]
+    sh = shtns_b200.sht(L)
+    layout = shtns_b200.SHT_PHI_CONTIGUOUS if phi else shtns_b200.SHT_THETA_CONTIGUOUS
+    sh.set_grid(nlat, nphi, flags=shtns_b200.sht_quick_init | layout, polar_opt=1e-10)
+    specs = [torch.from_numpy(rand_spec(L, L, 1, 60 + i, nfields=nf, zero_l0=(ncomp > 1 and i > 0))).to(dev)
+             for i in range(ncomp)]
+    kw = {} if ltr is None else {"ltr": ltr}
+    res = {}
+    for opt in (0, 2, 1):
+        assert lib.shtns_b200_set_option(sh._cfg, 3, opt) == 0
+        spat = [torch.empty((nf,) + sh.spat_shape, dtype=torch.float64, device=dev) for _ in range(ncomp)]
+        sh.synth_into(specs, spat, **kw)
+        path_s = lib.shtns_b200_get_option(sh._cfg, 6)
+        back = [torch.empty_like(x) for x in specs]
+        sh.analys_into(spat, back, **kw)
+        path_a = lib.shtns_b200_get_option(sh._cfg, 6)
+        torch.cuda.synchronize()
+        res[opt] = (spat, back, path_s, path_a)
+    assert lib.shtns_b200_kernel_errors(sh._cfg) == 0
+    assert res[0][2:] == (2, 2) and res[2][2:] == (1, 1) and res[1][2:] == (0, 0)
+    for a, b in zip(res[0][0] + res[0][1], res[2][0] + res[2][1]):
+        assert torch.equal(a, b)
+    for a, b in zip(res[0][0] + res[0][1], res[1][0] + res[1][1]):
+        assert float((a - b).abs().max()) <= 1e-13 * float(b.abs().max())
+    assert lib.shtns_b200_set_option(sh._cfg, 3, 3) == -1
