@@ -73,10 +73,14 @@ void cu_spat_to_SH_adjoint(shtns_cfg, cplx *Qg, double *Vg, int ltr);
 /* Tuning options of a plan.  option 1: latitude pairs per FFT CTA (1, 2, 4,
  * 8 where the fused chain's buffer fits; 0 = automatic); option 2: recurrence checkpoint spacing (8, 16, 32; rebuilds
  * the checkpoint table; not for clones or plans that have clones); option 3:
- * FFT kernels, 0 = automatic (for nphi = 3 * 2^k up to 6144: persistent CTAs
+ * FFT kernels, 0 = automatic (for nphi = 3 * 2^k up to 3072: persistent CTAs
  * that prefetch their next latitude tile with tensor copies while the current
- * one is transformed), 1 = always the generic mixed-radix kernels, 2 = the
- * fused kernels without prefetch.  Return 0 or -1.
+ * one is transformed, and on theta-contiguous grids write whole synthesis
+ * tiles with tensor stores; phi-contiguous analysis keeps the direct
+ * kernels), 1 = always the generic mixed-radix kernels, 2 = the fused
+ * kernels without prefetch, 3 = prefetched loads with per-thread stores.
+ * Option 6 (get only): FFT kernels of the last launch in this process, 0
+ * generic, 1 fused direct, 2 prefetched.  Return 0 or -1.
  * No counterpart in SHTns 3.5.2. */
 int shtns_b200_set_option(shtns_cfg, int option, int value);
 int shtns_b200_get_option(shtns_cfg, int option);

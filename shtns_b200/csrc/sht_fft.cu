@@ -384,7 +384,9 @@ __device__ __forceinline__ void twiddle(double2* u, const double2* __restrict__ 
 }
 
 // One middle pass (in place in X).  P = product of earlier radices.
-template <int N, int S, int R, int P>
+// DENSE: the outputs go to X[j * S + s] (rows of S complex values, for a
+// tensor store) instead of the padded sequence layout
+template <int N, int S, int R, int P, bool DENSE = false>
 __device__ __forceinline__ void mid_pass(double2* X, const double2* __restrict__ tw, int sign, int tid)
 {
 	using G = Geo<N, S>;
@@ -410,20 +412,21 @@ __device__ __forceinline__ void mid_pass(double2* X, const double2* __restrict__
 	for (int i = 0; i < NB; i++)
 		if (dst[i] >= 0) {
 			#pragma unroll
-			for (int q = 0; q < R; q++) X[G::at(ss[i], dst[i] + q * P)] = u[i][q];
+			for (int q = 0; q < R; q++) X[DENSE ? (dst[i] + q * P) * S + ss[i] : G::at(ss[i], dst[i] + q * P)] = u[i][q];
 		}
 	__syncthreads();
 }
 
 // Pass chain: first pass from a loader, middle passes in shared memory, last
-// pass either to shared memory (analysis) or to a storer (synthesis).
-template <int N, int S, int P, bool TO_GLOBAL, int R, int... Rest>
+// pass to shared memory (MODE 0), to a storer (MODE 1) or to shared memory in
+// rows of S complex values (MODE 2).
+template <int N, int S, int P, int MODE, int R, int... Rest>
 struct Chain {
 	template <class Store>
 	static __device__ __forceinline__ void run(double2* X, const double2* tw, int sign, Store& st, int tid)
 	{
 		if constexpr (sizeof...(Rest) == 0) {
-			if constexpr (TO_GLOBAL) {
+			if constexpr (MODE == 1) {
 				// last pass: k = b (b < P = N/R), outputs b + q*P go to global memory
 				using G = Geo<N, S>;
 				constexpr int NBF = N / R, TOT = S * NBF, NB = (TOT + G::T - 1) / G::T, TSTEP = N / (P * R);
@@ -442,11 +445,11 @@ struct Chain {
 					}
 				}
 			} else {
-				mid_pass<N, S, R, P>(X, tw, sign, tid);
+				mid_pass<N, S, R, P, MODE == 2>(X, tw, sign, tid);
 			}
 		} else {
 			mid_pass<N, S, R, P>(X, tw, sign, tid);
-			Chain<N, S, P * R, TO_GLOBAL, Rest...>::run(X, tw, sign, st, tid);
+			Chain<N, S, P * R, MODE, Rest...>::run(X, tw, sign, st, tid);
 		}
 	}
 };
@@ -455,7 +458,7 @@ struct NoHook { __device__ __forceinline__ void operator()() const {} };
 
 // after_first() runs once the first pass has written X and the block has
 // synchronised (the input is no longer read)
-template <int N, int S, bool TO_GLOBAL, class Load, class Store, class Hook, int R0, int... Rest>
+template <int N, int S, int MODE, class Load, class Store, class Hook, int R0, int... Rest>
 __device__ __forceinline__ void fused_fft(double2* X, const double2* tw, int sign, Load& ld, Store& st, const Hook& after_first,
                                           int tid, RadixList<R0, Rest...>)
 {
@@ -484,7 +487,7 @@ __device__ __forceinline__ void fused_fft(double2* X, const double2* tw, int sig
 	}
 	__syncthreads();
 	after_first();
-	Chain<N, S, R0, TO_GLOBAL, Rest...>::run(X, tw, sign, st, tid);
+	Chain<N, S, R0, MODE, Rest...>::run(X, tw, sign, st, tid);
 }
 
 template <int N, int S>
@@ -650,9 +653,34 @@ __device__ __forceinline__ void stage_init(uint64_t* bar)
 	__syncthreads();
 }
 
-template <int N, int S>
-__global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_synth_kernel(const __grid_constant__ CUtensorMap fmap, FftParams p,
-                                                                   TmaTiles tt)
+__device__ __forceinline__ void tma_store3(const CUtensorMap* map, const void* src, int c0, int c1, int c2)
+{
+	asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];"
+	             :: "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(su32(src)) : "memory");
+}
+
+// tensor stores of this thread have finished reading shared memory
+__device__ __forceinline__ void store_reads_done() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
+// Results written to X by every thread become visible to the tensor copies,
+// then one thread stores nbox boxes of box_bytes each.
+__device__ __forceinline__ void store_tile(const CUtensorMap* map, const char* X, int nbox, int box, int box_bytes, int c0,
+                                           int c2)
+{
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (int c = 0; c < nbox; c++) tma_store3(map, X + (size_t) c * box_bytes, c0, c * box, c2);
+		asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+	}
+}
+
+// TOUT: theta-contiguous output written by tensor stores of whole tiles
+// (rows of 2 S latitudes) from X, instead of 16-byte stores per latitude pair
+template <int N, int S, bool TOUT>
+__global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_synth_kernel(
+	const __grid_constant__ CUtensorMap fmap, const __grid_constant__ CUtensorMap o0, const __grid_constant__ CUtensorMap o1,
+	const __grid_constant__ CUtensorMap o2, FftParams p, TmaTiles tt)
 {
 	extern __shared__ __align__(128) char fsm[];
 	__shared__ __align__(8) uint64_t bar;
@@ -669,6 +697,7 @@ __global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_synth_k
 		fetch_tile(&bar, &fmap, stage, tt, 4 * S * (tile - fc * tt.nlg), fc, box_bytes);
 	}
 	for (uint32_t parity = 0; tile < tt.ntiles; tile += gridDim.x, parity ^= 1) {
+		if (TOUT && threadIdx.x == 0) store_reads_done();     // X is free again (previous tile's stores)
 		if (!stage_ready(&bar, parity)) return;
 		const int fc = tile / tt.nlg;
 		const int lat0 = (tile - fc * tt.nlg) * 2 * S;
@@ -689,20 +718,6 @@ __global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_synth_k
 			return (j <= mlo) ? make_double2(a.x - b.y, a.y + b.x) : make_double2(a.x + b.y, b.x - a.y);
 		};
 		const int c = fc / p.nf;
-		double* out = (c == 0 ? p.spat[0] : c == 1 ? p.spat[1] : p.spat[2]) + (long)(fc - c * p.nf) * p.spat_dist;
-		const bool phi = p.phi_contiguous, v2 = p.vec2;
-		auto st = [&](int s, int j, double2 z) {
-			const int row = lat0 + 2 * s;
-			if (row >= nlat) return;
-			if (!phi) {
-				double* o = out + (long)j * nlat + row;
-				if (v2) *reinterpret_cast<double2*>(o) = z;
-				else { o[0] = z.x; o[1] = z.y; }
-			} else {
-				out[(long)row * N + j] = z.x;
-				out[(long)(row + 1) * N + j] = z.y;
-			}
-		};
 		const int next = tile + gridDim.x;
 		auto prefetch = [&]() {
 			if (threadIdx.x == 0 && next < tt.ntiles) {
@@ -711,17 +726,38 @@ __global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_synth_k
 				fetch_tile(&bar, &fmap, stage, tt, 4 * S * (next - nfc * tt.nlg), nfc, box_bytes);
 			}
 		};
-		// thread index and twiddle pointer opaque per tile: the per-thread
-		// addresses of the passes are recomputed instead of held across tiles
-		fused_fft<N, S, true>(X, p.tw, +1, ld, st, prefetch, threadIdx.x, typename NphiPlan<N>::L{});
+		if constexpr (TOUT) {
+			int dummy = 0;
+			auto st = [&](int, int, double2) { dummy++; };
+			fused_fft<N, S, 2>(X, p.tw, +1, ld, st, prefetch, threadIdx.x, typename NphiPlan<N>::L{});
+			constexpr int BJ = box_j(N);
+			const CUtensorMap* om = (c == 0) ? &o0 : (c == 1 ? &o1 : &o2);
+			store_tile(om, base, N / BJ, BJ, BJ * S * 16, lat0, fc - c * p.nf);
+		} else {
+			double* out = (c == 0 ? p.spat[0] : c == 1 ? p.spat[1] : p.spat[2]) + (long)(fc - c * p.nf) * p.spat_dist;
+			const bool phi = p.phi_contiguous, v2 = p.vec2;
+			auto st = [&](int s, int j, double2 z) {
+				const int row = lat0 + 2 * s;
+				if (row >= nlat) return;
+				if (!phi) {
+					double* o = out + (long)j * nlat + row;
+					if (v2) *reinterpret_cast<double2*>(o) = z;
+					else { o[0] = z.x; o[1] = z.y; }
+				} else {
+					out[(long)row * N + j] = z.x;
+					out[(long)(row + 1) * N + j] = z.y;
+				}
+			};
+			fused_fft<N, S, 1>(X, p.tw, +1, ld, st, prefetch, threadIdx.x, typename NphiPlan<N>::L{});
+		}
 	}
+	if (TOUT && threadIdx.x == 0) store_reads_done();
 }
 
 template <int N, int S>
-__global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_analys_kernel(const __grid_constant__ CUtensorMap m0,
-                                                                    const __grid_constant__ CUtensorMap m1,
-                                                                    const __grid_constant__ CUtensorMap m2, FftParams p,
-                                                                    TmaTiles tt)
+__global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_analys_kernel(
+	const __grid_constant__ CUtensorMap m0, const __grid_constant__ CUtensorMap m1, const __grid_constant__ CUtensorMap m2,
+	FftParams p, TmaTiles tt)
 {
 	using G = Geo<N, S>;
 	extern __shared__ __align__(128) char fsm[];
@@ -756,7 +792,9 @@ __global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_analys_
 				issue(next);
 			}
 		};
-		fused_fft<N, S, false>(X, p.tw, -1, ld, st, prefetch, threadIdx.x, typename NphiPlan<N>::L{});
+		fused_fft<N, S, 0>(X, p.tw, -1, ld, st, prefetch, threadIdx.x, typename NphiPlan<N>::L{});
+		// Fourier rows with per-thread stores (a tensor store of the tile would
+		// hold every thread's outputs in registers across a barrier)
 		double2* Ff = p.F + (long)fc * p.fstride;
 		const double sc = 0.5 / N;
 		int ne = (p.mlim + 1) * S;
@@ -818,48 +856,69 @@ int sm_count()
 	return n;
 }
 
+// F[fc][k][theta] as FP64 rows of 2 nlat doubles: box (2 S latitudes, box k)
+bool f_map(CUtensorMap* m, const FftParams& p, int nfc, int S, int box)
+{
+	return encode3(m, p.F, 2 * (uint64_t) p.nlat, p.mlim + 1, nfc, 16 * (uint64_t) p.nlat, 16 * (uint64_t) p.fstride, 4 * S, box);
+}
+
+// theta-contiguous spatial component c: dims (nlat, nphi, fields)
+bool grid_map(CUtensorMap* m, const double* base, const FftParams& p, int N, int S)
+{
+	return encode3(m, base, p.nlat, N, p.nf, 8 * (uint64_t) p.nlat, 8 * (uint64_t) p.spat_dist, 2 * S, box_j(N));
+}
+
 template <int N, int S>
 bool launch_fft4(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 {
 	using G = Geo<N, S>;
-	alignas(64) CUtensorMap maps[3];
+	alignas(64) CUtensorMap maps[4];        // synthesis: F, output components; analysis: input components
 	TmaTiles tt;
 	tt.nlg = (p.nlat + 2 * S - 1) / (2 * S);
 	tt.ntiles = tt.nlg * nfc;
+	const int rows = p.mlim + 1;
+	const int kbox = rows < 256 ? rows : 256;            // k rows per box of F
+	const int ncomp = (nfc + p.nf - 1) / p.nf;
+	// tensor maps over the theta-contiguous grid (16-byte aligned, even nlat)
+	const bool grid_ok = p.vec2 && !p.phi_contiguous && !(p.nlat & 1) && N % box_j(N) == 0;
+	const bool tstore = (p.generic != 3);               // option 3 = 3: prefetched loads, direct stores
+	bool tout = false;
 	size_t stage_bytes;
 	if (synth) {
-		const int rows = p.mlim + 1;
-		tt.box = rows < 256 ? rows : 256;
+		tt.box = kbox;
 		tt.ncopy = (rows + tt.box - 1) / tt.box;
 		stage_bytes = (size_t) tt.ncopy * tt.box * 2 * S * 16;
-		if (!encode3(&maps[0], p.F, 2 * (uint64_t) p.nlat, rows, nfc, 16 * (uint64_t) p.nlat, 16 * (uint64_t) p.fstride, 4 * S, tt.box))
-			return false;
+		if (!f_map(&maps[0], p, nfc, S, tt.box)) return false;
+		tout = grid_ok && tstore;
+		for (int c = 0; c < 3 && tout; c++) tout = grid_map(&maps[1 + c], p.spat[c < ncomp ? c : 0], p, N, S);
 	} else {
 		// theta-contiguous grids only (phi-contiguous rows are read faster
 		// straight from global memory by the direct kernel)
-		if (!p.vec2 || p.phi_contiguous || (p.nlat & 1)) return false;
+		if (!grid_ok) return false;
 		tt.box = box_j(N);
-		if (N % tt.box) return false;
 		tt.ncopy = N / tt.box;
 		stage_bytes = (size_t) N * 2 * S * 8;
-		const int ncomp = (nfc + p.nf - 1) / p.nf;
-		for (int c = 0; c < 3; c++) {
-			const double* base = p.spat_in[c < ncomp ? c : 0];
-			if (!encode3(&maps[c], base, p.nlat, N, p.nf, 8 * (uint64_t) p.nlat, 8 * (uint64_t) p.spat_dist, 2 * S, tt.box))
-				return false;
-		}
+		for (int c = 0; c < 3; c++)
+			if (!grid_map(&maps[c], p.spat_in[c < ncomp ? c : 0], p, N, S)) return false;
 	}
 	tt.bytes = (unsigned) stage_bytes;
 	tt.stage_off = (int)(((size_t) S * G::SEQ * sizeof(double2) + 127) / 128 * 128);
 	const size_t smem = tt.stage_off + stage_bytes + 128;
 	if (smem > 226 * 1024) return false;
+	const void* fn = synth ? (tout ? (const void*) fft4_synth_kernel<N, S, true> : (const void*) fft4_synth_kernel<N, S, false>)
+	                       : (const void*) fft4_analys_kernel<N, S>;
 	int per_sm = 0;
-	cudaError_t e = synth ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft4_synth_kernel<N, S>, G::T, smem)
-	                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft4_analys_kernel<N, S>, G::T, smem);
-	if (e != cudaSuccess || per_sm <= 0) { cudaGetLastError(); return false; }
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, G::T, smem) != cudaSuccess || per_sm <= 0) {
+		cudaGetLastError();
+		return false;
+	}
 	const int grid = std::min(tt.ntiles, per_sm * sm_count());
-	if (synth) fft4_synth_kernel<N, S><<<grid, G::T, smem, st>>>(maps[0], p, tt);
-	else fft4_analys_kernel<N, S><<<grid, G::T, smem, st>>>(maps[0], maps[1], maps[2], p, tt);
+	if (synth) {
+		if (tout) fft4_synth_kernel<N, S, true><<<grid, G::T, smem, st>>>(maps[0], maps[1], maps[2], maps[3], p, tt);
+		else fft4_synth_kernel<N, S, false><<<grid, G::T, smem, st>>>(maps[0], maps[0], maps[0], maps[0], p, tt);
+	} else {
+		fft4_analys_kernel<N, S><<<grid, G::T, smem, st>>>(maps[0], maps[1], maps[2], p, tt);
+	}
 	return true;
 }
 
@@ -909,7 +968,7 @@ bool launch_fft4_n(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 
 bool launch_fused(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 {
-	if (p.generic == 0) {
+	if (p.generic == 0 || p.generic == 3) {
 		bool done = false;
 		switch (p.N) {
 			case 192: done = launch_fft4_n<192>(p, nfc, st, synth); break;
@@ -934,6 +993,14 @@ bool launch_fused(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 	}
 }
 
+template <int N, int S>
+void set_fft4_limits(int lim)
+{
+	cudaFuncSetAttribute(fft4_synth_kernel<N, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	cudaFuncSetAttribute(fft4_synth_kernel<N, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+	cudaFuncSetAttribute(fft4_analys_kernel<N, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+}
+
 template <int N>
 void set_fused_limits()
 {
@@ -941,16 +1008,9 @@ void set_fused_limits()
 	if constexpr (N + (N >> 3) + 8 <= 6400) {
 		// the prefetching kernels also hold an mbarrier in static shared memory
 		const int lim4 = 226 * 1024;
-		cudaFuncSetAttribute(fft4_synth_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim4);
-		cudaFuncSetAttribute(fft4_analys_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim4);
-		if constexpr (2 * N / 8 <= 768) {
-			cudaFuncSetAttribute(fft4_synth_kernel<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim4);
-			cudaFuncSetAttribute(fft4_analys_kernel<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim4);
-		}
-		if constexpr (4 * N / 8 <= 768) {
-			cudaFuncSetAttribute(fft4_synth_kernel<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim4);
-			cudaFuncSetAttribute(fft4_analys_kernel<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim4);
-		}
+		set_fft4_limits<N, 1>(lim4);
+		if constexpr (2 * N / 8 <= 768) set_fft4_limits<N, 2>(lim4);
+		if constexpr (4 * N / 8 <= 768) set_fft4_limits<N, 4>(lim4);
 	}
 	cudaFuncSetAttribute(fft3_synth_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 	cudaFuncSetAttribute(fft3_analys_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);

@@ -847,8 +847,9 @@ extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
 			launch_checkpoints(s, 0);
 			return shtb_cuda_ok(cudaDeviceSynchronize(), "checkpoint rebuild") ? 0 : -1;
 		}
-		case 3:   // FFT kernels: 0 automatic, 1 generic mixed-radix, 2 fused without prefetch
-			if (value < 0 || value > 2) return -1;
+		case 3:   // FFT kernels: 0 automatic, 1 generic mixed-radix, 2 fused without prefetch,
+		          // 3 prefetched loads with per-thread stores
+			if (value < 0 || value > 3) return -1;
 			s->fft_generic = value;
 			return 0;
 		default:

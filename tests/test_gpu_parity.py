@@ -324,9 +324,12 @@ def test_simt_legendre_matches_tensor_tiles(case):
                                   "l511_nlat770_ltr"])
 def test_prefetched_fft_matches_direct(case):
     """Option 3 (FFT kernels): the automatic choice, persistent CTAs that fetch
-    their next latitude tile with tensor copies (option 6 reports 2), computes
-    the same passes as the direct-load fused kernels (option 3 = 2): results
-    agree bit for bit, and with the generic mixed-radix kernels to rounding."""
+    their next latitude tile with tensor copies (option 6 reports 2) and on
+    theta-contiguous grids store whole synthesis tiles with tensor stores
+    (phi-contiguous analysis keeps the direct kernel), computes the
+    same passes as the same kernels with per-thread stores (option 3 = 3) and
+    as the direct-load fused kernels (option 3 = 2): results agree bit for
+    bit, and with the generic mixed-radix kernels to rounding."""
     import shtns_b200
     from shtns_b200 import capi
     lib = capi.load()
@@ -346,7 +349,7 @@ def test_prefetched_fft_matches_direct(case):
              for i in range(ncomp)]
     kw = {} if ltr is None else {"ltr": ltr}
     res = {}
-    for opt in (0, 2, 1):
+    for opt in (0, 3, 2, 1):
         assert lib.shtns_b200_set_option(sh._cfg, 3, opt) == 0
         spat = [torch.empty((nf,) + sh.spat_shape, dtype=torch.float64, device=dev) for _ in range(ncomp)]
         sh.synth_into(specs, spat, **kw)
@@ -357,9 +360,11 @@ def test_prefetched_fft_matches_direct(case):
         torch.cuda.synchronize()
         res[opt] = (spat, back, path_s, path_a)
     assert lib.shtns_b200_kernel_errors(sh._cfg) == 0
-    assert res[0][2:] == (2, 2) and res[2][2:] == (1, 1) and res[1][2:] == (0, 0)
-    for a, b in zip(res[0][0] + res[0][1], res[2][0] + res[2][1]):
-        assert torch.equal(a, b)
+    ana = 1 if phi else 2             # phi-contiguous analysis keeps the direct kernel
+    assert res[0][2:] == (2, ana) and res[3][2:] == (2, ana) and res[2][2:] == (1, 1) and res[1][2:] == (0, 0)
+    for o in (3, 2):
+        for a, b in zip(res[0][0] + res[0][1], res[o][0] + res[o][1]):
+            assert torch.equal(a, b)
     for a, b in zip(res[0][0] + res[0][1], res[1][0] + res[1][1]):
         assert float((a - b).abs().max()) <= 1e-13 * float(b.abs().max())
-    assert lib.shtns_b200_set_option(sh._cfg, 3, 3) == -1
+    assert lib.shtns_b200_set_option(sh._cfg, 3, 4) == -1
