@@ -582,6 +582,7 @@ struct TmaTiles {
 	int box;          // rows (k or j) per box
 	unsigned bytes;   // bytes per tile (all boxes, out-of-range parts included)
 	int stage_off;    // staging buffer offset in the dynamic shared memory (bytes)
+	int v4;           // F rows 32-byte aligned at even latitudes: one 32-byte store per latitude pair
 };
 
 constexpr uint64_t FT_WAIT_NS = 1000000000ull;   // time limit of every mbarrier wait
@@ -805,8 +806,13 @@ __global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_analys_
 			const double2 z = X[G::at(s, k)];
 			const double2 w = X[G::at(s, k ? N - k : 0)];
 			if (ra < nlat) {
-				Ff[(long)k * nlat + ra] = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
-				Ff[(long)k * nlat + ra + 1] = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
+				const double2 fa = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
+				const double2 fb = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
+				double2* o = Ff + (long)k * nlat + ra;
+				if (tt.v4)
+					asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};"
+					             :: "l"(o), "d"(fa.x), "d"(fa.y), "d"(fb.x), "d"(fb.y) : "memory");
+				else { o[0] = fa; o[1] = fb; }
 			}
 		}
 	}
@@ -902,6 +908,7 @@ bool launch_fft4(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 			if (!grid_map(&maps[c], p.spat_in[c < ncomp ? c : 0], p, N, S)) return false;
 	}
 	tt.bytes = (unsigned) stage_bytes;
+	tt.v4 = !((uintptr_t) p.F & 31) && !(p.nlat & 1) && !(p.fstride & 1);
 	tt.stage_off = (int)(((size_t) S * G::SEQ * sizeof(double2) + 127) / 128 * 128);
 	const size_t smem = tt.stage_off + stage_bytes + 128;
 	if (smem > 226 * 1024) return false;
