@@ -45,13 +45,14 @@ def spectral_inputs(nf, seed):
     return q, s, t
 
 
-# DRAM bytes (read + write) per field of one launch of each Legendre kernel on
-# this workload, from an ncu capture of the 8-field case (dram__bytes_read.sum +
-# dram__bytes_write.sum); the traffic grows in proportion to the field count.
+# DRAM bytes (read + write) per field of one launch of each Legendre and FFT
+# kernel on this workload, from an ncu capture of the 8-field case
+# (dram__bytes_read.sum + dram__bytes_write.sum); the traffic grows in
+# proportion to the field count.
 TRAFFIC_PER_FIELD = {"legendre_synthesis": (98.216960e6 + 92.500992e6) / 8,
                      "legendre_analysis": (153.142784e6 + 34.128384e6) / 8,
-                     "fft_synthesis": (151.062784e6 + 178.811648e6) / 8,
-                     "fft_analysis": (226.558976e6 + 114.498816e6) / 8}
+                     "fft_synthesis": (152.880640e6 + 178.261760e6) / 8,
+                     "fft_analysis": (226.571520e6 + 108.823552e6) / 8}
 TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 8-field case, scaled by fields"
 
 
@@ -362,7 +363,7 @@ def run_gpu(args):
         per_launch = ms_stage / np.maximum(calls, 1)
         share = ms_stage / max(ms_stage.sum(), 1e-30)
         names = ["prologue", "legendre_synthesis", "fft_synthesis", "fft_analysis", "legendre_analysis", "epilogue"]
-        dom = int(np.argmax(ms_stage))
+        dom = 1 + int(np.argmax(ms_stage[1:5]))       # dominant of the Legendre and FFT stages
         peaks = measured_peaks()
         hbm = peaks.get("hbm_gbs", 6650.0)
         fft_bytes = 3 * nf * (NLAT * (LMAX + 1) * 16 + NLAT * NPHI * 8)

@@ -555,8 +555,13 @@ __global__ void __launch_bounds__(Geo<N, S>::T) fft3_analys_kernel(FftParams p)
 		const double2 z = smem[G::at(s, k)];
 		const double2 w = smem[G::at(s, k ? N - k : 0)];
 		if (ra < nlat) {
-			Ff[(long)k * nlat + ra] = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
-			Ff[(long)k * nlat + ra + 1] = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
+			const double2 fa = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
+			const double2 fb = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
+			double2* o = Ff + (long)k * nlat + ra;
+			if (((uintptr_t) o & 31) == 0)      // one 32-byte store for the latitude pair
+				asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};"
+				             :: "l"(o), "d"(fa.x), "d"(fa.y), "d"(fb.x), "d"(fb.y) : "memory");
+			else { o[0] = fa; o[1] = fb; }
 		}
 	}
 }
