@@ -80,7 +80,12 @@ void cu_spat_to_SH_adjoint(shtns_cfg, cplx *Qg, double *Vg, int ltr);
  * kernels), 1 = always the generic mixed-radix kernels, 2 = the fused
  * kernels without prefetch, 3 = prefetched loads with per-thread stores.
  * Option 6 (get only): FFT kernels of the last launch in this process, 0
- * generic, 1 fused direct, 2 prefetched.  Return 0 or -1.
+ * generic, 1 fused direct, 2 prefetched.  Option 7 (test hook, default 0):
+ * bytes, a multiple of 16 up to 4096, that the prefetching FFT kernels wait
+ * for beyond what their tensor copies bring; a positive value makes their
+ * bounded wait (about one second) give up, so that tests can check the error
+ * path (shtns_b200_kernel_errors returns 1, no output is written).  Return 0
+ * or -1.
  * No counterpart in SHTns 3.5.2. */
 int shtns_b200_set_option(shtns_cfg, int option, int value);
 int shtns_b200_get_option(shtns_cfg, int option);

@@ -134,6 +134,7 @@ FftParams fft_params(shtns_cfg s, const Job& j, int nrows = 0)
 	p.phi_contiguous = s->phi_contiguous;
 	// generic kernels need two buffers
 	p.generic = (s->fft_generic == 1) ? (fft_smem_bytes(s->nphi, 1) <= 227 * 1024 ? 1 : 0) : s->fft_generic;
+	p.extra_tx = s->fft_extra_tx;
 	return p;
 }
 

@@ -912,7 +912,7 @@ bool launch_fft4(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 		for (int c = 0; c < 3; c++)
 			if (!grid_map(&maps[c], p.spat_in[c < ncomp ? c : 0], p, N, S)) return false;
 	}
-	tt.bytes = (unsigned) stage_bytes;
+	tt.bytes = (unsigned) (stage_bytes + p.extra_tx);
 	tt.v4 = !((uintptr_t) p.F & 31) && !(p.nlat & 1) && !(p.fstride & 1);
 	tt.stage_off = (int)(((size_t) S * G::SEQ * sizeof(double2) + 127) / 128 * 128);
 	const size_t smem = tt.stage_off + stage_bytes + 128;

@@ -78,6 +78,7 @@ struct shtns_info {
 	int ckseg;                           // checkpoint spacing in k
 	int fft_pairs;                       // latitude pairs per FFT CTA (0: automatic)
 	int fft_generic;                     // FFT kernels: 0 automatic, 1 generic mixed-radix, 2 fused without prefetch, 3 no tensor stores
+	int fft_extra_tx;                    // test hook: bytes the prefetching FFT kernels expect beyond their copies (0)
 	int tile_wm;                         // Legendre tile shape option (0 automatic)
 	std::vector<int> fft_radix;          // factorisation of nphi
 	double Y00_1, Y10_ct, Y11_st;
@@ -195,6 +196,7 @@ struct FftParams {
 	long spat_dist;
 	int phi_contiguous;
 	int vec2;                            // spatial pointers 16-byte aligned: latitude pairs moved as double2
+	int extra_tx;                        // test hook: extra bytes expected per prefetched tile (0)
 	int generic;                         // 0 automatic, 1 generic mixed-radix kernels, 2 fused kernels without prefetch,
 	                                     // 3 prefetched loads with per-thread stores
 };

@@ -852,6 +852,11 @@ extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
 			if (value < 0 || value > 3) return -1;
 			s->fft_generic = value;
 			return 0;
+		case 7:   // test hook: bytes the prefetching FFT kernels wait for beyond their tensor copies, 0..4096
+		          // (a positive value makes their bounded wait give up: error-path tests)
+			if (value < 0 || value > 4096 || (value & 15)) return -1;
+			s->fft_extra_tx = value;
+			return 0;
 		default:
 			return -1;
 	}
@@ -867,6 +872,7 @@ extern "C" int shtns_b200_get_option(shtns_cfg s, int option)
 		case 4: return s->split_ns;
 		case 5: return s->tile_wm;
 		case 6: return fft_last_path();   // FFT kernels of the last launch in this process
+		case 7: return s->fft_extra_tx;
 		default: return -1;
 	}
 }

@@ -368,3 +368,33 @@ def test_prefetched_fft_matches_direct(case):
     for a, b in zip(res[0][0] + res[0][1], res[1][0] + res[1][1]):
         assert float((a - b).abs().max()) <= 1e-13 * float(b.abs().max())
     assert lib.shtns_b200_set_option(sh._cfg, 3, 4) == -1
+
+
+def test_prefetched_fft_wait_limit_reports_and_recovers():
+    """The prefetching FFT kernels wait on an mbarrier for their tensor copies
+    with a time limit.  Option 7 makes them expect 16 bytes more than the
+    copies bring, so the wait gives up after about a second: the kernel sets
+    the error flag that shtns_b200_kernel_errors reads (and clears) and
+    returns without storing.  The context stays usable: the next transforms
+    on the same plan are correct."""
+    import shtns_b200
+    from shtns_b200 import capi
+    lib = capi.load()
+    dev = torch.device("cuda:0")
+    L = 63
+    sh = shtns_b200.sht(L)
+    sh.set_grid(96, 192, flags=shtns_b200.sht_quick_init | shtns_b200.SHT_THETA_CONTIGUOUS, polar_opt=0.0)
+    q = torch.from_numpy(rand_spec(L, L, 1, 71, nfields=2)).to(dev)
+    v = torch.empty((2,) + sh.spat_shape, dtype=torch.float64, device=dev)
+    assert lib.shtns_b200_kernel_errors(sh._cfg) == 0
+    assert lib.shtns_b200_set_option(sh._cfg, 7, 8) == -1          # not a multiple of 16
+    assert lib.shtns_b200_set_option(sh._cfg, 7, 16) == 0
+    sh.synth_into([q], [v])
+    assert lib.shtns_b200_get_option(sh._cfg, 6) == 2             # the prefetching kernel ran
+    assert lib.shtns_b200_kernel_errors(sh._cfg) == 1
+    assert lib.shtns_b200_kernel_errors(sh._cfg) == 0             # cleared by the read
+    assert lib.shtns_b200_set_option(sh._cfg, 7, 0) == 0
+    v = sh.synth(q)
+    back = sh.analys(v)
+    assert lib.shtns_b200_kernel_errors(sh._cfg) == 0
+    assert relerr(q.cpu().numpy(), back.cpu().numpy()) < 1e-12
