@@ -417,16 +417,60 @@ __device__ __forceinline__ void mid_pass(double2* X, const double2* __restrict__
 	__syncthreads();
 }
 
+// Last pass of an analysis chain ending in radix 3 (P = N/3): thread item
+// (s, b), b = 0 .. P/2, runs the butterflies b and P - b of sequence s, which
+// hold both members of the pairs (z_k, z_{N-k}) for k = b, P - b and P + b
+// (b = 0: k = 0, P; b = P/2: k = P/2), and hands each pair to st(s, k, z_k,
+// z_{N-k}).  Every k < N/2 is handed over once; no shared-memory output.
+template <int N, int S, class Store>
+__device__ __forceinline__ void last_pass_pairs(const double2* X, const double2* __restrict__ tw, int sign, Store& st, int tid)
+{
+	using G = Geo<N, S>;
+	constexpr int P = N / 3, H = P / 2, ITEMS = S * (H + 1), NB = (ITEMS + G::T - 1) / G::T;
+	#pragma unroll
+	for (int i = 0; i < NB; i++) {
+		const int g = tid + i * G::T;
+		if (g < ITEMS) {
+			const int s = g % S, b = g / S;
+			double2 u[3];
+			#pragma unroll
+			for (int q = 0; q < 3; q++) u[q] = X[G::at(s, b + q * P)];
+			if (b) twiddle<3>(u, tw, b, sign);
+			Dft<3>::run(u, sign);                       // z_{b + q P} = u[q]
+			if (b == 0) {
+				st(s, 0, u[0], u[0]);
+				st(s, P, u[1], u[2]);
+			} else if (b == H) {
+				st(s, H, u[0], u[2]);
+			} else {
+				const int bp = P - b;
+				double2 v[3];
+				#pragma unroll
+				for (int q = 0; q < 3; q++) v[q] = X[G::at(s, bp + q * P)];
+				twiddle<3>(v, tw, bp, sign);
+				Dft<3>::run(v, sign);                   // z_{P - b + q P} = v[q]
+				st(s, b, u[0], v[2]);
+				st(s, bp, v[0], u[2]);
+				st(s, P + b, u[1], v[1]);
+			}
+		}
+	}
+}
+
 // Pass chain: first pass from a loader, middle passes in shared memory, last
-// pass to shared memory (MODE 0), to a storer (MODE 1) or to shared memory in
-// rows of S complex values (MODE 2).
+// pass to shared memory (MODE 0), to a storer (MODE 1), to shared memory in
+// rows of S complex values (MODE 2), or as (z_k, z_{N-k}) pairs to a storer
+// (MODE 3, last radix 3).
 template <int N, int S, int P, int MODE, int R, int... Rest>
 struct Chain {
 	template <class Store>
 	static __device__ __forceinline__ void run(double2* X, const double2* tw, int sign, Store& st, int tid)
 	{
 		if constexpr (sizeof...(Rest) == 0) {
-			if constexpr (MODE == 1) {
+			if constexpr (MODE == 3) {
+				static_assert(R == 3 && P * 3 == N, "the pair pass is the last radix-3 pass");
+				last_pass_pairs<N, S>(X, tw, sign, st, tid);
+			} else if constexpr (MODE == 1) {
 				// last pass: k = b (b < P = N/R), outputs b + q*P go to global memory
 				using G = Geo<N, S>;
 				constexpr int NBF = N / R, TOT = S * NBF, NB = (TOT + G::T - 1) / G::T, TSTEP = N / (P * R);
@@ -528,7 +572,6 @@ template <int N, int S>
 __global__ void __launch_bounds__(Geo<N, S>::T) fft3_analys_kernel(FftParams p)
 {
 	extern __shared__ double2 smem[];
-	using G = Geo<N, S>;
 	const int fc = blockIdx.y;
 	const int lat0 = blockIdx.x * 2 * S;
 	const int nlat = p.nlat;
@@ -544,26 +587,22 @@ __global__ void __launch_bounds__(Geo<N, S>::T) fft3_analys_kernel(FftParams p)
 		}
 		return make_double2(__ldg(in + (long)row * N + j), __ldg(in + (long)(row + 1) * N + j));
 	};
-	int dummy = 0;
-	auto st = [&](int, int, double2) { dummy++; };
-	fused_fft<N, S, false>(smem, p.tw, -1, ld, st, NoHook{}, threadIdx.x, typename NphiPlan<N>::L{});
+	// Fourier rows straight from the last radix pass (pairs z_k, z_{N-k})
 	double2* Ff = p.F + (long)fc * p.fstride;
 	const double sc = 0.5 / N;
-	for (int e = threadIdx.x; e < (p.mlim + 1) * S; e += G::T) {
-		const int k = e / S, s = e - k * S;
+	const int ml = p.mlim;
+	auto st = [&](int s, int k, double2 z, double2 w) {
 		const int ra = lat0 + 2 * s;
-		const double2 z = smem[G::at(s, k)];
-		const double2 w = smem[G::at(s, k ? N - k : 0)];
-		if (ra < nlat) {
-			const double2 fa = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
-			const double2 fb = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
-			double2* o = Ff + (long)k * nlat + ra;
-			if (((uintptr_t) o & 31) == 0)      // one 32-byte store for the latitude pair
-				asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};"
-				             :: "l"(o), "d"(fa.x), "d"(fa.y), "d"(fb.x), "d"(fb.y) : "memory");
-			else { o[0] = fa; o[1] = fb; }
-		}
-	}
+		if (k > ml || ra >= nlat) return;
+		const double2 fa = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
+		const double2 fb = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
+		double2* o = Ff + (long)k * nlat + ra;
+		if (((uintptr_t) o & 31) == 0)      // one 32-byte store for the latitude pair
+			asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};"
+			             :: "l"(o), "d"(fa.x), "d"(fa.y), "d"(fb.x), "d"(fb.y) : "memory");
+		else { o[0] = fa; o[1] = fb; }
+	};
+	fused_fft<N, S, 3>(smem, p.tw, -1, ld, st, NoHook{}, threadIdx.x, typename NphiPlan<N>::L{});
 }
 
 // ---------------------------------------------------------------------------
@@ -789,8 +828,6 @@ __global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_analys_
 		int rs = 2 * S;                         // opaque per tile, as mlim in the synthesis
 		asm volatile("" : "+r"(rs));
 		auto ld = [&](int s, int j) -> double2 { return *reinterpret_cast<const double2*>(stg + j * rs + 2 * s); };
-		int dummy = 0;
-		auto st = [&](int, int, double2) { dummy++; };
 		const int next = tile + gridDim.x;
 		auto prefetch = [&]() {
 			if (threadIdx.x == 0 && next < tt.ntiles) {
@@ -798,45 +835,38 @@ __global__ void __launch_bounds__(Geo<N, S>::T, 768 / Geo<N, S>::T) fft4_analys_
 				issue(next);
 			}
 		};
-		fused_fft<N, S, 0>(X, p.tw, -1, ld, st, prefetch, threadIdx.x, typename NphiPlan<N>::L{});
-		// Fourier rows with per-thread stores (a tensor store of the tile would
-		// hold every thread's outputs in registers across a barrier)
+		// Fourier rows straight from the last radix pass: F_k of the two
+		// latitudes of sequence s from (z_k, z_{N-k}), one 32-byte store
 		double2* Ff = p.F + (long)fc * p.fstride;
 		const double sc = 0.5 / N;
-		int ne = (p.mlim + 1) * S;
-		asm volatile("" : "+r"(ne));             // opaque per tile, as the first pass's values
-		for (int e = threadIdx.x; e < ne; e += G::T) {
-			const int k = e / S, s = e - k * S;
+		const int ml = p.mlim;
+		auto st = [&](int s, int k, double2 z, double2 w) {
 			const int ra = lat0 + 2 * s;
-			const double2 z = X[G::at(s, k)];
-			const double2 w = X[G::at(s, k ? N - k : 0)];
-			if (ra < nlat) {
-				const double2 fa = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
-				const double2 fb = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
-				double2* o = Ff + (long)k * nlat + ra;
-				if (tt.v4)
-					asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};"
-					             :: "l"(o), "d"(fa.x), "d"(fa.y), "d"(fb.x), "d"(fb.y) : "memory");
-				else { o[0] = fa; o[1] = fb; }
-			}
-		}
+			if (k > ml || ra >= nlat) return;
+			const double2 fa = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
+			const double2 fb = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
+			double2* o = Ff + (long)k * nlat + ra;
+			if (tt.v4)
+				asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};"
+				             :: "l"(o), "d"(fa.x), "d"(fa.y), "d"(fb.x), "d"(fb.y) : "memory");
+			else { o[0] = fa; o[1] = fb; }
+		};
+		fused_fft<N, S, 3>(X, p.tw, -1, ld, st, prefetch, threadIdx.x, typename NphiPlan<N>::L{});
 	}
 }
 
+// the driver's tensor-map encoder, resolved once (thread-safe static initialisation)
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
-	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-	static bool tried = false;
-	if (!tried) {
-		tried = true;
+	static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
 		void* f = nullptr;
 		cudaDriverEntryPointQueryResult q;
 		if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
 		    q == cudaDriverEntryPointSuccess)
-			fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-		else
-			cudaGetLastError();
-	}
+			return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+		cudaGetLastError();
+		return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+	}();
 	return fn;
 }
 
@@ -858,12 +888,12 @@ bool encode3(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_
 
 int sm_count()
 {
-	static int n = 0;
-	if (!n) {
-		int dev = 0;
+	static const int n = [] {
+		int dev = 0, c = 0;
 		cudaGetDevice(&dev);
-		if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) { cudaGetLastError(); n = 148; }
-	}
+		if (cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || c <= 0) { cudaGetLastError(); c = 148; }
+		return c;
+	}();
 	return n;
 }
 
