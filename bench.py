@@ -347,6 +347,29 @@ def run_gpu(args):
     f1.record()
     f1.synchronize()
     ms_e2e = f0.elapsed_time(f1) / e2e_steps
+
+    # the link's own ceiling on this machine: the same copies on the same
+    # streams and chunks, without the transforms
+    def copy_step():
+        for (a, b), st in zip(bounds, streams):
+            with torch.cuda.stream(st):
+                for d, h in zip(spec, host_in):
+                    d[a:b].copy_(h[a:b], non_blocking=True)
+                for h, d in zip(host_out, back):
+                    h[a:b].copy_(d[a:b], non_blocking=True)
+
+    fork()
+    copy_step()
+    join()
+    torch.cuda.synchronize()
+    f0.record()
+    fork()
+    for _ in range(e2e_steps):
+        copy_step()
+    join()
+    f1.record()
+    f1.synchronize()
+    ms_link = f0.elapsed_time(f1) / e2e_steps
     if world > 1:
         t = torch.tensor([ms_e2e], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -416,8 +439,12 @@ def run_gpu(args):
             "e2e": {"value": world * nf / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
                     "d2h_bytes_per_step": bytes_io,
                     "form": f"{nch} field chunks on {nch} streams with plan clones: copies overlap transforms "
-                            "and the next step's copies (pinned-host link ceiling measured here: "
-                            "47.7 GB/s per direction when both run)"},
+                            "and the next step's copies",
+                    "link_ceiling": {"ms_per_step": ms_link,
+                                     "gbs_per_direction": bytes_io / (ms_link * 1e-3) / 1e9,
+                                     "value": world * nf / (ms_link * 1e-3),
+                                     "note": "the same pinned-host copies on the same streams without the "
+                                             "transforms, timed in this run (both directions at once)"}},
             "clocks": clk,
         }
         if world == 1 and not args.no_cpu:
