@@ -532,6 +532,13 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 	constexpr int SPT = (NSG + GPT - 1) / GPT;            // segments per generator thread
 	double2 ckn[SPT];
 	const int gtt = tid % LG_BK, gsg = tid / LG_BK;
+	// vector flag of each staging item's field-component (fixed per thread)
+	bool vecn[NBF];
+	#pragma unroll
+	for (int u = 0; u < NBF; u++) {
+		const int fc = fc0 + (tid + u * LG_THREADS) / LG_BK;
+		vecn[u] = fc < p.nfc && p.ctype[fc / p.nf] != 0;
+	}
 	auto load_next = [&](int tt0) {
 		#pragma unroll
 		for (int u = 0; u < NBF; u++) {
@@ -597,7 +604,7 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 			if (t < p.nlat_2 && fc < p.nfc) {
 				// adjoint of the synthesis: no quadrature weight, factor nphi (2 - delta_m0)
 				double w = p.adjoint ? p.nphi * (m > 0 ? 2.0 : 1.0) : p.w[t] * wfac;
-				if (p.ctype[fc / p.nf] != 0) {
+				if (vecn[u]) {
 					double s = p.sinv[t];
 					if (p.robert) s *= s;
 					w *= s;
