@@ -212,6 +212,12 @@ __global__ void __launch_bounds__(SA_NT) leg_analys_simt_kernel(LegParams p)
 		}
 	};
 	if (tstart < p.nlat_2) load_next(tstart);
+	bool vg[2];                                     // vector flag of each staging item's field-component
+	#pragma unroll
+	for (int i = 0; i < 2; i++) {
+		const int gf = (tid + i * nt) / SA_TB;
+		vg[i] = gf < NFC && p.ctype[gf / p.nf] != 0;
+	}
 	for (int tt0 = tstart; tt0 < p.nlat_2; tt0 += SA_TB) {
 		// phase 1: Y of (row gr, this thread's segments) and G of (row gt, component gf)
 		{
@@ -247,7 +253,7 @@ __global__ void __launch_bounds__(SA_NT) leg_analys_simt_kernel(LegParams p)
 				double er = 0.0, ei = 0.0, orr = 0.0, oi = 0.0;
 				if (tg < p.nlat_2) {
 					double w = p.adjoint ? p.nphi * (m > 0 ? 2.0 : 1.0) : p.w[tg] * wfac;
-					if (p.ctype[gf / p.nf] != 0) {
+					if (vg[i]) {
 						double s = p.sinv[tg];
 						if (p.robert) s *= s;
 						w *= s;
@@ -361,6 +367,9 @@ __global__ void __launch_bounds__(SR_NT) leg_analys_reg_kernel(LegParams p)
 		nx2 = __ldg(p.x2 + t);
 		nsv = __ldg(p.sinv + t);
 	};
+	bool vf[NFC];                                   // vector flag per field-component
+	#pragma unroll
+	for (int f = 0; f < NFC; f++) vf[f] = p.ctype[f / p.nf] != 0;
 	load_row(tmm + tid);
 	for (int t = tmm + tid; t < p.nlat_2; t += nt) {
 		// G of this row: w (F_N + F_S), w cos (F_N - F_S) per field-component
@@ -370,7 +379,7 @@ __global__ void __launch_bounds__(SR_NT) leg_analys_reg_kernel(LegParams p)
 		#pragma unroll
 		for (int f = 0; f < NFC; f++) {
 			double w = p.adjoint ? p.nphi * (m > 0 ? 2.0 : 1.0) : nw * wfac;
-			if (p.ctype[f / p.nf] != 0) {
+			if (vf[f]) {
 				double sv = nsv;
 				if (p.robert) sv *= sv;
 				w *= sv;
