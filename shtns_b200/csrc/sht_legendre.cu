@@ -567,6 +567,11 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 			                                               : make_double2(0.0, 0.0);
 		}
 	};
+	// recurrence coefficients of the CTA's k rows, staged once (rows at or
+	// beyond nk get zeros: their results are not stored)
+	__shared__ double cs[2 * BM];
+	for (int e = tid; e < 2 * BM; e += LG_THREADS) cs[e] = (k0 + e / 2 < nk) ? cm[2 * k0 + e] : 0.0;
+	__syncthreads();
 	const int tstart = (tmm / LG_BK) * LG_BK;
 	if (tstart < p.nlat_2) load_next(tstart);
 	for (int tt0 = tstart; tt0 < p.nlat_2; tt0 += LG_BK) {
@@ -582,7 +587,7 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 				a[0] = y0;
 				a[AA_LD] = y1;
 				if (gks < nk) {
-					const double* cc = cm + 2 * gks;
+					const double* cc = cs + 2 * sg * SEG;
 					#pragma unroll
 					for (int j = 2; j < SEG; j++) {
 						const double aa = fma(cc[2 * j - 1], x2, cc[2 * j - 2]);
