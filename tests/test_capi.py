@@ -119,3 +119,28 @@ def test_set_batch_validates():
     assert lib.shtns_set_batch(cfg, 0, 0, 0) == -1
     assert lib.shtns_set_batch(cfg, 4, 0, 0) == 0
     lib.shtns_destroy(cfg)
+
+
+def test_plan_options_validate_and_read_back():
+    """shtns_b200_set_option accepts the documented values and rejects the
+    others (return -1, nothing changed); shtns_b200_get_option reads back."""
+    lib = capi.load()
+    cfg = lib.shtns_create(31, 31, 1, capi.sht_orthonormal)
+    cases = {
+        1: ([0, 1, 2, 4, 8], [3, 16, -1]),          # latitude pairs per FFT CTA
+        3: ([0, 1, 2, 3], [4, -1]),                 # FFT kernels
+        4: ([0, 3, 5, 7], [1, 2, 8]),               # split-precision slices
+        5: ([0, 1, 2, 4, 8], [3, 16]),              # Legendre tile shape
+        7: ([0, 16, 4096], [8, 4112, -16]),         # test hook of the FFT wait
+    }
+    for opt, (good, bad) in cases.items():
+        for v in good:
+            assert lib.shtns_b200_set_option(cfg, opt, v) == 0, (opt, v)
+            assert lib.shtns_b200_get_option(cfg, opt) == v, (opt, v)
+        last = good[-1]
+        for v in bad:
+            assert lib.shtns_b200_set_option(cfg, opt, v) == -1, (opt, v)
+            assert lib.shtns_b200_get_option(cfg, opt) == last, (opt, v)
+    assert lib.shtns_b200_set_option(cfg, 99, 0) == -1
+    assert lib.shtns_b200_get_option(cfg, 99) == -1
+    lib.shtns_destroy(cfg)
