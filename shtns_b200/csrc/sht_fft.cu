@@ -19,6 +19,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 
 namespace {
@@ -989,8 +990,11 @@ bool launch_fft3_n(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 
 } // namespace
 
-static int g_last_fft_path = -1;
-static bool g_fft4_ran = false;
+// kernel family of the last FFT launch in the process (a diagnostic, any
+// thread), and whether the launch in progress on this thread took the
+// prefetching kernels
+static std::atomic<int> g_last_fft_path{-1};
+static thread_local bool g_fft4_ran = false;
 
 namespace {
 
@@ -1100,7 +1104,7 @@ bool fft_fused_available(int N)
 
 // kernel family of the last FFT launch (host side): 0 generic, 1 fused
 // direct loads, 2 fused with prefetched tiles
-int fft_last_path() { return g_last_fft_path; }
+int fft_last_path() { return g_last_fft_path.load(); }
 
 void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st)
 {
