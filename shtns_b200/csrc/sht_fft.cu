@@ -4,10 +4,16 @@
 // sht_gpu.cu:372-446).  As in the reference, two real latitudes a, b are
 // packed into one complex sequence z = v_a + i v_b, so one complex DFT of
 // length nphi transforms a latitude pair; the spectra are separated with
-// Hermitian symmetry.  Each CTA owns one field-component and 2*S consecutive
-// latitudes, holds the S complex sequences in shared memory and runs an
-// mixed-radix (8, 4, 2, 3, 5, 7) self-sorting Stockham transform between two
-// shared-memory buffers.
+// Hermitian symmetry.  A tile is one field-component and 2*S consecutive
+// latitudes; its S complex sequences are transformed in shared memory by a
+// self-sorting Stockham chain.  Three kernel families:
+//   * generic kernels: one tile per CTA, mixed radices (8, 4, 2, 3, 5, 7)
+//     chosen at run time, two shared-memory buffers (any supported nphi);
+//   * fused kernels (fft3_*): nphi = 3 * 2^k with a compile-time radix chain
+//     in one padded in-place buffer, one tile per CTA;
+//   * prefetching kernels (fft4_*, the default up to nphi 3072): persistent
+//     CTAs that fetch their next tile with tensor copies while the current one
+//     is transformed (below).
 //
 // Synthesis input is F[fc][m][theta] (m <= mlim, exact Fourier coefficients of
 // each latitude); output is v(phi_j) = sum_m (2 - delta_m0) Re(F_m e^{i m phi_j}).
