@@ -157,7 +157,8 @@ def reference_cpu_rate(target_s=10.0, fields_per_step=None, steps=None, warmup=1
     with quiet_stdout():
         ref = R.RefSHT(LMAX, LMAX, 1, R.sht_orthonormal, NLAT, NPHI, flags=R.sht_gauss | R.SHT_THETA_CONTIGUOUS,
                        eps=EPS, nthreads=nthreads)
-    q, s, t = spectral_inputs(2, 100)
+    nin = NFIELDS
+    q, s, t = spectral_inputs(nin, 100)
     sp = [np.zeros((NPHI, NLAT)) for _ in range(3)]
     sq = [np.zeros(ref.nlm, dtype=np.complex128) for _ in range(3)]
     P = lambda a: a.ctypes.data_as(C.c_void_p)
@@ -167,17 +168,17 @@ def reference_cpu_rate(target_s=10.0, fields_per_step=None, steps=None, warmup=1
         L.spat_to_SHqst(ref.cfg, P(sp[0]), P(sp[1]), P(sp[2]), P(sq[0]), P(sq[1]), P(sq[2]))
 
     for i in range(max(1, warmup)):
-        pair(i % 2)
+        pair(i % nin)
     n = 0
     t0 = time.perf_counter()
     if steps is None:
         while time.perf_counter() - t0 < target_s or n < 3:
-            pair(n % 2)
+            pair(n % nin)
             n += 1
     else:
         for _ in range(steps):
             for _ in range(fields_per_step):
-                pair(n % 2)
+                pair(n % nin)
                 n += 1
     dt = time.perf_counter() - t0
     ref.close()
@@ -190,9 +191,12 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    fps = 2
-    rate, n, dt, nth = reference_cpu_rate(steps=args.steps, fields_per_step=fps, warmup=args.warmup)
-    sample = f"{args.steps} steps x {fps} field-pairs of the lmax=511 qst workload ({n} pairs, {dt:.1f} s)"
+    # one step = the GPU arm's step: all NFIELDS field-pairs (the same seeded
+    # inputs), one field at a time on all host threads
+    fps = NFIELDS
+    rate, n, dt, nth = reference_cpu_rate(steps=args.steps, fields_per_step=fps, warmup=args.warmup * fps)
+    sample = (f"{args.steps} steps x {fps} field-pairs (the whole {fps}-field step) of the lmax=511 qst workload "
+              f"({n} pairs, {dt:.1f} s)")
     line = {
         "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,

@@ -209,6 +209,36 @@ static void fft_rec(const struct fftw_plan_s *p, int lev, long n, const cpx *in,
 	}
 }
 
+/* ---------- aliasing ----------
+ * FFTW plans may be in place with different input and output layouts (the
+ * reference's rotation FFT is an r2c of howmany transforms at stride howmany
+ * with idist = odist = 1, in == out).  The block loops above write a block's
+ * outputs before later blocks have read their inputs, so whenever the input
+ * and output spans overlap (and the layouts are not identical), every input
+ * is first gathered into a scratch array, as FFTW itself buffers such plans. */
+
+/* [lo, hi) byte span of elements (j, t), j < n, t < howmany, at
+ * base + (j*stride + t*dist)*elem bytes (strides may be negative). */
+static void span(const void *base, long n, long stride, long howmany, long dist, long elem,
+                 const char **lo, const char **hi)
+{
+	long a = 0, b = 0;
+	long js = (n - 1) * stride, ts = (howmany - 1) * dist;
+	if (js < 0) a += js; else b += js;
+	if (ts < 0) a += ts; else b += ts;
+	*lo = (const char *) base + a * elem;
+	*hi = (const char *) base + (b + 1) * elem;
+}
+
+static int spans_overlap(const void *in, long ni, long is, long idist, long ielem,
+                         const void *out, long no, long os, long odist, long oelem, long howmany)
+{
+	const char *il, *ih, *ol, *oh;
+	span(in, ni, is, howmany, idist, ielem, &il, &ih);
+	span(out, no, os, howmany, odist, oelem, &ol, &oh);
+	return il < oh && ol < ih;
+}
+
 /* Run transforms [t0, t1) of a complex plan; input/output element (j, t) is at
  * base + j*stride + t*dist, given as separate real and imaginary pointers with a
  * step of 2 doubles for interleaved complex data or 1 for split arrays. */
@@ -238,12 +268,34 @@ static void run_block(const struct fftw_plan_s *p, long t0, long t1,
 /* Generic complex execution.  step = 2 for interleaved complex arrays (real part
  * at 2*o, imag at 2*o+1), 1 for split arrays.  All reads of a block finish
  * before its writes, and blocks touch disjoint transforms, so in-place plans
- * (in == out, equal strides) are safe. */
+ * with equal layouts run directly; other overlapping plans are gathered first. */
 static void exec_complex(const struct fftw_plan_s *p, const double *ir, const double *ii,
                          double *orr, double *oi, long step)
 {
 	const long nblk = (p->howmany + VB - 1) / VB;
 	const long n = p->n;
+	const int same_layout = (ir == orr && ii == oi && p->is == p->os && p->idist == p->odist);
+	if (!same_layout &&
+	    (spans_overlap(ir, n, p->is * step, p->idist * step, 8, orr, n, p->os * step, p->odist * step, 8, p->howmany) ||
+	     spans_overlap(ir, n, p->is * step, p->idist * step, 8, oi, n, p->os * step, p->odist * step, 8, p->howmany) ||
+	     spans_overlap(ii, n, p->is * step, p->idist * step, 8, orr, n, p->os * step, p->odist * step, 8, p->howmany) ||
+	     spans_overlap(ii, n, p->is * step, p->idist * step, 8, oi, n, p->os * step, p->odist * step, 8, p->howmany))) {
+		/* gather all inputs (same re/im step as the output), then run from the copy */
+		const long tot = n * (long) p->howmany;
+		double *g = (double *) malloc(sizeof(double) * 2 * tot);
+		double *gr = g, *gi = (step == 2) ? g + 1 : g + tot;
+		for (long t = 0; t < p->howmany; t++)
+			for (long j = 0; j < n; j++) {
+				long o = j * p->is + t * p->idist, d = j + t * n;
+				gr[d * step] = ir[o * step];
+				gi[d * step] = ii[o * step];
+			}
+		struct fftw_plan_s q = *p;
+		q.is = 1; q.idist = n;
+		exec_complex(&q, gr, gi, orr, oi, step);
+		free(g);
+		return;
+	}
 	int nth = p->nthreads;
 #ifdef _OPENMP
 	if (omp_in_parallel()) nth = 1;
@@ -356,6 +408,17 @@ void fftw_execute_split_dft(const fftw_plan p, double *ri, double *ii, double *r
 void fftw_execute_dft_r2c(const fftw_plan p, double *in, fftw_complex *out)
 {
 	const long n = p->n, nc = n / 2 + 1;
+	if (spans_overlap(in, n, p->is, p->idist, 8, out, nc, p->os, p->odist, 16, p->howmany)) {
+		const long tot = n * (long) p->howmany;
+		double *g = (double *) malloc(sizeof(double) * tot);
+		for (long t = 0; t < p->howmany; t++)
+			for (long j = 0; j < n; j++) g[j + t * n] = in[j * p->is + t * p->idist];
+		struct fftw_plan_s q = *p;
+		q.is = 1; q.idist = n;
+		fftw_execute_dft_r2c(&q, g, out);
+		free(g);
+		return;
+	}
 	cpx *bin = (cpx *) malloc(sizeof(cpx) * n * VB);
 	cpx *bout = (cpx *) malloc(sizeof(cpx) * n * VB);
 	double *o = (double *) out;
@@ -382,6 +445,22 @@ void fftw_execute_dft_r2c(const fftw_plan p, double *in, fftw_complex *out)
 void fftw_execute_dft_c2r(const fftw_plan p, fftw_complex *in, double *out)
 {
 	const long n = p->n, nc = n / 2 + 1;
+	if (spans_overlap(in, nc, p->is, p->idist, 16, out, n, p->os, p->odist, 8, p->howmany)) {
+		const long tot = nc * (long) p->howmany;
+		fftw_complex *g = (fftw_complex *) malloc(sizeof(fftw_complex) * tot);
+		const double *x = (const double *) in;
+		for (long t = 0; t < p->howmany; t++)
+			for (long k = 0; k < nc; k++) {
+				long q = k * p->is + t * p->idist;
+				((double *) g)[2 * (k + t * nc)] = x[2 * q];
+				((double *) g)[2 * (k + t * nc) + 1] = x[2 * q + 1];
+			}
+		struct fftw_plan_s q = *p;
+		q.is = 1; q.idist = nc;
+		fftw_execute_dft_c2r(&q, g, out);
+		free(g);
+		return;
+	}
 	cpx *bin = (cpx *) malloc(sizeof(cpx) * n * VB);
 	cpx *bout = (cpx *) malloc(sizeof(cpx) * n * VB);
 	const double *x = (const double *) in;

@@ -1,6 +1,7 @@
 """Pins of the oracle (CPU): the reference library and the NumPy restatement
 against the reference's own known-answer test (examples/test_suite.c:96-152),
 against each other, and against the committed golden fixtures."""
+import ctypes as C
 import json
 import os
 
@@ -158,4 +159,91 @@ def test_round_trip_matches_reference_self_test_bound():
     ref = R.RefSHT(127, 127, 1, R.sht_orthonormal, 192, 384, flags=R.sht_quick_init | R.SHT_THETA_CONTIGUOUS)
     q = rand_spec(127, 127, 1, 1234)
     assert relerr(q, ref.analys(ref.synth(q))) < 1e-13
+    ref.close()
+
+
+def _fftw(L):
+    P, I = C.c_void_p, C.c_int
+    IP = C.POINTER(C.c_int)
+    L.fftw_plan_many_dft_r2c.restype = P
+    L.fftw_plan_many_dft_r2c.argtypes = [I, IP, I, P, IP, I, I, P, IP, I, I, C.c_uint]
+    L.fftw_plan_many_dft_c2r.restype = P
+    L.fftw_plan_many_dft_c2r.argtypes = [I, IP, I, P, IP, I, I, P, IP, I, I, C.c_uint]
+    L.fftw_execute_dft_r2c.argtypes = [P, P, P]
+    L.fftw_execute_dft_c2r.argtypes = [P, P, P]
+    L.fftw_destroy_plan.argtypes = [P]
+    return L
+
+
+@ref_built
+@pytest.mark.parametrize("howmany,nfft", [(33, 48), (9, 16), (127, 384)])
+def test_fftw_shim_in_place_strided_r2c_c2r(howmany, nfft):
+    """The rotation plan of sht_func.c:86-88: an in-place r2c of `howmany`
+    transforms of length nfft, element j of transform t at j*howmany + t
+    (istride = ostride = howmany, idist = odist = 1), executed on another
+    buffer as at sht_func.c:297; and the c2r of the same layout."""
+    L = _fftw(R.lib())
+    n = C.c_int(nfft)
+    nr, nc = C.c_int(nfft + 2), C.c_int(nfft // 2 + 1)
+    buf = np.zeros((nfft + 2) * howmany)
+    p = buf.ctypes.data_as(C.c_void_p)
+    plan = L.fftw_plan_many_dft_r2c(1, C.byref(n), howmany, p, C.byref(nr), howmany, 1, p, C.byref(nc),
+                                    howmany, 1, 64)
+    x = np.random.default_rng(5).standard_normal((nfft, howmany))
+    work = np.zeros((nfft + 2) * howmany)
+    work[:nfft * howmany] = x.ravel()
+    w = work.ctypes.data_as(C.c_void_p)
+    L.fftw_execute_dft_r2c(plan, w, w)
+    got = work.view(np.complex128)[:(nfft // 2 + 1) * howmany].reshape(nfft // 2 + 1, howmany)
+    want = np.fft.rfft(x, axis=0)
+    assert np.abs(got - want).max() / np.abs(want).max() < 1e-14
+    L.fftw_destroy_plan(plan)
+    # c2r of the same layout, in place: back to nfft * x
+    plan = L.fftw_plan_many_dft_c2r(1, C.byref(n), howmany, p, C.byref(nc), howmany, 1, p, C.byref(nr),
+                                    howmany, 1, 64)
+    L.fftw_execute_dft_c2r(plan, w, w)
+    back = work[:nfft * howmany].reshape(nfft, howmany) / nfft
+    assert np.abs(back - x).max() / np.abs(x).max() < 1e-14
+    L.fftw_destroy_plan(plan)
+
+
+def _rmat(axis, ang):
+    c, s = np.cos(ang), np.sin(ang)
+    if axis == "y":
+        return np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]])
+    return np.array([[1, 0, 0], [0, c, -s], [0, s, c]])
+
+
+@ref_built
+@pytest.mark.parametrize("lmax", [20, 48])
+def test_reference_y_and_x_rotations_are_active_rotations(lmax):
+    """SH_Yrotate, SH_Yrotate90 and SH_Xrotate90 (sht_func.c:101-385, the
+    pseudo-spectral path through the in-place r2c above) map the field f to
+    f(R^-1 x), R the rotation about y (or x) by the angle: checked at points
+    with the reference's own SH_to_point."""
+    Lb = R.lib()
+    cfg = Lb.shtns_create.restype
+    P, D = C.c_void_p, C.c_double
+    Lb.SH_Yrotate.argtypes = [cfg, P, D, P]
+    Lb.SH_Yrotate90.argtypes = [cfg, P, P]
+    Lb.SH_Xrotate90.argtypes = [cfg, P, P]
+    Lb.SH_to_point.argtypes = [cfg, P, D, D]
+    Lb.SH_to_point.restype = D
+    ref = R.RefSHT(lmax, lmax, 1, R.sht_orthonormal, 2 * (lmax + 2), 4 * (lmax + 2),
+                   flags=R.sht_quick_init | R.SHT_THETA_CONTIGUOUS, eps=0.0)
+    q = rand_spec(lmax, lmax, 1, 12)
+    ptr = lambda a: a.ctypes.data_as(P)
+    scale = np.abs(q).sum()
+    pts = [v / np.linalg.norm(v) for v in np.random.default_rng(3).standard_normal((6, 3))]
+    for name, axis, ang in (("Yrotate", "y", 0.7), ("Yrotate90", "y", np.pi / 2), ("Xrotate90", "x", np.pi / 2)):
+        out = np.zeros_like(q)
+        if name == "Yrotate":
+            Lb.SH_Yrotate(ref.cfg, ptr(q), ang, ptr(out))
+        else:
+            getattr(Lb, "SH_" + name)(ref.cfg, ptr(q), ptr(out))
+        for v in pts:
+            w = _rmat(axis, -ang) @ v
+            a = Lb.SH_to_point(ref.cfg, ptr(out), v[2], np.arctan2(v[1], v[0]))
+            b = Lb.SH_to_point(ref.cfg, ptr(q), w[2], np.arctan2(w[1], w[0]))
+            assert abs(a - b) < 1e-13 * scale, (name, v)
     ref.close()

@@ -1,10 +1,7 @@
-"""Rotations on the GPU against the reference library's rotation objects and
-SH_Zrotate (sht_func.c:37-53, 1380-2200) on the same inputs and angles, and
-against point values for the rotations about y and x (an active rotation R
-maps the field f to f(R^-1 x)).  The reference's SH_Yrotate / SH_Yrotate90 /
-SH_Xrotate90 go through its pseudo-spectral FFT path, whose outputs in the
-oracle build are not rotations of the field, so those three are checked
-against point values and against the Euler-angle rotation instead.
+"""Rotations on the GPU against the reference library's rotation objects,
+SH_Zrotate, SH_Yrotate, SH_Yrotate90 and SH_Xrotate90 (sht_func.c:37-385,
+1380-2200) on the same inputs and angles, and against point values for the
+rotations about y and x (an active rotation R maps the field f to f(R^-1 x)).
 Bar: 1e-12 relative to the largest coefficient."""
 import ctypes as C
 
@@ -35,6 +32,9 @@ def _ref():
     L.shtns_rotation_wigner_d_matrix.restype = I
     L.shtns_rotation_wigner_d_matrix.argtypes = [P, I, P]
     L.SH_Zrotate.argtypes = [L.shtns_create.restype, P, D, P]
+    L.SH_Yrotate.argtypes = [L.shtns_create.restype, P, D, P]
+    L.SH_Yrotate90.argtypes = [L.shtns_create.restype, P, P]
+    L.SH_Xrotate90.argtypes = [L.shtns_create.restype, P, P]
     return R, L
 
 
@@ -191,3 +191,26 @@ def test_rotation_round_trip_and_norm_at_lmax_1023():
     e0 = np.bincount(li, weights=w * np.abs(q) ** 2)
     e1 = np.bincount(li, weights=w * np.abs(a) ** 2)
     assert np.abs(e1 / e0 - 1).max() < 1e-12
+
+
+@pytest.mark.parametrize("lmax", [20, 48, 127])
+def test_y_and_x_rotations_match_reference(lmax):
+    """SH_Yrotate (several angles), SH_Yrotate90 and SH_Xrotate90 against the
+    reference's own pseudo-spectral implementation (sht_func.c:101-385)."""
+    import shtns_b200
+    R, L = _ref()
+    ref = R.RefSHT(lmax, lmax, 1, R.sht_orthonormal, 2 * (lmax + 2), 4 * (lmax + 2),
+                   flags=R.sht_quick_init | R.SHT_THETA_CONTIGUOUS, eps=0.0)
+    sh = shtns_b200.sht(lmax)
+    q = rand_spec(lmax, lmax, 1, 21)
+    for alpha in (0.7, -1.3, np.pi / 2, 2.9):
+        a = np.zeros_like(q)
+        L.SH_Yrotate(ref.cfg, _p(q), alpha, _p(a))
+        assert relerr(a, sh.Yrotate(q, alpha)) < TOL, alpha
+    a = np.zeros_like(q)
+    L.SH_Yrotate90(ref.cfg, _p(q), _p(a))
+    assert relerr(a, sh.Yrotate90(q)) < TOL
+    a = np.zeros_like(q)
+    L.SH_Xrotate90(ref.cfg, _p(q), _p(a))
+    assert relerr(a, sh.Xrotate90(q)) < TOL
+    ref.close()
