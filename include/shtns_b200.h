@@ -84,8 +84,10 @@ void cu_spat_to_SH_adjoint(shtns_cfg, cplx *Qg, double *Vg, int ltr);
  * bytes, a multiple of 16 up to 4096, that the prefetching FFT kernels wait
  * for beyond what their tensor copies bring; a positive value makes their
  * bounded wait (about one second) give up, so that tests can check the error
- * path (shtns_b200_kernel_errors returns 1, no output is written).  Return 0
- * or -1.
+ * path (shtns_b200_kernel_errors returns 1, no output is written).  Option 9
+ * (test hook, set only, any plan): fills the static scratch array of
+ * cu_SH_to_spat_noalloc on the current device with the byte value 0..255
+ * (0xFF: NaN doubles) and waits for it.  Return 0 or -1.
  * No counterpart in SHTns 3.5.2. */
 int shtns_b200_set_option(shtns_cfg, int option, int value);
 int shtns_b200_get_option(shtns_cfg, int option);
@@ -132,7 +134,9 @@ void shtns_b200_group_analys(shtns_group, double **Vr, cplx **Qlm, const int *nf
  * every GPU loading this library holds until the process exits; plan and
  * batch must need at most that much (coefficient buffer + Fourier buffer,
  * e.g. one field up to lmax=511 on 768x1536), larger requests are rejected
- * with an error (shtns_b200_status() == 1) and nothing is written.  The
+ * with an error (shtns_b200_status() == 1) and nothing is written, as are
+ * plans with split-precision synthesis (option 4) on.  Plan options 1, 3 and
+ * 5 apply as in cu_SH_to_spat.  The
  * first call on a device resolves the array's address (and may load this
  * library's device code): make it before any stream capture.  All calls
  * share the array, so calls that overlap on the GPU race and must be

@@ -30,14 +30,10 @@ bool ensure(void** p, size_t* cap, size_t bytes, const char* what)
 	return true;
 }
 
-struct Job {
-	int ncomp;
-	int type[3];      // 0 scalar, 1 V (theta / spheroidal), 2 W (phi / toroidal)
-	int nf, nfc, ncol, llim, mlim, vec_extra;
-};
+} // namespace
 
-// bufs: 1 = coefficient buffer, 2 = Fourier buffer (both by default)
-bool setup_job(shtns_cfg s, Job& j, int ncomp, const int* types, int ltr, unsigned bufs = 3)
+// bufs: 1 = coefficient buffer, 2 = Fourier buffer (0: shape only, nothing allocated)
+bool setup_job(shtns_cfg s, Job& j, int ncomp, const int* types, int ltr, unsigned bufs)
 {
 	if (!s || !s->grid_set) { shtb_set_error(1, "transform on a plan without grid"); return false; }
 	if (ltr < 0) { shtb_set_error(1, "negative truncation degree"); return false; }
@@ -98,7 +94,7 @@ PrepParams prep_params(shtns_cfg s, const Job& j)
 }
 
 // nrows: grid rows transformed (the plan's nlat, or a block of them)
-FftParams fft_params(shtns_cfg s, const Job& j, int nrows = 0)
+FftParams fft_params(shtns_cfg s, const Job& j, int nrows)
 {
 	if (nrows <= 0) nrows = s->nlat;
 	FftParams p;
@@ -137,6 +133,8 @@ FftParams fft_params(shtns_cfg s, const Job& j, int nrows = 0)
 	p.extra_tx = s->fft_extra_tx;
 	return p;
 }
+
+namespace {
 
 int aligned16(const void* a, const void* b, const void* c, long dist)
 {

@@ -201,6 +201,22 @@ struct FftParams {
 	                                     // 3 prefetched loads with per-thread stores
 };
 
+// ---- one transform call: its shape and the kernels' parameter blocks (sht_api.cu) ----
+struct Job {
+	int ncomp;
+	int type[3];      // 0 scalar, 1 V (theta / spheroidal), 2 W (phi / toroidal)
+	int nf, nfc, ncol, llim, mlim, vec_extra;
+};
+// Fills j for ncomp components of the given types at truncation ltr and grows
+// the plan's work buffers named by bufs (1 coefficient buffer, 2 Fourier
+// buffer; 0 allocates nothing).  false (error recorded) on a bad call.
+bool setup_job(shtns_cfg s, Job& j, int ncomp, const int* types, int ltr, unsigned bufs = 3);
+// Parameter blocks with every plan option applied; work-buffer pointers are
+// the plan's own (d_qq, d_F), which a caller may replace.
+LegParams leg_params(shtns_cfg s, const Job& j);
+PrepParams prep_params(shtns_cfg s, const Job& j);
+FftParams fft_params(shtns_cfg s, const Job& j, int nrows = 0);
+
 // ---- launchers (sht_legendre.cu / sht_fft.cu) ----
 void launch_checkpoints(shtns_cfg s, cudaStream_t st);
 void launch_prep_synth(const PrepParams& p, cudaStream_t st);
@@ -221,6 +237,12 @@ void launch_fft_synth(const FftParams& p, int nfc, cudaStream_t st);
 void launch_fft_analys(const FftParams& p, int nfc, cudaStream_t st);
 int fft_take_wait_error();
 int fft_last_path();
+
+// ---- Gauss-Legendre grid on the current device (sht_gauss.cu) ----
+bool gauss_grid_gpu(int n, std::vector<double>& x, std::vector<double>& st, std::vector<double>& w);
+
+// ---- static scratch of cu_SH_to_spat_noalloc (sht_noalloc.cu) ----
+int shtb_noalloc_fill(int byte);
 
 // ---- error reporting (sht_plan.cu) ----
 void shtb_set_error(int code, const std::string& msg);

@@ -55,20 +55,37 @@ void* scratch_address(int dev)
 
 } // namespace
 
+// Test hook behind shtns_b200_set_option(s, 9, byte): fills the static array
+// of the current device with one byte value (0xFF gives NaN doubles), so that
+// a test can show that no call reads scratch it did not write.  cudaMemset on
+// the array's device address allocates nothing.
+int shtb_noalloc_fill(int byte)
+{
+	int dev = -1;
+	if (!shtb_cuda_ok(cudaGetDevice(&dev), "static scratch fill")) return -1;
+	void* base = scratch_address(dev);
+	if (!base) return -1;
+	if (!shtb_cuda_ok(cudaMemset(base, byte & 0xFF, SHTB_STATIC_SCRATCH_BYTES), "static scratch fill")) return -1;
+	return shtb_cuda_ok(cudaDeviceSynchronize(), "static scratch fill") ? 0 : -1;
+}
+
 extern "C" void cu_SH_to_spat_noalloc(shtns_cfg s, cplx* Qlm, double* Vr, int ltr)
 {
 	if (!s || !s->grid_set) { shtb_set_error(1, "transform on a plan without grid"); return; }
-	if (ltr < 0) { shtb_set_error(1, "negative truncation degree"); return; }
+	if (s->split_ns) {
+		shtb_set_error(1, "cu_SH_to_spat_noalloc: split-precision synthesis (plan option 4) needs tables and "
+		                  "buffers allocated on first use; switch it off (option 4 = 0) for this entry point");
+		return;
+	}
 	int dev = -1;
 	if (!shtb_cuda_ok(cudaGetDevice(&dev), "cu_SH_to_spat_noalloc")) return;
 	if (dev != s->dev) { shtb_set_error(1, "cu_SH_to_spat_noalloc: current device differs from the plan's device"); return; }
-	const int nf = s->batch;
-	const int nfc = nf;
-	const int ncol = 16 * ((nfc + 3) / 4);
-	const int llim = std::min<int>(ltr, s->lmax);
-	const int mlim = std::min<int>(s->mmax, llim / s->mres);
-	const size_t qq_bytes = ((sizeof(double) * (size_t) s->ktot * ncol) + 255) & ~(size_t) 255;
-	const size_t F_bytes = sizeof(double2) * (size_t) nfc * (s->mmax + 1) * s->nlat;
+	// the call's shape with every plan option applied; bufs = 0: no plan buffer is grown
+	static const int scalar_type[1] = {0};
+	Job j;
+	if (!setup_job(s, j, 1, scalar_type, ltr, 0)) return;
+	const size_t qq_bytes = ((sizeof(double) * (size_t) s->ktot * j.ncol) + 255) & ~(size_t) 255;
+	const size_t F_bytes = sizeof(double2) * (size_t) j.nfc * (s->mmax + 1) * s->nlat;
 	if (qq_bytes + F_bytes > SHTB_STATIC_SCRATCH_BYTES) {
 		shtb_set_error(1, "cu_SH_to_spat_noalloc: this plan and batch need " + std::to_string(qq_bytes + F_bytes) +
 		                  " bytes of scratch, more than the static " + std::to_string(SHTB_STATIC_SCRATCH_BYTES) + " bytes");
@@ -79,45 +96,18 @@ extern "C" void cu_SH_to_spat_noalloc(shtns_cfg s, cplx* Qlm, double* Vr, int lt
 	double* qq = static_cast<double*>(base);
 	double2* F = reinterpret_cast<double2*>(static_cast<char*>(base) + qq_bytes);
 
-	PrepParams pp;
-	memset(&pp, 0, sizeof(pp));
-	pp.lmax = s->lmax; pp.llim = llim; pp.mlim = mlim; pp.mres = s->mres;
-	pp.nf = nf; pp.ncomp = 1; pp.ncol = ncol;
-	pp.spec_dist = s->spec_dist;
-	pp.xs = s->d_xs; pp.xa = s->d_xa;
-	pp.stdt_lo = s->d_stdt_lo; pp.stdt_hi = s->d_stdt_hi; pp.van_lo = s->d_van_lo; pp.van_hi = s->d_van_hi;
-	pp.l2 = s->d_l2; pp.mt = s->mt; pp.qq = qq;
+	PrepParams pp = prep_params(s, j);
 	pp.Q = reinterpret_cast<const double2*>(Qlm);
-
-	LegParams lp;
-	memset(&lp, 0, sizeof(lp));
-	lp.nlat = s->nlat; lp.nlat_2 = s->nlat_2; lp.llim = llim; lp.mlim = mlim; lp.mres = s->mres;
-	lp.vec_extra = 0; lp.ncol = ncol; lp.nfc = nfc; lp.ckseg = s->ckseg;
-	lp.south_first = s->south_first; lp.robert = s->robert;
-	lp.mpos_inv = 1.0 / s->mpos_renorm;
-	lp.x = s->d_x; lp.x2 = s->d_x2; lp.sinv = s->d_sinv; lp.w = s->d_w; lp.c = s->d_c;
-	lp.ck = s->d_ck; lp.mt = s->mt; lp.nf = nf;
+	pp.qq = qq;
+	LegParams lp = leg_params(s, j);
 	lp.qq = qq; lp.F = F;
-	lp.fstride = (long)(s->mmax + 1) * s->nlat;
-
-	FftParams fp;
-	memset(&fp, 0, sizeof(fp));
-	fp.N = s->nphi; fp.nlat = s->nlat; fp.mlim = mlim;
-	fp.nradix = (int) s->fft_radix.size();
-	for (int i = 0; i < fp.nradix; i++) fp.rcode |= (unsigned long long) s->fft_radix[i] << (4 * i);
-	int S = 4;
-	while (S > 1 && fft_smem_bytes(s->nphi, S) > 112 * 1024) S /= 2;
-	while (S > 1 && 2 * S > (int) s->nlat) S /= 2;
-	fp.S = S;
-	fp.tw = s->d_tw; fp.F = F;
-	fp.fstride = lp.fstride;
-	fp.nf = nf; fp.spat_dist = s->spat_dist;
-	fp.phi_contiguous = s->phi_contiguous;
+	FftParams fp = fft_params(s, j);
+	fp.F = F;
 	fp.spat[0] = Vr;
 	fp.vec2 = (((uintptr_t) Vr & 15) == 0) && (s->spat_dist % 2 == 0);
 
 	launch_prep_synth(pp, s->comp_stream);
 	launch_leg_synth(lp, s->comp_stream);
-	launch_fft_synth(fp, nfc, s->comp_stream);
+	launch_fft_synth(fp, j.nfc, s->comp_stream);
 	shtb_cuda_ok(cudaGetLastError(), "cu_SH_to_spat_noalloc launch");
 }

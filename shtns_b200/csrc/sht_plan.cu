@@ -275,39 +275,6 @@ static void vector_tables(shtns_cfg s)
 	for (int l = 1; l <= lmax + 1; l++) s->l_2[l] = 1.0 / ((double) l * (l + 1));
 }
 
-// Gauss-Legendre nodes and weights (north half), Newton iteration on P_n
-// from the asymptotic guess, in long double.
-static void gauss_grid(int n, std::vector<long double>& x, std::vector<long double>& w)
-{
-	const int m = n / 2;
-	x.resize(m); w.resize(m);
-	for (int i = 0; i < m; i++) {
-		long double z = (1.0L - (n - 1.0L) / (8.0L * n * n * n)) * std::cos((3.14159265358979323846264338327950288L * (4 * i + 3)) / (4 * n + 2));
-		long double pp = 1, p1 = 0, p2 = 0;
-		for (int it = 0; it < 100; it++) {
-			p1 = z; p2 = 1.0L;
-			for (long l = 2; l <= n; l++) {
-				long double p3 = p2;
-				p2 = p1;
-				p1 = ((2 * l - 1) * z * p2 - (l - 1) * p3) / l;
-			}
-			pp = n * (p2 - z * p1);
-			long double z1 = z;
-			z -= p1 * (1.0L - z * z) / pp;
-			if (std::fabs((double)(z - z1)) <= (double)(z1 + z) * 0.5 * 1e-19) break;
-		}
-		p1 = z; p2 = 1.0L;
-		for (long l = 2; l <= n; l++) {
-			long double p3 = p2;
-			p2 = p1;
-			p1 = ((2 * l - 1) * z * p2 - (l - 1) * p3) / l;
-		}
-		pp = n * (p2 - z * p1);
-		x[i] = z;
-		w[i] = 2.0L * (1.0L - z * z) / (pp * pp);
-	}
-}
-
 // max over l of |P_l^m(x)| (classic recurrence in long double: its exponent
 // range covers every seed below degree 16384)
 static double max_plm(shtns_cfg s, int im, long double x, long double sint)
@@ -540,23 +507,22 @@ extern "C" int shtns_set_grid_auto(shtns_cfg s, enum shtns_type flags, double ep
 	s->phi_contiguous = (layout & SHT_PHI_CONTIGUOUS) ? 1 : 0;
 	s->south_first = (layout & SHT_SOUTH_POLE_FIRST) ? 1 : 0;
 	s->eps = eps;
-	// Gauss grid
-	std::vector<long double> xg, wg;
-	gauss_grid(nl, xg, wg);
+	// Gauss grid, generated on the GPU (sht_gauss.cu): nodes and weights
+	// refined in double-double and rounded to FP64; sin(theta) is that of the
+	// node as rounded to FP64, not of the extended-precision node, so every
+	// table describes the same point.  Near the poles an inconsistent pair is
+	// amplified (|d sin / sin| = x |dx| / sin^2: 4e-10 at the first row of a
+	// 6144-point grid), which would scale the m >= 1 terms.
+	std::vector<double> xg, sg, wg;
+	if (!gauss_grid_gpu(nl, xg, sg, wg)) { plan_error("Gauss grid generation failed: " + g_last_error); return -1; }
 	s->ct_v.assign(nl, 0.0); s->st_v.assign(nl, 0.0);
 	s->wq.assign(s->nlat_2, 0.0);
 	const double latdir = s->south_first ? -1.0 : 1.0;
-	// sin(theta) of the node as rounded to double, not of the extended-precision
-	// node: every table then describes the same point.  Near the poles an
-	// inconsistent pair is amplified (|d sin / sin| = x |dx| / sin^2: 4e-10 at
-	// the first row of a 6144-point grid), which would scale the m >= 1 terms.
 	for (int t = 0; t < s->nlat_2; t++) {
-		const long double xr = (long double)(double) xg[t];
-		const double st = (double) std::sqrt((1.0L - xr) * (1.0L + xr));
-		s->ct_v[t] = latdir * (double) xg[t];
-		s->ct_v[nl - 1 - t] = -latdir * (double) xg[t];
-		s->st_v[t] = st; s->st_v[nl - 1 - t] = st;
-		s->wq[t] = (double) wg[t];
+		s->ct_v[t] = latdir * xg[t];
+		s->ct_v[nl - 1 - t] = -latdir * xg[t];
+		s->st_v[t] = sg[t]; s->st_v[nl - 1 - t] = sg[t];
+		s->wq[t] = wg[t];
 	}
 	s->ct = s->ct_v.data(); s->st = s->st_v.data();
 	// polar threshold (sht_init.c:522-557): tm[im] = first north row with max_l |P_lm| >= eps
@@ -568,8 +534,7 @@ extern "C" int shtns_set_grid_auto(shtns_cfg s, enum shtns_type flags, double ep
 			do {
 				it++;
 				if (it >= s->nlat_2) break;
-				const long double xr = (long double)(double) xg[it];
-				v = max_plm(s, im, xr, std::sqrt((1.0L - xr) * (1.0L + xr)));
+				v = max_plm(s, im, (long double) xg[it], (long double) sg[it]);
 			} while (v < eps);
 			s->tm_h[im] = it < s->nlat_2 ? it : s->nlat_2;
 		}
@@ -857,6 +822,9 @@ extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
 			if (value < 0 || value > 4096 || (value & 15)) return -1;
 			s->fft_extra_tx = value;
 			return 0;
+		case 9:   // test hook: fill the no-allocation entry point's static scratch with this byte
+			if (value < 0 || value > 255) return -1;
+			return shtb_noalloc_fill(value);
 		default:
 			return -1;
 	}

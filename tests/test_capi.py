@@ -144,3 +144,32 @@ def test_plan_options_validate_and_read_back():
     assert lib.shtns_b200_set_option(cfg, 99, 0) == -1
     assert lib.shtns_b200_get_option(cfg, 99) == -1
     lib.shtns_destroy(cfg)
+
+
+def test_public_headers_compile_as_c99_and_cxx():
+    """include/shtns.h, shtns_cuda.h and shtns_b200.h compile in a C99 unit
+    (complex.h cplx, enums, extern "C" guards) and in a C++ unit, and the C
+    caller of the device API (tests/c/cu_roundtrip.c) compiles and links
+    against libshtns_b200.so with -Wall -Wextra -Werror.  Nothing is run."""
+    import subprocess
+    import tempfile
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    inc = os.path.join(root, "include")
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    cuda_lib = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "lib64")
+    src = ('#include "shtns.h"\n#include "shtns_cuda.h"\n#include "shtns_b200.h"\n'
+           'int f(shtns_cfg s) { return (int) s->nlm + (int) sizeof(cplx) + sht_quick_init + SHT_ALLOW_GPU; }\n')
+    with tempfile.TemporaryDirectory() as d:
+        for lang, std in (("c", "-std=c99"), ("c++", "-std=c++17")):
+            p = os.path.join(d, "h." + ("c" if lang == "c" else "cpp"))
+            with open(p, "w") as f:
+                f.write(src)
+            r = subprocess.run(["gcc" if lang == "c" else "g++", std, "-Wall", "-Wextra", "-Werror", "-fsyntax-only",
+                                "-I", inc, "-I", cuda_inc, p], capture_output=True, text=True)
+            assert r.returncode == 0, r.stderr
+        exe = os.path.join(d, "cu_roundtrip")
+        r = subprocess.run(["gcc", "-std=c99", "-D_DEFAULT_SOURCE", "-Wall", "-Wextra", "-Werror", "-I", inc,
+                            "-I", cuda_inc, os.path.join(root, "tests", "c", "cu_roundtrip.c"),
+                            "-L", os.path.join(root, "shtns_b200"), "-lshtns_b200", "-L", cuda_lib, "-lcudart",
+                            "-lm", "-o", exe], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
