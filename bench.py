@@ -232,6 +232,44 @@ def fp64_gemm_peak(torch, dev):
     return best
 
 
+def cufft_reference_times(torch, dev, spat, nf, reps=5):
+    """cuFFT with the reference's theta-contiguous plan (sht_gpu.cu:186-190:
+    Z2Z of length nphi over the nlat/2 latitude pairs of one field, one
+    execution per field-component, as the reference's cu_* transforms call
+    it) over the step's 3 x nf grids, out of place into a buffer of the same
+    size.  Milliseconds per direction (all field-components), best of reps.
+    cuFFT writes the whole pair spectrum; the library's FFT stages also
+    separate the two real spectra of each pair and keep only m <= mmax."""
+    from tests import cufft
+    st = torch.cuda.current_stream()
+    plan = cufft.PairPlan(NPHI, NLAT, st.cuda_stream)
+    out = [torch.empty_like(x) for x in spat]
+    res = {}
+    for name, direction in (("z2z_forward_ms", cufft.CUFFT_FORWARD), ("z2z_inverse_ms", cufft.CUFFT_INVERSE)):
+        def run():
+            for x, y in zip(spat, out):
+                for f in range(nf):
+                    plan.exec(x[f].data_ptr(), y[f].data_ptr(), direction)
+        run()
+        torch.cuda.synchronize()
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            run()
+            e1.record()
+            e1.synchronize()
+            t = e0.elapsed_time(e1)
+            best = t if best is None else min(best, t)
+        res[name] = best
+    plan.destroy()
+    del out
+    torch.cuda.empty_cache()
+    res["plan"] = (f"cufftPlanMany Z2Z n={NPHI}, istride=ostride={NLAT // 2}, idist=odist=1, batch={NLAT // 2}; "
+                   f"{3 * nf} executions per direction, out of place")
+    return res
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -380,6 +418,8 @@ def run_gpu(args):
         ms_e2e = float(t.item())
     bytes_io = 3 * nf * sh.nlm * 16
 
+    cufft_times = cufft_reference_times(torch, dev, spat, nf) if rank == 0 else None
+
     if rank == 0:
         ms_step = ms_total / args.steps
         value = world * nf / (ms_step * 1e-3)
@@ -438,6 +478,10 @@ def run_gpu(args):
                              ((3 * nf * sh.nlm * 16 * 2 + 3 * nf * NLAT * NPHI * 8) / 1e9)},
             "roofline": roof,
             "stages": stages,
+            "cufft_reference": dict(cufft_times, **{
+                "ours_fft_synthesis_ms": float(per_launch[2]), "ours_fft_analysis_ms": float(per_launch[3]),
+                "speedup_synthesis": cufft_times["z2z_inverse_ms"] / float(per_launch[2]),
+                "speedup_analysis": cufft_times["z2z_forward_ms"] / float(per_launch[3])}) if cufft_times else None,
             "roundtrip_relerr": rt_err,
             "gpu_launches": int(launches),
             "e2e": {"value": world * nf / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
