@@ -615,10 +615,12 @@ HD_UNIT = "field-pairs/s (SH_to_spat+spat_to_SH, lmax=4095, 6144x12288)"
 
 def run_highdeg(args):
     """lmax=4095 on the 6144 x 12288 Gauss grid, 8 scalar fields: the FP64
-    transform pair against split-precision synthesis (FP16 tensor cores, 5, 6
-    and 7 slices per operand; analysis stays FP64).  value = FP64 pairs/s;
-    each split form reports its synthesis and pair rates and its max / RMS
-    error against the FP64 synthesis of the same coefficients."""
+    transform pair against the split-precision pair from the precomputed
+    INT8 digit table (synthesis and analysis on the INT8 tensor cores, 5, 6
+    and 7 digits; 7 is the form within 1e-11), and the on-the-fly FP16
+    split synthesis for comparison.  value = pairs/s of the 7-digit table
+    form; every form reports its pair, synthesis and Legendre stage times and
+    its max / RMS error against the FP64 stages on the same inputs."""
     import torch
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
@@ -632,6 +634,7 @@ def run_highdeg(args):
     q = torch.from_numpy(rand_spec(HD_L, HD_L, 1, 400, power=1.0, nfields=nf)).to(dev)
     v = torch.empty((nf,) + sh.spat_shape, dtype=torch.float64, device=dev)
     r = torch.empty_like(q)
+    ref = {}
 
     def timed(fn, steps):
         for _ in range(args.warmup):
@@ -648,9 +651,26 @@ def run_highdeg(args):
     def synth():
         sh.synth_into([q], [v])
 
+    def analys():
+        sh.analys_into([ref["v64"]], [r])
+
     def pair():
         sh.synth_into([q], [v])
         sh.analys_into([v], [r])
+
+    def stages(fn):
+        lib.shtns_b200_set_timing(sh._cfg, 1)
+        fn()
+        torch.cuda.synchronize()
+        st = np.zeros(6)
+        ca = np.zeros(6, dtype=np.int64)
+        lib.shtns_b200_stage_times(sh._cfg, st.ctypes.data_as(C.c_void_p), ca.ctypes.data_as(C.c_void_p))
+        lib.shtns_b200_set_timing(sh._cfg, 0)
+        return st / np.maximum(ca, 1)
+
+    def rel(a, b):
+        d = a - b
+        return float(d.abs().max() / b.abs().max()), float((d * d).mean().sqrt() / (b * b).mean().sqrt())
 
     steps = max(3, min(args.steps, 10))
     clocks = ClockSampler(0)
@@ -659,34 +679,42 @@ def run_highdeg(args):
     sh.set_split(0)
     ms_pair = timed(pair, steps)
     ms_syn = timed(synth, steps)
-    v64 = v.clone()
-    rt = float((r - q).abs().max() / q.abs().max())
-    lib.shtns_b200_set_timing(sh._cfg, 1)
-    synth()
-    torch.cuda.synchronize()
-    st = np.zeros(6)
-    ca = np.zeros(6, dtype=np.int64)
-    lib.shtns_b200_stage_times(sh._cfg, st.ctypes.data_as(C.c_void_p), ca.ctypes.data_as(C.c_void_p))
-    lib.shtns_b200_set_timing(sh._cfg, 0)
-    forms = {"fp64": {"synth_ms": ms_syn, "pair_ms": ms_pair, "legendre_synth_ms": st[1] / max(ca[1], 1),
+    ref["v64"] = v.clone()
+    v64 = ref["v64"]
+    ms_ana = timed(analys, steps)
+    q64 = r.clone()
+    rt = float((q64 - q).abs().max() / q.abs().max())
+    st = stages(pair)
+    forms = {"fp64": {"pair_ms": ms_pair, "synth_ms": ms_syn, "analys_ms": ms_ana,
+                      "legendre_synth_ms": st[1], "legendre_analys_ms": st[4],
                       "pairs_per_s": nf / (ms_pair * 1e-3)}}
     for ns in (5, 6, 7):
-        sh.set_split(ns)
-        ms_s = timed(synth, steps)
-        d = v - v64
-        err_max = float(d.abs().max() / v64.abs().max())
-        err_rms = float((d * d).mean().sqrt() / (v64 * v64).mean().sqrt())
-        ms_p = timed(pair, steps)
-        lib.shtns_b200_set_timing(sh._cfg, 1)
-        synth()
+        sh.set_split(ns, form=0)
         torch.cuda.synchronize()
-        st[:] = 0
-        ca[:] = 0
-        lib.shtns_b200_stage_times(sh._cfg, st.ctypes.data_as(C.c_void_p), ca.ctypes.data_as(C.c_void_p))
-        lib.shtns_b200_set_timing(sh._cfg, 0)
-        forms["split%d" % ns] = {"synth_ms": ms_s, "pair_ms": ms_p, "legendre_synth_ms": st[1] / max(ca[1], 1),
-                                 "pairs_per_s": nf / (ms_p * 1e-3), "max_rel_err": err_max, "rms_rel_err": err_rms,
+        t0 = time.perf_counter()
+        synth()                       # first use builds the digit table
+        torch.cuda.synchronize()
+        build_s = time.perf_counter() - t0
+        ms_s = timed(synth, steps)
+        es = rel(v, v64)
+        ms_a = timed(analys, steps)
+        ea = rel(r, q64)
+        ms_p = timed(pair, steps)
+        st = stages(pair)
+        tab = int(lib.shtns_b200_split_table_bytes(sh._cfg))
+        forms["table%d" % ns] = {"pair_ms": ms_p, "synth_ms": ms_s, "analys_ms": ms_a,
+                                 "legendre_synth_ms": st[1], "legendre_analys_ms": st[4],
+                                 "pairs_per_s": nf / (ms_p * 1e-3), "speedup_vs_fp64": ms_pair / ms_p,
+                                 "synth_max_rel_err": es[0], "synth_rms_rel_err": es[1],
+                                 "analys_max_rel_err": ea[0], "analys_rms_rel_err": ea[1],
+                                 "table_bytes": tab, "table_build_s": build_s,
                                  "kernel_errors": int(sh.kernel_errors())}
+    sh.set_split(7, form=1)
+    ms_s = timed(synth, steps)
+    es = rel(v, v64)
+    st = stages(synth)
+    forms["fp16_onthefly7"] = {"synth_ms": ms_s, "legendre_synth_ms": st[1], "synth_max_rel_err": es[0],
+                               "synth_rms_rel_err": es[1], "kernel_errors": int(sh.kernel_errors())}
     sh.set_split(0)
     clk = clocks.stop()
     tm = np.zeros(HD_L + 1, dtype=np.int32)
@@ -695,17 +723,32 @@ def run_highdeg(args):
     ks = (HD_L - np.arange(HD_L + 1)) // 2 + 1
     flops = 8.0 * float((rows * ks).sum()) * nf
     peak = fp64_gemm_peak(torch, dev)
-    ach = flops / (forms["fp64"]["legendre_synth_ms"] * 1e-3) / 1e12
+    hbm = measured_peaks().get("hbm_gbs", 6650.0)
+    t7 = forms["table7"]
+    # the table kernels stream the digit table once per launch (plus the
+    # digit stacks of the other operand, mostly from L2, and the outputs)
+    ach_s = t7["table_bytes"] / (t7["legendre_synth_ms"] * 1e-3) / 1e9
+    ach_a = t7["table_bytes"] / (t7["legendre_analys_ms"] * 1e-3) / 1e9
     line = {
-        "metric": METRIC, "value": nf / (ms_pair * 1e-3), "unit": HD_UNIT, "n_gpus": 1, "steps": steps,
-        "warmup": args.warmup, "ms_per_step": ms_pair, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1)/(l+1))",
+        "metric": METRIC, "value": nf / (t7["pair_ms"] * 1e-3), "unit": HD_UNIT, "n_gpus": 1, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": t7["pair_ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int8 digits x7, exact int32 sums, f64 combine",
+        "data": "synthetic (seeded N(0,1)/(l+1))",
         "config": {"workload": "lmax4095_8fields", "lmax": HD_L, "nlat": HD_NLAT, "nphi": HD_NPHI, "fields": nf,
-                   "polar_eps": EPS, "layout": "theta-contiguous", "form": "FP64 synthesis + analysis"},
+                   "polar_eps": EPS, "layout": "theta-contiguous",
+                   "form": "split precision: 7-digit INT8 table, synthesis + analysis"},
+        "split_speedup_vs_fp64": t7["speedup_vs_fp64"],
         "forms": forms,
-        "roofline": {"kernel": "leg_synth_kernel (FP64)", "bound": "tensor", "achieved": ach, "peak": peak,
-                     "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
-                     "peak_source": "measured in this run: cuBLAS DGEMM 8192^3"},
+        "roofline": {"kernel": "ptab_synth_kernel / ptab_analys_kernel (7 digits)", "bound": "hbm",
+                     "achieved": ach_s, "achieved_analysis": ach_a, "peak": hbm, "unit": "GB/s",
+                     "frac": ach_s / hbm, "frac_analysis": ach_a / hbm, "traffic": None,
+                     "work_per_launch": f"{t7['table_bytes']:.4e} bytes of digit table",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "fp64_roofline": {"kernel": "leg_synth_kernel (FP64)", "bound": "tensor",
+                          "achieved": flops / (forms["fp64"]["legendre_synth_ms"] * 1e-3) / 1e12, "peak": peak,
+                          "unit": "TFLOP/s",
+                          "frac": flops / (forms["fp64"]["legendre_synth_ms"] * 1e-3) / 1e12 / peak,
+                          "peak_source": "measured in this run: cuBLAS DGEMM 8192^3"},
         "roundtrip_relerr": rt,
         "clocks": clk,
     }

@@ -99,15 +99,27 @@ int shtns_b200_get_option(shtns_cfg, int option);
  * picks the SIMT kernels for at most 4 field-components in the synthesis and
  * 3 in the analysis, 128 x 32 for calls with at most 32 GEMM columns (8
  * field-components) and 64 x 64 otherwise.  Plan groups always use 64 x 64.
- * Option 4 of shtns_b200_set_option: split-precision Legendre synthesis on
- * the FP16 tensor cores with 3, 4 or 5 balanced 8-bit slices per operand
- * (about 24, 32, 40 bits; products summed exactly in FP32 over windows of 256
- * steps and in FP64 across them); 0 (default) keeps the FP64 contraction.
- * Waits for the device; returns 1 (and clears it) if a bounded wait of the
- * split-precision kernel or of the prefetching FFT kernels gave up since the
- * last call, else 0.
+ * Option 4 of shtns_b200_set_option: split-precision Legendre stages with 3
+ * to 7 balanced 8-bit digits per operand (products summed exactly; the
+ * result carries about 8 x digits - 2 bits relative to the row and column
+ * maxima; 7 digits stay within 1e-11 of FP64 at lmax 4095); 0 (default)
+ * keeps the FP64 contraction.  Option 8 picks the form: 0 (default) a table
+ * of the Legendre values as INT8 digits, built on the device on first use
+ * (digits x 128-row x 128-step blocks over the orders, latitude tiles at or
+ * beyond the polar threshold: about 69 GB for 7 digits at lmax 4095 on
+ * 6144 latitudes) and contracted on the INT8 tensor cores with INT32
+ * accumulation, synthesis and analysis, whole transforms with mres = 1;
+ * 1: synthesis only, slices regenerated on the fly and contracted on the
+ * FP16 tensor cores (analysis in FP64).  Clones use the table of their
+ * base plan.
+ * shtns_b200_kernel_errors waits for the device; returns 1 (and clears it)
+ * if a bounded wait of a split-precision kernel or of the prefetching FFT
+ * kernels gave up since the last call, else 0.
+ * shtns_b200_split_table_bytes: bytes of the plan's digit table (0 when
+ * none has been built).
  * No counterpart in SHTns 3.5.2. */
 int shtns_b200_kernel_errors(shtns_cfg);
+size_t shtns_b200_split_table_bytes(shtns_cfg);
 
 /* Plan groups: scalar transforms of fields of different lmax, each on the grid
  * of its own plan, with the Legendre stage of all plans in one persistent

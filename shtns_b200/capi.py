@@ -132,6 +132,7 @@ PROTOTYPES = {
     "SHqst_to_spat_ml": (None, [CFG, I, P, P, P, P, P, P, I]),
     "spat_to_SHqst_ml": (None, [CFG, I, P, P, P, P, P, P, I]),
     "shtns_b200_kernel_errors": (I, [CFG]),
+    "shtns_b200_split_table_bytes": (C.c_size_t, [CFG]),
     "shtns_b200_get_option": (I, [CFG, I]),
     "shtns_b200_group_create": (P, [I, P]),
     "shtns_b200_group_destroy": (None, [P]),

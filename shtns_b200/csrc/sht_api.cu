@@ -198,7 +198,8 @@ void run_analys(shtns_cfg s, int ncomp, const int* types, const double* i0, cons
 	int kmax_all = 0;
 	for (int im = 0; im <= j.mlim; im++) kmax_all = std::max(kmax_all, (j.llim + j.vec_extra - im * s->mres) / 2 + 1);
 	shtb_stage_begin(s, 4);
-	launch_leg_analys(lp, kmax_all, s->comp_stream);
+	if (s->split_ns && s->split_form == 0) launch_ptab_analys(s, lp, s->comp_stream);
+	else launch_leg_analys(lp, kmax_all, s->comp_stream);
 	shtb_stage_end(s);
 	PrepParams pp = prep_params(s, j);
 	if (adjoint) pp.xa = s->d_xs;

@@ -107,6 +107,19 @@ struct shtns_info {
 	void *d_bsl; size_t bsl_cap;         // coefficient slices
 	int *d_bexp; size_t bexp_cap;        // column exponents [im][column]
 	int *d_split_err;                    // set by the kernel when a wait gives up
+	// split precision from a precomputed digit table (option 4 with option 8 = 0):
+	// Y_k(theta) of every order as int8 digits, built on first use and owned by
+	// the original plan (clones use their base plan's table)
+	int split_form;                      // 0 digit table (synthesis and analysis), 1 on-the-fly FP16 (synthesis only)
+	void *d_ptab; size_t ptab_bytes;     // digit table
+	int ptab_ns;                         // digits per value of the table
+	long *d_ptoff;                       // per order: first 16 KB digit-block of the order
+	long *d_pkoff;                       // per order: first 128-step block (coefficient digit stacks)
+	long *d_pvoff;                       // per order: first kept theta tile (weighted Fourier digit stacks)
+	int *d_pt0;                          // per order: first theta tile kept by the polar threshold
+	long ptab_kblocks, ptab_ttiles;      // sums over the orders of the above counts
+	void *d_pbs; size_t pbs_cap;         // per call: B-operand digit stacks
+	int *d_pexp; size_t pexp_cap;        // per call: column exponents [im][column]
 	// local evaluation (points, latitudes, operators): classic-recurrence
 	// tables on the device, allocated on first use (no grid needed), and staging
 	double *d_alm; long *d_almoff;
@@ -224,6 +237,10 @@ void launch_post_analys_m(const PrepParams& p, int mmax, cudaStream_t st);
 void launch_leg_synth(const LegParams& p, cudaStream_t st);
 void launch_leg_analys(const LegParams& p, int kmax_all, cudaStream_t st);
 void launch_leg_synth_split(shtns_cfg s, const LegParams& p, cudaStream_t st);
+bool split_row_exponents(shtns_cfg s, cudaStream_t st);
+void launch_ptab_synth(shtns_cfg s, const LegParams& p, cudaStream_t st);
+void launch_ptab_analys(shtns_cfg s, const LegParams& p, cudaStream_t st);
+void free_ptab(shtns_cfg s);
 bool leg_simt_selected(const LegParams& p, bool synth);
 void launch_leg_synth_simt(const LegParams& p, cudaStream_t st);
 void launch_leg_analys_simt(const LegParams& p, int kmax_all, cudaStream_t st);

@@ -669,6 +669,9 @@ extern "C" shtns_cfg cushtns_clone(shtns_cfg b, cudaStream_t compute_stream, cud
 	s->d_alm = nullptr; s->d_almoff = nullptr; s->d_loc = nullptr; s->loc_cap = 0;
 	s->d_yexp = nullptr; s->d_boff = nullptr; s->split_chunks = 0; s->split_kc = 0;
 	s->d_bsl = nullptr; s->bsl_cap = 0; s->d_bexp = nullptr; s->bexp_cap = 0; s->d_split_err = nullptr;
+	s->d_ptab = nullptr; s->ptab_bytes = 0; s->ptab_ns = 0; s->d_ptoff = nullptr; s->d_pkoff = nullptr;
+	s->d_pvoff = nullptr; s->d_pt0 = nullptr; s->ptab_kblocks = 0; s->ptab_ttiles = 0;
+	s->d_pbs = nullptr; s->pbs_cap = 0; s->d_pexp = nullptr; s->pexp_cap = 0;
 	s->xfer_stream = nullptr; s->own_xfer = 0;
 	s->ev.clear(); s->ev_stage.clear(); s->ev_used = 0; s->timing = 0;
 	cushtns_set_streams(s, compute_stream, transfer_stream);
@@ -807,6 +810,7 @@ extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
 			}
 			cudaFree(old);
 			s->d_ck = nck;
+			free_split(s);          // split-precision tables derive from the checkpoints
 			const int nm = s->mmax + 1;
 			cudaMemcpy(s->d_mint + 4 * nm, s->ckoff_h.data(), sizeof(int) * nm, cudaMemcpyHostToDevice);
 			launch_checkpoints(s, 0);
@@ -821,6 +825,10 @@ extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
 		          // (a positive value makes their bounded wait give up: error-path tests)
 			if (value < 0 || value > 4096 || (value & 15)) return -1;
 			s->fft_extra_tx = value;
+			return 0;
+		case 8:   // split-precision form: 0 precomputed int8 digit table (synthesis and analysis), 1 on-the-fly FP16 (synthesis)
+			if (value != 0 && value != 1) return -1;
+			s->split_form = value;
 			return 0;
 		case 9:   // test hook: fill the no-allocation entry point's static scratch with this byte
 			if (value < 0 || value > 255) return -1;
@@ -841,6 +849,7 @@ extern "C" int shtns_b200_get_option(shtns_cfg s, int option)
 		case 5: return s->tile_wm;
 		case 6: return fft_last_path();   // FFT kernels of the last launch in this process
 		case 7: return s->fft_extra_tx;
+		case 8: return s->split_form;
 		default: return -1;
 	}
 }

@@ -1,0 +1,882 @@
+// Split-precision Legendre stages from a precomputed table of Legendre
+// values, on the INT8 tensor cores (tcgen05.mma kind::i8).
+//
+// The per-order contractions of the FP64 transform,
+//   synthesis  out[t, c] = sum_k Y_k(t) q[k, c]      (t: north latitude)
+//   analysis   q[k, c]   = sum_t Y_k(t) G[t, c]      (G: weighted N/S fold of F)
+// are evaluated as exact integer sums of products of 8-bit digits
+// (Ozaki-style splitting, with integer instead of floating-point slices):
+//   Y_k(t)  = 2^(e_t + 2) sum_i a_i[t,k] 2^(-8(i+1))      e_t: exponent of max_k |Y_k(t)|
+//   q[k, c] = 2^(f_c + 2) sum_j b_j[k,c] 2^(-8(j+1))      f_c: exponent of max_k |q[k, c]|
+// a_i, b_j in [-128, 127] (the leading digit in [-65, 65]: values are scaled
+// below 1/4).  Products with i + j < NS are kept; D_s = sum_{i+j=s} sum_k
+// a_i b_j accumulates exactly in INT32 tensor memory (|a_i b_j| <= 2^14, at
+// most NS * 3072 terms per accumulator below 2^31), and
+//   out = 2^(e_t + f_c + 4) sum_s 2^(-8(s+2)) D_s
+// is formed in FP64 once per tile.  NS = 7 keeps 54 bits.  For the analysis
+// the row scale moves to the other operand: G'[t, c] = 2^(e_t + 2) G[t, c] is
+// split with its own column exponent, so the same integer digits of Y serve
+// both directions.
+//
+// The digits of Y (the table, built once per plan on first use from the
+// recurrence checkpoints with the FP64 kernels' own arithmetic) are stored in
+// 16 KB digit-blocks of 128 latitudes x 128 Ishioka steps, as 8 x 16-byte core
+// matrices: core matrix (a, b) = latitudes 8a..8a+7, steps 16b..16b+15 at byte
+// (16 b + a) 128, step fastest.  The synthesis reads a block as the K-major A
+// operand (M = latitudes, K = steps), the analysis reads the same bytes as
+// the MN-major A operand (M = steps, K = latitudes).  Per order the table
+// keeps the latitude tiles at or beyond the polar threshold and the step
+// blocks up to the plan's last step (degree lmax + 1).
+//
+// Kernel shape (both directions, one CTA per 128-row tile of one order and 32
+// GEMM columns = 8 field-components; 192 threads, two CTAs per SM):
+//   warp 0, one thread: bulk copies (cp.async.bulk, no multicast) of the
+//     coefficient (or weighted Fourier) digit stack of the next 128-step (or
+//     128-latitude) block and of its NS digit-blocks of Y into a ring of
+//     shared-memory slots, completion on mbarriers;
+//   warp 1, one thread: per digit-block i, tcgen05.mma (M = 128, N = 32 (NS -
+//     i), K = 32) into accumulator columns 32 i .. 32 NS - 1 against the stacked
+//     digits j < NS - i; tcgen05.commit frees the slot;
+//   warps 2-5: read the NS INT32 accumulators (tcgen05.ld), combine them in
+//     FP64 and store F (synthesis: folded hemispheres, as leg_synth_tile) or
+//     the Ishioka-basis coefficients (analysis).
+// Every mbarrier wait is bounded (about one second by %globaltimer); a wait
+// that gives up records an error flag (shtns_b200_kernel_errors), the CTA
+// waits (bounded) for the copies and products it issued, frees its tensor
+// memory and returns.
+//
+// The reference computes these sums in FP64 on the CPU
+// (SHT/kernel_SH_to_spat.gen.c:388-409, kernel_spat_to_SH.gen.c:502-598);
+// this path is a project extension.
+#include "sht_internal.h"
+
+#include <algorithm>
+#include <cstdint>
+
+namespace {
+
+constexpr int PB_T = 128;                  // latitudes per digit-block and per synthesis CTA
+constexpr int PB_K = 128;                  // Ishioka steps per digit-block and per analysis CTA
+constexpr int PB_BYTES = PB_T * PB_K;      // one digit-block: 16 KB
+constexpr int PT_NC = 32;                  // GEMM columns per CTA
+constexpr int PT_THREADS = 192;
+constexpr int PT_RA = 3;                   // digit-block slots
+constexpr uint64_t PT_WAIT_NS = 1000000000ull;
+
+template <int NS>
+struct PtLayout {
+	static constexpr int B_BYTES = NS * PT_NC * 128;          // digit stack of one block: NS x 32 rows x 128 bytes
+	static constexpr int B_GRP = NS * (PT_NC / 8) * 128;      // bytes between 16-step (or 16-latitude) groups of a stack
+	static constexpr int A_OFF = 0;
+	static constexpr int B_OFF = PT_RA * PB_BYTES;
+	static constexpr int BAR_OFF = B_OFF + 2 * B_BYTES;
+	static constexpr int TOTAL = BAR_OFF + 128;
+	static constexpr int TMEM_COLS = 256;
+	static_assert(PT_NC * NS <= TMEM_COLS, "accumulators exceed the allocation");
+	static_assert(TOTAL + 1024 <= 113 * 1024, "two CTAs per SM");
+};
+
+// ---- PTX helpers ----
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+	uint64_t t;
+	asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+	return t;
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity)
+{
+	uint32_t done;
+	asm volatile("{\n\t.reg .pred p;\n\t"
+	             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+	             "selp.u32 %0, 1, 0, p;\n\t}"
+	             : "=r"(done) : "r"(a), "r"(parity) : "memory");
+	return done != 0;
+}
+
+// bounded wait for the phase of parity `parity`; false when the time limit
+// passes (the CTA's abort flag is then set) or another thread set the flag
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag)
+{
+	const uint32_t a = smem_u32(bar);
+	const uint64_t t0 = global_ns();
+	for (int it = 0;; it++) {
+		if (mbar_try(a, parity)) return true;
+		if ((it & 255) == 255) {
+			if (*abort_flag) return false;
+			if (global_ns() - t0 > PT_WAIT_NS) { *abort_flag = 1; return false; }
+		}
+	}
+}
+
+// the same wait without the flag (clean-up), bounded
+__device__ __forceinline__ void mbar_wait_quiet(uint64_t* bar, uint32_t parity)
+{
+	const uint32_t a = smem_u32(bar);
+	const uint64_t t0 = global_ns();
+	for (int it = 0;; it++) {
+		if (mbar_try(a, parity)) return;
+		if ((it & 255) == 255 && global_ns() - t0 > PT_WAIT_NS) return;
+	}
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// plain bulk copy global -> this CTA's shared memory (16-byte aligned, size a
+// multiple of 16), completion counted in bytes on the mbarrier
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+	             :: "r"(dst), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// shared-memory matrix descriptor, no swizzle; lbo / sbo in bytes (K-major:
+// lbo between core matrices along K, sbo between 8-row groups along M/N;
+// MN-major: lbo between 8-row groups along K, sbo between 16-byte chunks
+// along M/N)
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+	uint64_t d = 0;
+	d |= (uint64_t)((addr >> 4) & 0x3FFF);
+	d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+	d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+	d |= (uint64_t)1 << 46;            // descriptor version of sm_100
+	return d;
+}
+
+// instruction descriptor of kind::i8: signed x signed -> INT32; a_mn / b_mn:
+// 1 for an MN-major operand
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N, int a_mn, int b_mn)
+{
+	return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) a_mn << 15) | ((uint32_t) b_mn << 16) |
+	       ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+	asm volatile("{\n\t.reg .pred p;\n\t"
+	             "setp.ne.b32 p, %4, 0;\n\t"
+	             "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+	             :: "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc) : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar)
+{
+	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+	             :: "r"(smem_u32(bar)) : "memory");
+}
+
+// 16 consecutive INT32 columns of this warp's 32 lanes
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int* v)
+{
+	uint32_t r[16];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+	             "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+	             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+	               "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+	             : "r"(taddr));
+	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+	#pragma unroll
+	for (int i = 0; i < 16; i++) v[i] = (int) r[i];
+}
+
+// NS balanced 8-bit digits of v, |v| < 1/4: v ~ sum_i d_i 2^(-8(i+1)), d_i in
+// [-128, 127] for i >= 1 and d_0 in [-65, 65].  The value is rounded once to
+// an integer multiple of 2^(-8 NS) (exact FP64 scaling, one conversion), then
+// the digits are peeled from the bottom with sign-extended bytes.
+template <int NS>
+__device__ __forceinline__ void digits(double v, int* d)
+{
+	long long T = __double2ll_rn(v * (double)(1ull << (8 * NS)));
+	#pragma unroll
+	for (int i = NS - 1; i >= 1; i--) {
+		const int lo = (int)(signed char)(T & 0xFF);
+		d[i] = lo;
+		T = (T - lo) >> 8;
+	}
+	d[0] = (int) T;
+}
+
+// sixteen values of one column (or row) as NS 16-byte digit rows
+template <int NS>
+__device__ __forceinline__ void pack16(const double (&v)[16], uint4 (&w)[NS])
+{
+	uint32_t acc[NS][4];
+	#pragma unroll
+	for (int i = 0; i < NS; i++) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0u;
+	#pragma unroll
+	for (int e = 0; e < 16; e++) {
+		int d[NS];
+		digits<NS>(v[e], d);
+		#pragma unroll
+		for (int i = 0; i < NS; i++) acc[i][e >> 2] |= ((uint32_t) d[i] & 0xFFu) << (8 * (e & 3));
+	}
+	#pragma unroll
+	for (int i = 0; i < NS; i++) w[i] = make_uint4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+}
+
+struct PtabRef {
+	const uint8_t* tab;
+	const long* toff;        // per order: first digit-block
+	const long* koff;        // per order: first 128-step block (coefficient stacks)
+	const long* voff;        // per order: first kept latitude tile (Fourier stacks)
+	const int* t0;           // per order: first latitude tile kept
+	const short* yexp;       // row exponents [im][north row]
+	int ntb;                 // latitude tiles of the grid
+	int lmax;                // table steps of order m: (lmax + 1 - m) / 2 + 1
+};
+
+__device__ __forceinline__ int tab_kblocks(const PtabRef& t, int m) { return ((t.lmax + 1 - m) / 2 + 1 + PB_K - 1) / PB_K; }
+
+// ---------------------------------------------------------------------------
+// Table: CTA (latitude tile tb, order im), one thread per latitude.  Y_k is
+// regenerated from the checkpoint at the start of every SEG-step segment with
+// the FP64 kernels' operations (leg_synth_tile), on values scaled by
+// 2^-(e_t + 2) (a power of two: the recurrence commutes with it).
+template <int NS>
+__global__ void __launch_bounds__(PB_T) ptab_build_kernel(PtabRef t, int nlat_2, int mres, int seg,
+                                                          const double* __restrict__ x2g, const double* __restrict__ c,
+                                                          MTables mt, const double2* __restrict__ ck, uint8_t* __restrict__ tab)
+{
+	const int tb = blockIdx.x, im = blockIdx.y;
+	const int t0 = t.t0[im];
+	if (tb < t0) return;
+	const int m = im * mres;
+	const int kmax = (t.lmax + 1 - m) / 2 + 1;
+	const int nbk = (kmax + PB_K - 1) / PB_K;
+	const int r = threadIdx.x;
+	const int row = tb * PB_T + r;
+	const bool live = row < nlat_2;
+	const int e = live ? t.yexp[(long)im * nlat_2 + row] : -2000;
+	const double rsc = (live && e > -1000) ? ldexp(1.0, -(e + 2)) : 0.0;
+	const double x2 = live ? x2g[row] : 0.0;
+	const double* cc = c + mt.coff[im];
+	const double2* ckm = ck + (long)mt.ckoff[im] * nlat_2 + (live ? row : 0);
+	uint8_t* base = tab + (t.toff[im] + (long)(tb - t0) * NS * nbk) * PB_BYTES + (r >> 3) * 128 + (r & 7) * 16;
+	double y0 = 0.0, y1 = 0.0;
+	for (int kg = 0; kg < nbk * (PB_K / 16); kg++) {
+		double v[16];
+		#pragma unroll
+		for (int e16 = 0; e16 < 16; e16++) {
+			const int k = kg * 16 + e16;
+			double y = 0.0;
+			if (rsc != 0.0 && k < kmax) {
+				const int j = k % seg;
+				if (j == 0) {
+					const double2 q = __ldg(ckm + (long)(k / seg) * nlat_2);
+					y0 = q.x * rsc; y1 = q.y * rsc;
+					y = y0;
+				} else if (j == 1) {
+					y = y1;
+				} else {
+					const double a = fma(__ldg(cc + 2 * k - 1), x2, __ldg(cc + 2 * k - 2));
+					const double y2 = fma(a, y1, y0);
+					y0 = y1; y1 = y2;
+					y = y2;
+				}
+			}
+			v[e16] = y;
+		}
+		uint4 w[NS];
+		pack16<NS>(v, w);
+		const int kb = kg / (PB_K / 16), b = kg % (PB_K / 16);
+		#pragma unroll
+		for (int i = 0; i < NS; i++)
+			*reinterpret_cast<uint4*>(base + ((long) i * nbk + kb) * PB_BYTES + b * 16 * 128) = w[i];
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Coefficient digit stacks (synthesis B operand).  CTA (column tile ct, order
+// im): column exponents f_c over the call's steps, then per 128-step block a
+// stack of NS x 32 rows (row n = 32 j + column, digit j) x 128 steps, K-major:
+// 16-step group g at g B_GRP, row n at (n / 8) 128 + (n % 8) 16.
+template <int NS>
+__global__ void __launch_bounds__(256) ptab_qslice_kernel(PtabRef t, const double* __restrict__ qq, int ncol, MTables mt,
+                                                          int llim, int vec_extra, int mres, int nct,
+                                                          uint8_t* __restrict__ bs, int* __restrict__ bexp)
+{
+	using L = PtLayout<NS>;
+	__shared__ double red[8][PT_NC];
+	__shared__ double colsc[PT_NC];
+	const int ct = blockIdx.x, im = blockIdx.y;
+	const int m = im * mres;
+	const int nk = (llim + vec_extra - m) / 2 + 1;
+	const int nbk = (nk + PB_K - 1) / PB_K;
+	const double* qrow = qq + (long)mt.koff[im] * ncol;
+	const int tid = threadIdx.x;
+	{
+		const int cl = tid & 31, kr = tid >> 5;
+		const int col = ct * PT_NC + cl;
+		double mx = 0.0;
+		if (col < ncol)
+			for (int k = kr; k < nk; k += 8) mx = fmax(mx, fabs(qrow[(long)k * ncol + col]));
+		red[kr][cl] = mx;
+	}
+	__syncthreads();
+	if (tid < PT_NC) {
+		double mx = 0.0;
+		for (int q = 0; q < 8; q++) mx = fmax(mx, red[q][tid]);
+		int e = 0;
+		if (mx > 0.0) frexp(mx, &e);
+		colsc[tid] = (mx > 0.0) ? ldexp(1.0, -(e + 2)) : 0.0;
+		bexp[(long)im * (nct * PT_NC) + ct * PT_NC + tid] = (mx > 0.0) ? e : -2000;
+	}
+	__syncthreads();
+	for (int u = tid; u < nbk * (PB_K / 16) * PT_NC; u += 256) {
+		const int cl = u & 31, kgl = u >> 5;
+		const int col = ct * PT_NC + cl;
+		double v[16];
+		#pragma unroll
+		for (int e16 = 0; e16 < 16; e16++) {
+			const int k = kgl * 16 + e16;
+			v[e16] = (k < nk && col < ncol) ? qrow[(long)k * ncol + col] * colsc[cl] : 0.0;
+		}
+		uint4 w[NS];
+		pack16<NS>(v, w);
+		const int kb = kgl / (PB_K / 16), g = kgl % (PB_K / 16);
+		uint8_t* blk = bs + ((t.koff[im] + kb) * nct + ct) * (long) L::B_BYTES + (long) g * L::B_GRP;
+		#pragma unroll
+		for (int j = 0; j < NS; j++) {
+			const int n = PT_NC * j + cl;
+			*reinterpret_cast<uint4*>(blk + (n >> 3) * 128 + (n & 7) * 16) = w[j];
+		}
+	}
+}
+
+// Weighted Fourier digit stacks (analysis B operand).  CTA (column tile ct,
+// order im): G'[t, c] = 2^(e_t + 2) G[t, c] with G_even = w (F_N + F_S), G_odd
+// = w cos(theta) (F_N - F_S) as leg_analys_tile builds it (zero below the
+// polar threshold), column exponents g_c over the kept latitudes, then per
+// latitude tile a stack of NS x 32 rows x 128 latitudes, K-major (16-latitude
+// groups at B_GRP).  Thread item: (field-component fl of the tile, 16
+// latitudes): its four columns (even re, im; odd re, im).
+template <int NS>
+__global__ void __launch_bounds__(256) ptab_gslice_kernel(PtabRef t, LegParams p, int nct, uint8_t* __restrict__ bs,
+                                                          int* __restrict__ bexp)
+{
+	using L = PtLayout<NS>;
+	__shared__ double red[32][8][4];
+	__shared__ double colsc[8][4];
+	const int ct = blockIdx.x, im = blockIdx.y;
+	const int m = im * p.mres;
+	const int t0 = t.t0[im];
+	const int tmm = p.mt.tm[im];
+	const int ngrp = (t.ntb - t0) * (PB_T / 16);          // 16-latitude groups kept
+	const double wfac = (m > 0) ? p.mpos_inv : 1.0;
+	const int tid = threadIdx.x, fl = tid & 7;
+	const int fc = ct * 8 + fl;
+	const bool fc_ok = fc < p.nfc;
+	const bool vec = fc_ok && p.ctype[fc / p.nf] != 0;
+	const double2* Ff = p.F + (long)(fc_ok ? fc : 0) * p.fstride + (long)im * p.nlat;
+	auto value = [&](int row, double (&g)[4]) {
+		g[0] = g[1] = g[2] = g[3] = 0.0;
+		if (!fc_ok || row < tmm || row >= p.nlat_2) return;
+		const int e = t.yexp[(long)im * p.nlat_2 + row];
+		if (e <= -1000) return;
+		double w = p.adjoint ? p.nphi * (m > 0 ? 2.0 : 1.0) : p.w[row] * wfac;
+		if (vec) {
+			double s = p.sinv[row];
+			if (p.robert) s *= s;
+			w *= s;
+		}
+		w = ldexp(w, e + 2);
+		const double wo = w * p.x[row];
+		const int rn = p.south_first ? p.nlat - 1 - row : row;
+		const int rs = p.nlat - 1 - rn;
+		const double2 fn = __ldg(Ff + rn), fs = __ldg(Ff + rs);
+		g[0] = w * (fn.x + fs.x); g[1] = w * (fn.y + fs.y);
+		g[2] = wo * (fn.x - fs.x); g[3] = wo * (fn.y - fs.y);
+	};
+	// pass 1: column maxima
+	{
+		double mx[4] = {0.0, 0.0, 0.0, 0.0};
+		for (int gi = tid >> 3; gi < ngrp; gi += 32)
+			for (int e16 = 0; e16 < 16; e16++) {
+				double g[4];
+				value((t0 * (PB_T / 16) + gi) * 16 + e16, g);
+				#pragma unroll
+				for (int q = 0; q < 4; q++) mx[q] = fmax(mx[q], fabs(g[q]));
+			}
+		#pragma unroll
+		for (int q = 0; q < 4; q++) red[tid >> 3][fl][q] = mx[q];
+	}
+	__syncthreads();
+	if (tid < 32) {
+		const int f = tid >> 2, q = tid & 3;
+		double mx = 0.0;
+		for (int r = 0; r < 32; r++) mx = fmax(mx, red[r][f][q]);
+		int e = 0;
+		if (mx > 0.0) frexp(mx, &e);
+		colsc[f][q] = (mx > 0.0) ? ldexp(1.0, -(e + 2)) : 0.0;
+		// column of (field-component f, even/odd q >> 1, re/im q & 1) within the tile
+		const int cl = 16 * (f >> 2) + 2 * (f & 3) + (q & 1) + 8 * (q >> 1);
+		bexp[(long)im * (nct * PT_NC) + ct * PT_NC + cl] = (mx > 0.0) ? e : -2000;
+	}
+	__syncthreads();
+	// pass 2: digits, one column at a time (the F rows are re-read from L1)
+	for (int gi = tid >> 3; gi < ngrp; gi += 32) {
+		const int tt = gi / (PB_T / 16), g = gi % (PB_T / 16);
+		uint8_t* blk = bs + ((t.voff[im] + tt) * nct + ct) * (long) L::B_BYTES + (long) g * L::B_GRP;
+		#pragma unroll 1
+		for (int q = 0; q < 4; q++) {
+			double v[16];
+			#pragma unroll
+			for (int e16 = 0; e16 < 16; e16++) {
+				double gq[4];
+				value((t0 * (PB_T / 16) + gi) * 16 + e16, gq);
+				v[e16] = (q == 0 ? gq[0] : q == 1 ? gq[1] : q == 2 ? gq[2] : gq[3]) * colsc[fl][q];
+			}
+			uint4 w[NS];
+			pack16<NS>(v, w);
+			const int cl = 16 * (fl >> 2) + 2 * (fl & 3) + (q & 1) + 8 * (q >> 1);
+			#pragma unroll
+			for (int j = 0; j < NS; j++) {
+				const int n = PT_NC * j + cl;
+				*reinterpret_cast<uint4*>(blk + (n >> 3) * 128 + (n & 7) * 16) = w[j];
+			}
+		}
+	}
+}
+
+// ---------------------------------------------------------------------------
+// The contraction.  SYNTH: CTA = (latitude tile `tile`, order im), K loop over
+// nblk 128-step blocks; otherwise CTA = (128-step block `tile`, order im), K
+// loop over the nblk kept latitude tiles.  On return the epilogue threads
+// (warps 2-5) hold, for their row, acc[c] = sum_s 2^(-8 s) D_s[c], c < 32.
+// Returns false if a wait gave up (acc not valid).
+template <int NS, bool SYNTH>
+__device__ __forceinline__ bool ptab_contract(const PtabRef& t, const uint8_t* __restrict__ bs, int im, int tile,
+                                              int ct, int nct, int nblk, uint8_t* smem, double (&acc)[PT_NC],
+                                              int* err)
+{
+	using L = PtLayout<NS>;
+	uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
+	uint64_t* fullA = bars;                  // PT_RA
+	uint64_t* emptyA = bars + PT_RA;         // PT_RA
+	uint64_t* fullB = bars + 2 * PT_RA;      // 2
+	uint64_t* emptyB = bars + 2 * PT_RA + 2; // 2
+	uint64_t* done = bars + 2 * PT_RA + 4;
+	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L::BAR_OFF + 8 * (2 * PT_RA + 5));
+	volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L::BAR_OFF + 8 * (2 * PT_RA + 5) + 4);
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+	if (warp == 1) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+		             :: "r"(smem_u32(tmem_slot)), "r"((uint32_t) L::TMEM_COLS) : "memory");
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+	}
+	if (tid == 0) {
+		for (int i = 0; i < 2 * PT_RA + 5; i++) mbar_init(&bars[i], 1);
+		*abort_flag = 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = *tmem_slot;
+	const uint32_t sA = smem_u32(smem + L::A_OFF), sB = smem_u32(smem + L::B_OFF);
+	const long nbk = tab_kblocks(t, im);        // step blocks of the order in the table (mres = 1: m = im)
+	const int t0 = t.t0[im];
+
+	bool ok = true;
+	if (warp == 0 && lane == 0) {
+		// producer: per block the digit stack, then the NS digit-blocks of Y
+		int issuedA[PT_RA], issuedB[2] = {0, 0};
+		#pragma unroll
+		for (int q = 0; q < PT_RA; q++) issuedA[q] = 0;
+		for (int b = 0; b < nblk && ok; b++) {
+			const int bsl = b & 1;
+			if (b >= 2) ok = mbar_wait(&emptyB[bsl], ((b - 2) >> 1) & 1, abort_flag);
+			if (!ok) break;
+			const long bblk = SYNTH ? (t.koff[im] + b) : (t.voff[im] + b);
+			mbar_expect_tx(&fullB[bsl], L::B_BYTES);
+			bulk_g2s(sB + bsl * L::B_BYTES, bs + (bblk * nct + ct) * (long) L::B_BYTES, L::B_BYTES, &fullB[bsl]);
+			issuedB[bsl]++;
+			// digit-block (kept latitude tile ttr, digit i, step block kb) of the order
+			const int ttr = SYNTH ? tile - t0 : b;
+			const int kb = SYNTH ? b : tile;
+			for (int i = 0; i < NS && ok; i++) {
+				const int u = b * NS + i, slot = u % PT_RA;
+				if (u >= PT_RA) ok = mbar_wait(&emptyA[slot], ((u / PT_RA) - 1) & 1, abort_flag);
+				if (!ok) break;
+				const long blk = t.toff[im] + ((long) ttr * NS + i) * nbk + kb;
+				mbar_expect_tx(&fullA[slot], PB_BYTES);
+				bulk_g2s(sA + slot * PB_BYTES, t.tab + blk * PB_BYTES, PB_BYTES, &fullA[slot]);
+				#pragma unroll
+				for (int q = 0; q < PT_RA; q++) if (q == slot) issuedA[q]++;
+			}
+		}
+		// only the last copy into each slot can still be in flight: wait (bounded)
+		// for it so that no copy lands after the CTA has left
+		#pragma unroll
+		for (int q = 0; q < PT_RA; q++) if (issuedA[q]) mbar_wait_quiet(&fullA[q], (issuedA[q] - 1) & 1);
+		#pragma unroll
+		for (int q = 0; q < 2; q++) if (issuedB[q]) mbar_wait_quiet(&fullB[q], (issuedB[q] - 1) & 1);
+	} else if (warp == 1 && lane == 0) {
+		// tensor-core issue
+		bool any = false;
+		for (int b = 0; b < nblk && ok; b++) {
+			const int bsl = b & 1;
+			ok = mbar_wait(&fullB[bsl], (b >> 1) & 1, abort_flag);
+			for (int i = 0; i < NS && ok; i++) {
+				const int u = b * NS + i, slot = u % PT_RA;
+				ok = mbar_wait(&fullA[slot], (u / PT_RA) & 1, abort_flag);
+				if (!ok) break;
+				tc_fence_after();
+				const uint32_t idesc = idesc_i8(128, PT_NC * (NS - i), SYNTH ? 0 : 1, 0);
+				#pragma unroll
+				for (int kk = 0; kk < 4; kk++) {
+					uint64_t ad;
+					if (SYNTH) {
+						// A K-major: M = latitudes (8-row groups 128 B apart), K = steps (16-step core matrices 2048 B apart)
+						ad = sdesc(sA + slot * PB_BYTES + kk * 2 * 2048, 2048, 128);
+					} else {
+						// A MN-major: M = steps (16-byte chunks 2048 B apart), K = latitudes (8-row groups 128 B apart)
+						ad = sdesc(sA + slot * PB_BYTES + kk * 4 * 128, 128, 2048);
+					}
+					// B K-major: N = stacked digit rows (8-row groups 128 B apart), K in 16-byte core matrices B_GRP apart
+					const uint64_t bd = sdesc(sB + bsl * L::B_BYTES + kk * 2 * L::B_GRP, L::B_GRP, 128);
+					mma_i8(tmem + PT_NC * i, ad, bd, idesc, (b | i | kk) ? 1u : 0u);
+				}
+				any = true;
+				mma_commit(&emptyA[slot]);
+			}
+			if (ok) mma_commit(&emptyB[bsl]);
+		}
+		if (any) {
+			mma_commit(done);
+			if (!ok) mbar_wait_quiet(done, 0);      // products in flight finish before the memory is freed
+		}
+	}
+	// epilogue threads wait for the last products
+	if (warp >= 2) ok = mbar_wait(done, 0, abort_flag);
+	__syncwarp();
+	ok = __all_sync(0xffffffffu, ok) && (*abort_flag == 0);
+	if (warp >= 2 && ok) {
+		tc_fence_after();
+		const uint32_t trow = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+		#pragma unroll
+		for (int c = 0; c < PT_NC; c++) acc[c] = 0.0;
+		#pragma unroll
+		for (int s = NS - 1; s >= 0; s--) {
+			int v[16];
+			#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				tmem_ld16(trow + PT_NC * s + 16 * h, v);
+				#pragma unroll
+				for (int c = 0; c < 16; c++) acc[16 * h + c] = fma(acc[16 * h + c], 0.00390625, (double) v[c]);
+			}
+		}
+	}
+	tc_fence_before();
+	__syncthreads();
+	const bool aborted = (*abort_flag != 0);
+	if (aborted && tid == 0 && err) atomicExch(err, 1);
+	if (warp == 1) {
+		tc_fence_after();
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+		             :: "r"(tmem), "r"((uint32_t) L::TMEM_COLS) : "memory");
+	}
+	return !aborted;
+}
+
+template <int NS>
+__global__ void __launch_bounds__(PT_THREADS, 2) ptab_synth_kernel(PtabRef t, LegParams p, const uint8_t* __restrict__ bs,
+                                                                   const int* __restrict__ bexp, int nct, int* err)
+{
+	extern __shared__ __align__(1024) uint8_t smem_raw[];
+	uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+	const int tb = blockIdx.x % t.ntb, ct = blockIdx.x / t.ntb;
+	const int im = blockIdx.y;
+	const int m = im * p.mres;
+	const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
+	const int nblk = (nk + PB_K - 1) / PB_K;
+	const bool live = tb >= t.t0[im] && nk > 0;
+	double acc[PT_NC];
+	bool ok = false;
+	if (live) ok = ptab_contract<NS, true>(t, bs, im, tb, ct, nct, nblk, smem, acc, err);
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	if (warp < 2) return;
+	const int row = tb * PB_T + 32 * (warp & 3) + lane;
+	if (row >= p.nlat_2) return;
+	const int tmm = p.mt.tm[im];
+	const int e = t.yexp[(long)im * p.nlat_2 + row];
+	const bool val = ok && row >= tmm && e > -1000;
+	const double cx = p.x[row];
+	const int* be = bexp + (long)im * (nct * PT_NC) + ct * PT_NC;
+	#pragma unroll
+	for (int fl = 0; fl < 8; fl++) {
+		const int fc = ct * 8 + fl;
+		if (fc >= p.nfc) break;
+		const int c0 = 16 * (fl >> 2) + 2 * (fl & 3);          // even re; +1 im; +8 odd
+		auto col = [&](int cl) { return (val && be[cl] > -1000) ? acc[cl] * ldexp(1.0, e + be[cl] + 4 - 16) : 0.0; };
+		const double er = col(c0), ei = col(c0 + 1), orr = col(c0 + 8), oi = col(c0 + 9);
+		double nr = fma(cx, orr, er), ni = fma(cx, oi, ei);
+		double sr = fma(-cx, orr, er), si = fma(-cx, oi, ei);
+		const bool vec = (p.ctype[fc / p.nf] != 0) && !p.robert;
+		if (vec) { const double s = p.sinv[row]; nr *= s; ni *= s; sr *= s; si *= s; }
+		if (p.adjoint) {
+			const double s = p.w[row] * (m > 0 ? p.mpos_inv : 1.0) / (p.nphi * (m > 0 ? 2.0 : 1.0));
+			nr *= s; ni *= s; sr *= s; si *= s;
+		}
+		double2* Ff = p.F + (long)fc * p.fstride + (long)im * p.nlat;
+		const int rn = p.south_first ? p.nlat - 1 - row : row;
+		const int rs = p.nlat - 1 - rn;
+		Ff[rn] = make_double2(nr, ni);
+		Ff[rs] = make_double2(sr, si);
+	}
+}
+
+template <int NS>
+__global__ void __launch_bounds__(PT_THREADS, 2) ptab_analys_kernel(PtabRef t, LegParams p, const uint8_t* __restrict__ bs,
+                                                                    const int* __restrict__ bexp, int nct, int nkb, int* err)
+{
+	extern __shared__ __align__(1024) uint8_t smem_raw[];
+	uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+	const int kb = blockIdx.x % nkb, ct = blockIdx.x / nkb;
+	const int im = blockIdx.y;
+	const int m = im * p.mres;
+	const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
+	if (kb * PB_K >= nk) return;
+	const int ntt = t.ntb - t.t0[im];
+	double acc[PT_NC];
+	bool ok = false;
+	if (ntt > 0) ok = ptab_contract<NS, false>(t, bs, im, kb, ct, nct, ntt, smem, acc, err);
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	if (warp < 2) return;
+	const int k = kb * PB_K + 32 * (warp & 3) + lane;
+	if (k >= nk) return;
+	const int* be = bexp + (long)im * (nct * PT_NC) + ct * PT_NC;
+	double* qrow = p.qq + ((long)p.mt.koff[im] + k) * p.ncol + ct * PT_NC;
+	#pragma unroll
+	for (int c = 0; c < PT_NC; c += 2) {
+		if (ct * PT_NC + c >= p.ncol) break;
+		const double a = (ok && be[c] > -1000) ? acc[c] * ldexp(1.0, be[c] + 2 - 16) : 0.0;
+		const double b = (ok && be[c + 1] > -1000) ? acc[c + 1] * ldexp(1.0, be[c + 1] + 2 - 16) : 0.0;
+		*reinterpret_cast<double2*>(qrow + c) = make_double2(a, b);
+	}
+}
+
+bool grow(void** ptr, size_t* cap, size_t bytes, const char* what)
+{
+	if (*ptr && *cap >= bytes) return true;
+	if (*ptr) cudaFree(*ptr);
+	*ptr = nullptr; *cap = 0;
+	if (cudaMalloc(ptr, bytes) != cudaSuccess) {
+		cudaGetLastError();
+		shtb_set_error(3, std::string("out of device memory for ") + what);
+		return false;
+	}
+	*cap = bytes;
+	return true;
+}
+
+PtabRef ptab_ref(shtns_cfg o)
+{
+	PtabRef t;
+	t.tab = static_cast<const uint8_t*>(o->d_ptab);
+	t.toff = o->d_ptoff; t.koff = o->d_pkoff; t.voff = o->d_pvoff; t.t0 = o->d_pt0;
+	t.yexp = o->d_yexp;
+	t.ntb = (o->nlat_2 + PB_T - 1) / PB_T;
+	t.lmax = o->lmax;
+	return t;
+}
+
+template <int NS>
+void build_table(shtns_cfg o, cudaStream_t st)
+{
+	const PtabRef t = ptab_ref(o);
+	dim3 grid(t.ntb, o->mmax + 1);
+	ptab_build_kernel<NS><<<grid, PB_T, 0, st>>>(t, o->nlat_2, o->mres, o->ckseg, o->d_x2, o->d_c, o->mt, o->d_ck,
+	                                             static_cast<uint8_t*>(o->d_ptab));
+	shtb_count_launch();
+}
+
+// The digit table of plan o (the original plan of a clone) with ns digits,
+// built on first use.
+bool ptab_ensure(shtns_cfg o, int ns, cudaStream_t st)
+{
+	if (o->d_ptab && o->ptab_ns == ns) return true;
+	free_ptab(o);
+	if (o->mres != 1) { shtb_set_error(1, "split-precision tables need mres = 1"); return false; }
+	const int ntb = (o->nlat_2 + PB_T - 1) / PB_T;
+	const int nm = o->mmax + 1;
+	std::vector<long> toff(nm), koff(nm), voff(nm);
+	std::vector<int> t0(nm);
+	long nblocks = 0, kb = 0, tv = 0;
+	for (int im = 0; im < nm; im++) {
+		t0[im] = std::min(o->tm_h[im] / PB_T, ntb);
+		const int ntt = ntb - t0[im];
+		const int nbk = (o->kmax_h[im] + PB_K - 1) / PB_K;
+		toff[im] = nblocks; koff[im] = kb; voff[im] = tv;
+		nblocks += (long) ntt * ns * nbk;
+		kb += nbk; tv += ntt;
+	}
+	// exactness of the INT32 accumulators: ns products of at most 2^14 per step or latitude
+	const long kmax_all = std::max<long>(o->kmax_h[0], (long) ntb * PB_T);
+	if ((double) kmax_all * ns * 16384.0 >= 2147483647.0) {
+		shtb_set_error(1, "split-precision table: grid too large for exact accumulation");
+		return false;
+	}
+	const size_t bytes = (size_t) nblocks * PB_BYTES;
+	size_t fr = 0, tot = 0;
+	cudaMemGetInfo(&fr, &tot);
+	if (bytes + ((size_t) 1 << 30) > fr) {
+		shtb_set_error(3, "split-precision table needs " + std::to_string(bytes >> 20) + " MiB, " +
+		                  std::to_string(fr >> 20) + " MiB free");
+		return false;
+	}
+	bool okm = shtb_cuda_ok(cudaMalloc(&o->d_ptab, bytes), "split-precision table");
+	okm = okm && shtb_cuda_ok(cudaMalloc(&o->d_ptoff, sizeof(long) * 3 * nm), "split-precision table offsets");
+	okm = okm && shtb_cuda_ok(cudaMalloc(&o->d_pt0, sizeof(int) * nm), "split-precision table offsets");
+	if (!okm) { free_ptab(o); return false; }
+	o->d_pkoff = o->d_ptoff + nm; o->d_pvoff = o->d_ptoff + 2 * nm;
+	cudaMemcpy(o->d_ptoff, toff.data(), sizeof(long) * nm, cudaMemcpyHostToDevice);
+	cudaMemcpy(o->d_pkoff, koff.data(), sizeof(long) * nm, cudaMemcpyHostToDevice);
+	cudaMemcpy(o->d_pvoff, voff.data(), sizeof(long) * nm, cudaMemcpyHostToDevice);
+	cudaMemcpy(o->d_pt0, t0.data(), sizeof(int) * nm, cudaMemcpyHostToDevice);
+	o->ptab_bytes = bytes; o->ptab_ns = ns;
+	o->ptab_kblocks = kb; o->ptab_ttiles = tv;
+	if (!split_row_exponents(o, st)) { free_ptab(o); shtb_set_error(3, "out of device memory for row exponents"); return false; }
+	switch (ns) {
+		case 3: build_table<3>(o, st); break;
+		case 4: build_table<4>(o, st); break;
+		case 5: build_table<5>(o, st); break;
+		case 6: build_table<6>(o, st); break;
+		default: build_table<7>(o, st); break;
+	}
+	return shtb_cuda_ok(cudaGetLastError(), "split-precision table");
+}
+
+// per-call buffers of plan s: digit stacks for nblocks blocks and the column exponents
+bool ptab_buffers(shtns_cfg s, int ns, long nblocks, int nct)
+{
+	const size_t bb = (size_t) ns * PT_NC * 128;
+	if (!grow(&s->d_pbs, &s->pbs_cap, bb * (size_t) nblocks * nct, "split-precision digit stacks")) return false;
+	const size_t eb = sizeof(int) * (size_t)(s->mmax + 1) * nct * PT_NC;
+	return grow(reinterpret_cast<void**>(&s->d_pexp), &s->pexp_cap, eb, "split-precision column exponents");
+}
+
+bool split_err_flag(shtns_cfg s, cudaStream_t st)
+{
+	if (s->d_split_err) return true;
+	if (cudaMalloc(&s->d_split_err, sizeof(int)) != cudaSuccess) { cudaGetLastError(); return false; }
+	cudaMemsetAsync(s->d_split_err, 0, sizeof(int), st);
+	return true;
+}
+
+template <int NS>
+void synth_ns(shtns_cfg s, shtns_cfg o, const LegParams& p, int nct, cudaStream_t st)
+{
+	using L = PtLayout<NS>;
+	const PtabRef t = ptab_ref(o);
+	const size_t smem = L::TOTAL + 1024;
+	static bool attr = false;
+	if (!attr) {
+		cudaFuncSetAttribute(ptab_synth_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+		attr = true;
+	}
+	ptab_qslice_kernel<NS><<<dim3(nct, p.mlim + 1), 256, 0, st>>>(t, p.qq, p.ncol, p.mt, p.llim, p.vec_extra, p.mres, nct,
+	                                                             static_cast<uint8_t*>(s->d_pbs), s->d_pexp);
+	shtb_count_launch();
+	ptab_synth_kernel<NS><<<dim3(t.ntb * nct, p.mlim + 1), PT_THREADS, smem, st>>>(
+		t, p, static_cast<const uint8_t*>(s->d_pbs), s->d_pexp, nct, s->d_split_err);
+	shtb_count_launch();
+}
+
+template <int NS>
+void analys_ns(shtns_cfg s, shtns_cfg o, const LegParams& p, int nct, cudaStream_t st)
+{
+	using L = PtLayout<NS>;
+	const PtabRef t = ptab_ref(o);
+	const size_t smem = L::TOTAL + 1024;
+	static bool attr = false;
+	if (!attr) {
+		cudaFuncSetAttribute(ptab_analys_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+		attr = true;
+	}
+	ptab_gslice_kernel<NS><<<dim3(nct, p.mlim + 1), 256, 0, st>>>(t, p, nct, static_cast<uint8_t*>(s->d_pbs), s->d_pexp);
+	shtb_count_launch();
+	const int nk0 = (p.llim + p.vec_extra) / 2 + 1;             // steps of order 0, the largest
+	const int nkb = (nk0 + PB_K - 1) / PB_K;
+	ptab_analys_kernel<NS><<<dim3(nkb * nct, p.mlim + 1), PT_THREADS, smem, st>>>(
+		t, p, static_cast<const uint8_t*>(s->d_pbs), s->d_pexp, nct, nkb, s->d_split_err);
+	shtb_count_launch();
+}
+
+bool ptab_check(const LegParams& p)
+{
+	if (p.rb.n || p.im0) { shtb_set_error(1, "split precision runs whole transforms on the plain Fourier buffer only"); return false; }
+	return true;
+}
+
+} // namespace
+
+void launch_ptab_synth(shtns_cfg s, const LegParams& p, cudaStream_t st)
+{
+	if (!ptab_check(p)) return;
+	shtns_cfg o = s->is_clone ? s->base : s;
+	const int ns = s->split_ns;
+	if (!ptab_ensure(o, ns, st) || !split_err_flag(s, st)) return;
+	const int nct = (p.ncol + PT_NC - 1) / PT_NC;
+	if (!ptab_buffers(s, ns, o->ptab_kblocks, nct)) return;
+	switch (ns) {
+		case 3: synth_ns<3>(s, o, p, nct, st); break;
+		case 4: synth_ns<4>(s, o, p, nct, st); break;
+		case 5: synth_ns<5>(s, o, p, nct, st); break;
+		case 6: synth_ns<6>(s, o, p, nct, st); break;
+		default: synth_ns<7>(s, o, p, nct, st); break;
+	}
+}
+
+void launch_ptab_analys(shtns_cfg s, const LegParams& p, cudaStream_t st)
+{
+	if (!ptab_check(p)) return;
+	shtns_cfg o = s->is_clone ? s->base : s;
+	const int ns = s->split_ns;
+	if (!ptab_ensure(o, ns, st) || !split_err_flag(s, st)) return;
+	const int nct = (p.ncol + PT_NC - 1) / PT_NC;
+	if (!ptab_buffers(s, ns, o->ptab_ttiles, nct)) return;
+	switch (ns) {
+		case 3: analys_ns<3>(s, o, p, nct, st); break;
+		case 4: analys_ns<4>(s, o, p, nct, st); break;
+		case 5: analys_ns<5>(s, o, p, nct, st); break;
+		case 6: analys_ns<6>(s, o, p, nct, st); break;
+		default: analys_ns<7>(s, o, p, nct, st); break;
+	}
+}
+
+void free_ptab(shtns_cfg s)
+{
+	if (!s->is_clone) {
+		void* ptrs[] = {s->d_ptab, s->d_ptoff, s->d_pt0};
+		for (void* q : ptrs) if (q) cudaFree(q);
+	}
+	s->d_ptab = nullptr; s->ptab_bytes = 0; s->ptab_ns = 0;
+	s->d_ptoff = s->d_pkoff = s->d_pvoff = nullptr; s->d_pt0 = nullptr;
+	s->ptab_kblocks = 0; s->ptab_ttiles = 0;
+	if (s->d_pbs) cudaFree(s->d_pbs);
+	if (s->d_pexp) cudaFree(s->d_pexp);
+	s->d_pbs = nullptr; s->pbs_cap = 0; s->d_pexp = nullptr; s->pexp_cap = 0;
+}
+
+extern "C" size_t shtns_b200_split_table_bytes(shtns_cfg s)
+{
+	if (!s) return 0;
+	const shtns_cfg o = s->is_clone ? s->base : s;
+	return o->d_ptab ? o->ptab_bytes : 0;
+}

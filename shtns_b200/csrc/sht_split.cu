@@ -646,6 +646,12 @@ static bool split_tables(shtns_cfg s, int kc, cudaStream_t st)
 		s->split_chunks = tot;
 		s->split_kc = kc;
 	}
+	return split_row_exponents(s, st);
+}
+
+// Row exponents of the plan (yexp_kernel), computed once on first use.
+bool split_row_exponents(shtns_cfg s, cudaStream_t st)
+{
 	if (!s->d_yexp) {
 		if (cudaMalloc(&s->d_yexp, sizeof(short) * (size_t)(s->mmax + 1) * s->nlat_2) != cudaSuccess) {
 			cudaGetLastError(); return false;
@@ -659,6 +665,7 @@ static bool split_tables(shtns_cfg s, int kc, cudaStream_t st)
 
 void launch_leg_synth_split(shtns_cfg s, const LegParams& p, cudaStream_t st)
 {
+	if (s->split_form == 0) { launch_ptab_synth(s, p, st); return; }
 	if (p.rb.n) { shtb_set_error(1, "split-precision synthesis writes the plain Fourier buffer only"); return; }
 	const int ns = s->split_ns;
 	const int nc = ns <= 5 ? 32 : 16;             // accumulators: nc ns (ns + 1) / 2 <= 512 columns
@@ -680,6 +687,7 @@ void launch_leg_synth_split(shtns_cfg s, const LegParams& p, cudaStream_t st)
 
 void free_split(shtns_cfg s)
 {
+	free_ptab(s);
 	void* ptrs[] = {s->d_yexp, s->d_boff, s->d_bsl, s->d_bexp, s->d_split_err};
 	for (void* q : ptrs) if (q) cudaFree(q);
 	s->d_yexp = nullptr; s->d_boff = nullptr; s->split_chunks = 0; s->split_kc = 0;

@@ -145,12 +145,20 @@ class sht:
         c._clone_of = self
         return c
 
-    def set_split(self, nslices):
-        """Split-precision Legendre synthesis on the FP16 tensor cores with
-        `nslices` (3 to 7) 8-bit slices per operand; 0 restores the FP64
-        contraction.  Analysis always runs in FP64."""
+    def set_split(self, nslices, form=0):
+        """Split-precision Legendre stages with `nslices` (3 to 7) 8-bit digits
+        per operand; 0 restores the FP64 contraction.  form 0 (default): a
+        precomputed table of the Legendre values as INT8 digits, contracted on
+        the INT8 tensor cores with exact INT32 accumulation, for synthesis and
+        analysis (the table, about nslices bytes per latitude, order and
+        degree pair, is built on first use); form 1: synthesis only, slices
+        regenerated on the fly and contracted on the FP16 tensor cores
+        (analysis in FP64)."""
+        if form not in (0, 1):
+            raise ValueError("form must be 0 or 1")
         if self._lib.shtns_b200_set_option(self._cfg, 4, int(nslices)) != 0:
             raise ValueError("nslices must be 0 or 3..7")
+        self._lib.shtns_b200_set_option(self._cfg, 8, int(form))
 
     def kernel_errors(self):
         """1 if a bounded wait inside a split-precision kernel gave up (the

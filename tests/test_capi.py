@@ -132,6 +132,7 @@ def test_plan_options_validate_and_read_back():
         4: ([0, 3, 5, 7], [1, 2, 8]),               # split-precision slices
         5: ([0, 1, 2, 4, 8], [3, 16]),              # Legendre tile shape
         7: ([0, 16, 4096], [8, 4112, -16]),         # test hook of the FFT wait
+        8: ([0, 1], [2, -1]),                       # split-precision form
     }
     for opt, (good, bad) in cases.items():
         for v in good:

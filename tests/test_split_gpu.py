@@ -1,4 +1,5 @@
-"""Split-precision Legendre synthesis on the FP16 tensor cores (option 4).
+"""Split-precision Legendre synthesis on the FP16 tensor cores (option 4 with
+option 8 = 1: slices regenerated on the fly; synthesis only).
 
 Slices are 8-bit integers, so each kept product is summed exactly; the error
 comes only from the NS slices per operand (about 8 NS bits, relative to the
@@ -41,7 +42,7 @@ def test_split_accuracy_per_slices():
     v64 = sh.synth(q)
     errs = {}
     for ns in (3, 4, 5, 6, 7):
-        sh.set_split(ns)
+        sh.set_split(ns, form=1)
         errs[ns] = _rel(sh.synth(q), v64)
         assert errs[ns] < BOUND[ns], (ns, errs[ns])
         assert sh.kernel_errors() == 0
@@ -58,7 +59,7 @@ def test_split_checkpoint_spacings_agree(ns):
     sh = _plan(255)
     q = torch.from_numpy(rand_spec(255, 255, 1, 9, power=1.0, nfields=4)).to(dev)
     v64 = sh.synth(q)
-    sh.set_split(ns)
+    sh.set_split(ns, form=1)
     outs = []
     for seg in (8, 16, 32):
         assert lib.shtns_b200_set_option(sh._cfg, 2, seg) == 0
@@ -77,7 +78,7 @@ def test_split_vector_and_truncated():
     t = torch.from_numpy(rand_spec(L, L, 1, 13, power=1.5, zero_l0=True, nfields=3)).to(dev)
     ref = sh.synth(q, s, t)
     ref_l = sh.synth(q, ltr=100)
-    sh.set_split(7)
+    sh.set_split(7, form=1)
     out = sh.synth(q, s, t)
     out_l = sh.synth(q, ltr=100)
     assert sh.kernel_errors() == 0
@@ -92,9 +93,9 @@ def test_split_high_degree():
     sh = _plan(L, nlat=6144, eps=1e-10)
     q = torch.from_numpy(rand_spec(L, L, 1, 15, power=1.0, nfields=2)).to(dev)
     v64 = sh.synth(q)
-    sh.set_split(7)
+    sh.set_split(7, form=1)
     e7 = _rel(sh.synth(q), v64)
-    sh.set_split(6)
+    sh.set_split(6, form=1)
     e6 = _rel(sh.synth(q), v64)
     assert sh.kernel_errors() == 0
     assert e7 < 1e-12 and e6 < 5e-10
