@@ -669,8 +669,8 @@ def run_highdeg(args):
         return st / np.maximum(ca, 1)
 
     def rel(a, b):
-        d = a - b
-        return float(d.abs().max() / b.abs().max()), float((d * d).mean().sqrt() / (b * b).mean().sqrt())
+        d, bb = (a - b).abs(), b.abs()
+        return float(d.max() / bb.max()), float((d * d).mean().sqrt() / (bb * bb).mean().sqrt())
 
     steps = max(3, min(args.steps, 10))
     clocks = ClockSampler(0)

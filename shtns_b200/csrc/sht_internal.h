@@ -117,6 +117,7 @@ struct shtns_info {
 	long *d_pkoff;                       // per order: first 128-step block (coefficient digit stacks)
 	long *d_pvoff;                       // per order: first kept theta tile (weighted Fourier digit stacks)
 	int *d_pt0;                          // per order: first theta tile kept by the polar threshold
+	int *d_pkf;                          // per (order, kept theta tile): first step block with a nonzero digit
 	long ptab_kblocks, ptab_ttiles;      // sums over the orders of the above counts
 	void *d_pbs; size_t pbs_cap;         // per call: B-operand digit stacks
 	int *d_pexp; size_t pexp_cap;        // per call: column exponents [im][column]

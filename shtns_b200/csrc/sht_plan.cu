@@ -670,7 +670,7 @@ extern "C" shtns_cfg cushtns_clone(shtns_cfg b, cudaStream_t compute_stream, cud
 	s->d_yexp = nullptr; s->d_boff = nullptr; s->split_chunks = 0; s->split_kc = 0;
 	s->d_bsl = nullptr; s->bsl_cap = 0; s->d_bexp = nullptr; s->bexp_cap = 0; s->d_split_err = nullptr;
 	s->d_ptab = nullptr; s->ptab_bytes = 0; s->ptab_ns = 0; s->d_ptoff = nullptr; s->d_pkoff = nullptr;
-	s->d_pvoff = nullptr; s->d_pt0 = nullptr; s->ptab_kblocks = 0; s->ptab_ttiles = 0;
+	s->d_pvoff = nullptr; s->d_pt0 = nullptr; s->d_pkf = nullptr; s->ptab_kblocks = 0; s->ptab_ttiles = 0;
 	s->d_pbs = nullptr; s->pbs_cap = 0; s->d_pexp = nullptr; s->pexp_cap = 0;
 	s->xfer_stream = nullptr; s->own_xfer = 0;
 	s->ev.clear(); s->ev_stage.clear(); s->ev_used = 0; s->timing = 0;

@@ -26,7 +26,11 @@
 // operand (M = latitudes, K = steps), the analysis reads the same bytes as
 // the MN-major A operand (M = steps, K = latitudes).  Per order the table
 // keeps the latitude tiles at or beyond the polar threshold and the step
-// blocks up to the plan's last step (degree lmax + 1).
+// blocks up to the plan's last step (degree lmax + 1).  Below the turning
+// point of each latitude (degrees l < m / sin(theta)) the Legendre values
+// decay exponentially; the build records, per order and latitude tile, the
+// first step block holding a nonzero digit, and the contraction skips the
+// blocks before it (their digits are all zero, so nothing is lost).
 //
 // Kernel shape (both directions, one CTA per 128-row tile of one order and 32
 // GEMM columns = 8 field-components; 192 threads, two CTAs per SM):
@@ -61,6 +65,7 @@ constexpr int PB_BYTES = PB_T * PB_K;      // one digit-block: 16 KB
 constexpr int PT_NC = 32;                  // GEMM columns per CTA
 constexpr int PT_THREADS = 192;
 constexpr int PT_RA = 3;                   // digit-block slots
+constexpr int PT_MAXITEMS = 128;           // step blocks or latitude tiles of one contraction
 constexpr uint64_t PT_WAIT_NS = 1000000000ull;
 
 template <int NS>
@@ -70,7 +75,8 @@ struct PtLayout {
 	static constexpr int A_OFF = 0;
 	static constexpr int B_OFF = PT_RA * PB_BYTES;
 	static constexpr int BAR_OFF = B_OFF + 2 * B_BYTES;
-	static constexpr int TOTAL = BAR_OFF + 128;
+	static constexpr int ITEM_OFF = BAR_OFF + 128;             // work items of the CTA: int2 (A block, B block)
+	static constexpr int TOTAL = ITEM_OFF + PT_MAXITEMS * 8;
 	static constexpr int TMEM_COLS = 256;
 	static_assert(PT_NC * NS <= TMEM_COLS, "accumulators exceed the allocation");
 	static_assert(TOTAL + 1024 <= 113 * 1024, "two CTAs per SM");
@@ -234,6 +240,7 @@ struct PtabRef {
 	const long* koff;        // per order: first 128-step block (coefficient stacks)
 	const long* voff;        // per order: first kept latitude tile (Fourier stacks)
 	const int* t0;           // per order: first latitude tile kept
+	const int* kf;           // per (order, kept tile) at voff: first step block with a nonzero digit
 	const short* yexp;       // row exponents [im][north row]
 	int ntb;                 // latitude tiles of the grid
 	int lmax;                // table steps of order m: (lmax + 1 - m) / 2 + 1
@@ -266,6 +273,10 @@ __global__ void __launch_bounds__(PB_T) ptab_build_kernel(PtabRef t, int nlat_2,
 	const double* cc = c + mt.coff[im];
 	const double2* ckm = ck + (long)mt.ckoff[im] * nlat_2 + (live ? row : 0);
 	uint8_t* base = tab + (t.toff[im] + (long)(tb - t0) * NS * nbk) * PB_BYTES + (r >> 3) * 128 + (r & 7) * 16;
+	__shared__ int first_nz;
+	if (r == 0) first_nz = nbk;
+	__syncthreads();
+	int my_first = nbk;
 	double y0 = 0.0, y1 = 0.0;
 	for (int kg = 0; kg < nbk * (PB_K / 16); kg++) {
 		double v[16];
@@ -294,9 +305,14 @@ __global__ void __launch_bounds__(PB_T) ptab_build_kernel(PtabRef t, int nlat_2,
 		pack16<NS>(v, w);
 		const int kb = kg / (PB_K / 16), b = kg % (PB_K / 16);
 		#pragma unroll
-		for (int i = 0; i < NS; i++)
+		for (int i = 0; i < NS; i++) {
 			*reinterpret_cast<uint4*>(base + ((long) i * nbk + kb) * PB_BYTES + b * 16 * 128) = w[i];
+			if ((w[i].x | w[i].y | w[i].z | w[i].w) && kb < my_first) my_first = kb;
+		}
 	}
+	atomicMin(&first_nz, my_first);
+	__syncthreads();
+	if (r == 0) const_cast<int*>(t.kf)[t.voff[im] + (tb - t0)] = first_nz;
 }
 
 // ---------------------------------------------------------------------------
@@ -454,14 +470,16 @@ __global__ void __launch_bounds__(256) ptab_gslice_kernel(PtabRef t, LegParams p
 
 // ---------------------------------------------------------------------------
 // The contraction.  SYNTH: CTA = (latitude tile `tile`, order im), K loop over
-// nblk 128-step blocks; otherwise CTA = (128-step block `tile`, order im), K
-// loop over the nblk kept latitude tiles.  On return the epilogue threads
-// (warps 2-5) hold, for their row, acc[c] = sum_s 2^(-8 s) D_s[c], c < 32.
-// Returns false if a wait gave up (acc not valid).
+// the 128-step blocks from the tile's first nonzero block to nblk; otherwise
+// CTA = (128-step block `tile`, order im), K loop over the kept latitude
+// tiles whose first nonzero block is at or before it.  On return 1 the
+// epilogue threads (warps 2-5) hold, for their row, acc[c] = sum_s 2^(-8 s)
+// D_s[c], c < 32; 0: nothing to contract (the result is zero); -1: a wait
+// gave up (acc not valid).
 template <int NS, bool SYNTH>
-__device__ __forceinline__ bool ptab_contract(const PtabRef& t, const uint8_t* __restrict__ bs, int im, int tile,
-                                              int ct, int nct, int nblk, uint8_t* smem, double (&acc)[PT_NC],
-                                              int* err)
+__device__ __forceinline__ int ptab_contract(const PtabRef& t, const uint8_t* __restrict__ bs, int im, int tile,
+                                             int ct, int nct, int nblk, uint8_t* smem, double (&acc)[PT_NC],
+                                             int* err)
 {
 	using L = PtLayout<NS>;
 	uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
@@ -472,7 +490,29 @@ __device__ __forceinline__ bool ptab_contract(const PtabRef& t, const uint8_t* _
 	uint64_t* done = bars + 2 * PT_RA + 4;
 	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L::BAR_OFF + 8 * (2 * PT_RA + 5));
 	volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L::BAR_OFF + 8 * (2 * PT_RA + 5) + 4);
+	int* nitems_s = reinterpret_cast<int*>(smem + L::BAR_OFF + 8 * (2 * PT_RA + 5) + 8);
+	int2* items = reinterpret_cast<int2*>(smem + L::ITEM_OFF);
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const long nbk = tab_kblocks(t, im);        // step blocks of the order in the table (mres = 1: m = im)
+	const int t0 = t.t0[im];
+	const long toff = t.toff[im], voff = t.voff[im];
+
+	// work items (first digit-block of Y relative to the order, digit stack block)
+	if (tid == 0) {
+		int n = 0;
+		if (SYNTH) {
+			const int ttr = tile - t0;
+			for (int kb = t.kf[voff + ttr]; kb < nblk && n < PT_MAXITEMS; kb++)
+				items[n++] = make_int2((int)((long) ttr * NS * nbk + kb), (int)(t.koff[im] + kb));
+		} else {
+			for (int ttr = 0; ttr < nblk && n < PT_MAXITEMS; ttr++)
+				if (t.kf[voff + ttr] <= tile) items[n++] = make_int2((int)((long) ttr * NS * nbk + tile), (int)(voff + ttr));
+		}
+		*nitems_s = n;
+	}
+	__syncthreads();
+	const int nit = *nitems_s;
+	if (nit == 0) return 0;
 
 	if (warp == 1) {
 		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -489,31 +529,26 @@ __device__ __forceinline__ bool ptab_contract(const PtabRef& t, const uint8_t* _
 	tc_fence_after();
 	const uint32_t tmem = *tmem_slot;
 	const uint32_t sA = smem_u32(smem + L::A_OFF), sB = smem_u32(smem + L::B_OFF);
-	const long nbk = tab_kblocks(t, im);        // step blocks of the order in the table (mres = 1: m = im)
-	const int t0 = t.t0[im];
 
 	bool ok = true;
 	if (warp == 0 && lane == 0) {
-		// producer: per block the digit stack, then the NS digit-blocks of Y
+		// producer: per item the digit stack, then the NS digit-blocks of Y
 		int issuedA[PT_RA], issuedB[2] = {0, 0};
 		#pragma unroll
 		for (int q = 0; q < PT_RA; q++) issuedA[q] = 0;
-		for (int b = 0; b < nblk && ok; b++) {
+		for (int b = 0; b < nit && ok; b++) {
 			const int bsl = b & 1;
+			const int2 it = items[b];
 			if (b >= 2) ok = mbar_wait(&emptyB[bsl], ((b - 2) >> 1) & 1, abort_flag);
 			if (!ok) break;
-			const long bblk = SYNTH ? (t.koff[im] + b) : (t.voff[im] + b);
 			mbar_expect_tx(&fullB[bsl], L::B_BYTES);
-			bulk_g2s(sB + bsl * L::B_BYTES, bs + (bblk * nct + ct) * (long) L::B_BYTES, L::B_BYTES, &fullB[bsl]);
+			bulk_g2s(sB + bsl * L::B_BYTES, bs + ((long) it.y * nct + ct) * (long) L::B_BYTES, L::B_BYTES, &fullB[bsl]);
 			issuedB[bsl]++;
-			// digit-block (kept latitude tile ttr, digit i, step block kb) of the order
-			const int ttr = SYNTH ? tile - t0 : b;
-			const int kb = SYNTH ? b : tile;
 			for (int i = 0; i < NS && ok; i++) {
 				const int u = b * NS + i, slot = u % PT_RA;
 				if (u >= PT_RA) ok = mbar_wait(&emptyA[slot], ((u / PT_RA) - 1) & 1, abort_flag);
 				if (!ok) break;
-				const long blk = t.toff[im] + ((long) ttr * NS + i) * nbk + kb;
+				const long blk = toff + it.x + (long) i * nbk;
 				mbar_expect_tx(&fullA[slot], PB_BYTES);
 				bulk_g2s(sA + slot * PB_BYTES, t.tab + blk * PB_BYTES, PB_BYTES, &fullA[slot]);
 				#pragma unroll
@@ -529,7 +564,7 @@ __device__ __forceinline__ bool ptab_contract(const PtabRef& t, const uint8_t* _
 	} else if (warp == 1 && lane == 0) {
 		// tensor-core issue
 		bool any = false;
-		for (int b = 0; b < nblk && ok; b++) {
+		for (int b = 0; b < nit && ok; b++) {
 			const int bsl = b & 1;
 			ok = mbar_wait(&fullB[bsl], (b >> 1) & 1, abort_flag);
 			for (int i = 0; i < NS && ok; i++) {
@@ -591,7 +626,7 @@ __device__ __forceinline__ bool ptab_contract(const PtabRef& t, const uint8_t* _
 		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
 		             :: "r"(tmem), "r"((uint32_t) L::TMEM_COLS) : "memory");
 	}
-	return !aborted;
+	return aborted ? -1 : 1;
 }
 
 template <int NS>
@@ -607,15 +642,15 @@ __global__ void __launch_bounds__(PT_THREADS, 2) ptab_synth_kernel(PtabRef t, Le
 	const int nblk = (nk + PB_K - 1) / PB_K;
 	const bool live = tb >= t.t0[im] && nk > 0;
 	double acc[PT_NC];
-	bool ok = false;
-	if (live) ok = ptab_contract<NS, true>(t, bs, im, tb, ct, nct, nblk, smem, acc, err);
+	int res = 0;
+	if (live) res = ptab_contract<NS, true>(t, bs, im, tb, ct, nct, nblk, smem, acc, err);
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	if (warp < 2) return;
 	const int row = tb * PB_T + 32 * (warp & 3) + lane;
 	if (row >= p.nlat_2) return;
 	const int tmm = p.mt.tm[im];
 	const int e = t.yexp[(long)im * p.nlat_2 + row];
-	const bool val = ok && row >= tmm && e > -1000;
+	const bool val = res == 1 && row >= tmm && e > -1000;
 	const double cx = p.x[row];
 	const int* be = bexp + (long)im * (nct * PT_NC) + ct * PT_NC;
 	#pragma unroll
@@ -654,8 +689,8 @@ __global__ void __launch_bounds__(PT_THREADS, 2) ptab_analys_kernel(PtabRef t, L
 	if (kb * PB_K >= nk) return;
 	const int ntt = t.ntb - t.t0[im];
 	double acc[PT_NC];
-	bool ok = false;
-	if (ntt > 0) ok = ptab_contract<NS, false>(t, bs, im, kb, ct, nct, ntt, smem, acc, err);
+	int res = 0;
+	if (ntt > 0) res = ptab_contract<NS, false>(t, bs, im, kb, ct, nct, ntt, smem, acc, err);
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	if (warp < 2) return;
 	const int k = kb * PB_K + 32 * (warp & 3) + lane;
@@ -665,8 +700,8 @@ __global__ void __launch_bounds__(PT_THREADS, 2) ptab_analys_kernel(PtabRef t, L
 	#pragma unroll
 	for (int c = 0; c < PT_NC; c += 2) {
 		if (ct * PT_NC + c >= p.ncol) break;
-		const double a = (ok && be[c] > -1000) ? acc[c] * ldexp(1.0, be[c] + 2 - 16) : 0.0;
-		const double b = (ok && be[c + 1] > -1000) ? acc[c + 1] * ldexp(1.0, be[c + 1] + 2 - 16) : 0.0;
+		const double a = (res == 1 && be[c] > -1000) ? acc[c] * ldexp(1.0, be[c] + 2 - 16) : 0.0;
+		const double b = (res == 1 && be[c + 1] > -1000) ? acc[c + 1] * ldexp(1.0, be[c + 1] + 2 - 16) : 0.0;
 		*reinterpret_cast<double2*>(qrow + c) = make_double2(a, b);
 	}
 }
@@ -689,7 +724,7 @@ PtabRef ptab_ref(shtns_cfg o)
 {
 	PtabRef t;
 	t.tab = static_cast<const uint8_t*>(o->d_ptab);
-	t.toff = o->d_ptoff; t.koff = o->d_pkoff; t.voff = o->d_pvoff; t.t0 = o->d_pt0;
+	t.toff = o->d_ptoff; t.koff = o->d_pkoff; t.voff = o->d_pvoff; t.t0 = o->d_pt0; t.kf = o->d_pkf;
 	t.yexp = o->d_yexp;
 	t.ntb = (o->nlat_2 + PB_T - 1) / PB_T;
 	t.lmax = o->lmax;
@@ -728,6 +763,10 @@ bool ptab_ensure(shtns_cfg o, int ns, cudaStream_t st)
 	}
 	// exactness of the INT32 accumulators: ns products of at most 2^14 per step or latitude
 	const long kmax_all = std::max<long>(o->kmax_h[0], (long) ntb * PB_T);
+	if ((o->kmax_h[0] + PB_K - 1) / PB_K > PT_MAXITEMS || ntb > PT_MAXITEMS) {
+		shtb_set_error(1, "split-precision table: more than 128 step blocks or latitude tiles");
+		return false;
+	}
 	if ((double) kmax_all * ns * 16384.0 >= 2147483647.0) {
 		shtb_set_error(1, "split-precision table: grid too large for exact accumulation");
 		return false;
@@ -743,6 +782,7 @@ bool ptab_ensure(shtns_cfg o, int ns, cudaStream_t st)
 	bool okm = shtb_cuda_ok(cudaMalloc(&o->d_ptab, bytes), "split-precision table");
 	okm = okm && shtb_cuda_ok(cudaMalloc(&o->d_ptoff, sizeof(long) * 3 * nm), "split-precision table offsets");
 	okm = okm && shtb_cuda_ok(cudaMalloc(&o->d_pt0, sizeof(int) * nm), "split-precision table offsets");
+	okm = okm && shtb_cuda_ok(cudaMalloc(&o->d_pkf, sizeof(int) * std::max<long>(tv, 1)), "split-precision table offsets");
 	if (!okm) { free_ptab(o); return false; }
 	o->d_pkoff = o->d_ptoff + nm; o->d_pvoff = o->d_ptoff + 2 * nm;
 	cudaMemcpy(o->d_ptoff, toff.data(), sizeof(long) * nm, cudaMemcpyHostToDevice);
@@ -863,11 +903,11 @@ void launch_ptab_analys(shtns_cfg s, const LegParams& p, cudaStream_t st)
 void free_ptab(shtns_cfg s)
 {
 	if (!s->is_clone) {
-		void* ptrs[] = {s->d_ptab, s->d_ptoff, s->d_pt0};
+		void* ptrs[] = {s->d_ptab, s->d_ptoff, s->d_pt0, s->d_pkf};
 		for (void* q : ptrs) if (q) cudaFree(q);
 	}
 	s->d_ptab = nullptr; s->ptab_bytes = 0; s->ptab_ns = 0;
-	s->d_ptoff = s->d_pkoff = s->d_pvoff = nullptr; s->d_pt0 = nullptr;
+	s->d_ptoff = s->d_pkoff = s->d_pvoff = nullptr; s->d_pt0 = nullptr; s->d_pkf = nullptr;
 	s->ptab_kblocks = 0; s->ptab_ttiles = 0;
 	if (s->d_pbs) cudaFree(s->d_pbs);
 	if (s->d_pexp) cudaFree(s->d_pexp);
