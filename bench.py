@@ -339,6 +339,56 @@ def run_gpu(args):
     # correctness of what was timed
     rt_err = max(float((a - b).abs().max() / a.abs().max()) for a, b in zip(spec, back))
 
+    # the split-precision form of the same step (INT8 digit table, 7 digits,
+    # synthesis and analysis on the INT8 tensor cores), timed the same way
+    # after its table is built; errors against the FP64 stages on the same inputs
+    split = None
+    if not args.no_split:
+        spat64 = [x.clone() for x in spat]
+        back64 = [x.clone() for x in back]
+        sh.set_split(args.split_digits)
+        t0b = time.perf_counter()
+        step()
+        torch.cuda.synchronize()
+        build_s = time.perf_counter() - t0b
+        for _ in range(args.warmup):
+            step()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        lib.shtns_b200_set_timing(sh._cfg, 1)
+        n0s = lib.shtns_b200_launch_count()
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        e1.synchronize()
+        launches_split = lib.shtns_b200_launch_count() - n0s
+        ms_split = e0.elapsed_time(e1) / args.steps
+        st_s = np.zeros(6)
+        ca_s = np.zeros(6, dtype=np.int64)
+        lib.shtns_b200_stage_times(sh._cfg, st_s.ctypes.data_as(C.c_void_p), ca_s.ctypes.data_as(C.c_void_p))
+        lib.shtns_b200_set_timing(sh._cfg, 0)
+        err_syn = max(float((a - b).abs().max() / b.abs().max()) for a, b in zip(spat, spat64))
+        sh.analys_into(spat64, back)
+        err_ana = max(float((a - b).abs().max() / b.abs().max()) for a, b in zip(back, back64))
+        kerr = int(sh.kernel_errors())
+        tab = int(lib.shtns_b200_split_table_bytes(sh._cfg))
+        sh.set_split(0)
+        del spat64, back64
+        if world > 1:
+            t = torch.tensor([ms_split], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_split = float(t.item())
+        per = st_s / np.maximum(ca_s, 1)
+        split = {"digits": args.split_digits, "value": world * nf / (ms_split * 1e-3), "ms_per_step": ms_split,
+                 "stages_ms": dict(zip(["prologue", "legendre_synthesis", "fft_synthesis", "fft_analysis",
+                                        "legendre_analysis", "epilogue"], [float(x) for x in per])),
+                 "synth_max_rel_err": err_syn, "analys_max_rel_err": err_ana, "kernel_errors": kerr,
+                 "table_bytes": tab, "table_build_s": build_s, "gpu_launches": int(launches_split),
+                 "form": "INT8 digit table of the Legendre values (built once per plan), tcgen05 kind::i8 with exact "
+                         "INT32 sums, FP64 combine; errors relative to the largest FP64 output"}
+
     # end to end through the public API: pinned host spectra in, spectra out.
     # The step's fields go in E2E_CHUNKS chunks, each on its own stream with
     # its own plan clone (cushtns_clone), so that the host->device copy of one
@@ -478,6 +528,7 @@ def run_gpu(args):
                              ((3 * nf * sh.nlm * 16 * 2 + 3 * nf * NLAT * NPHI * 8) / 1e9)},
             "roofline": roof,
             "stages": stages,
+            "split_precision": dict(split, speedup_vs_fp64=split["value"] / value) if split else None,
             "cufft_reference": dict(cufft_times, **{
                 "ours_fft_synthesis_ms": float(per_launch[2]), "ours_fft_analysis_ms": float(per_launch[3]),
                 "speedup_synthesis": cufft_times["z2z_inverse_ms"] / float(per_launch[2]),
@@ -994,6 +1045,8 @@ def main():
     ap.add_argument("--fields", type=int, default=NFIELDS)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-split", action="store_true", help="skip the split-precision form of the qst step")
+    ap.add_argument("--split-digits", type=int, default=7)
     ap.add_argument("--e2e-chunks", type=int, default=E2E_CHUNKS,
                     help="field chunks (streams) of the end-to-end step")
     ap.add_argument("--exchange", default="nccl", choices=["nccl", "fused"],

@@ -119,6 +119,7 @@ struct shtns_info {
 	int *d_pt0;                          // per order: first theta tile kept by the polar threshold
 	int *d_pkf;                          // per (order, kept theta tile): first step block with a nonzero digit
 	long ptab_kblocks, ptab_ttiles;      // sums over the orders of the above counts
+	std::vector<long> koff_blocks_h;     // host copy of d_pkoff
 	void *d_pbs; size_t pbs_cap;         // per call: B-operand digit stacks
 	int *d_pexp; size_t pexp_cap;        // per call: column exponents [im][column]
 	// local evaluation (points, latitudes, operators): classic-recurrence

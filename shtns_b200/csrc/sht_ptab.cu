@@ -64,8 +64,7 @@ constexpr int PB_K = 128;                  // Ishioka steps per digit-block and 
 constexpr int PB_BYTES = PB_T * PB_K;      // one digit-block: 16 KB
 constexpr int PT_NC = 32;                  // GEMM columns per CTA
 constexpr int PT_THREADS = 192;
-constexpr int PT_RA = 3;                   // digit-block slots
-constexpr int PT_MAXITEMS = 128;           // step blocks or latitude tiles of one contraction
+constexpr int PT_RA = 8;                   // digit-block slots of the copy ring
 constexpr uint64_t PT_WAIT_NS = 1000000000ull;
 
 template <int NS>
@@ -75,11 +74,12 @@ struct PtLayout {
 	static constexpr int A_OFF = 0;
 	static constexpr int B_OFF = PT_RA * PB_BYTES;
 	static constexpr int BAR_OFF = B_OFF + 2 * B_BYTES;
-	static constexpr int ITEM_OFF = BAR_OFF + 128;             // work items of the CTA: int2 (A block, B block)
-	static constexpr int TOTAL = ITEM_OFF + PT_MAXITEMS * 8;
-	static constexpr int TMEM_COLS = 256;
-	static_assert(PT_NC * NS <= TMEM_COLS, "accumulators exceed the allocation");
-	static_assert(TOTAL + 1024 <= 113 * 1024, "two CTAs per SM");
+	static constexpr int NBAR = 2 * PT_RA + 2 + 2 + 2 + 2 + 1;   // fullA, emptyA, fullB, emptyB, tfull, tempty, drain
+	static constexpr int BE_OFF = BAR_OFF + 8 * NBAR + 16;     // column exponents of the current item, per epilogue warp
+	static constexpr int TOTAL = BE_OFF + 4 * PT_NC * 4;
+	static constexpr int ACC_COLS = 256;                        // one accumulator buffer (NS x 32 used)
+	static_assert(PT_NC * NS <= ACC_COLS, "accumulators exceed a buffer");
+	static_assert(TOTAL + 1024 <= 227 * 1024, "shared memory");
 };
 
 // ---- PTX helpers ----
@@ -197,6 +197,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int* v)
 	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 	#pragma unroll
 	for (int i = 0; i < 16; i++) v[i] = (int) r[i];
+}
+
+// 2^n as a double from its exponent bits (normal range; ldexp otherwise)
+__device__ __forceinline__ double pow2(int n)
+{
+	if (n >= -1022 && n <= 1023) return __longlong_as_double((long long)(n + 1023) << 52);
+	return ldexp(1.0, n);
 }
 
 // NS balanced 8-bit digits of v, |v| < 1/4: v ~ sum_i d_i 2^(-8(i+1)), d_i in
@@ -378,149 +385,216 @@ __global__ void __launch_bounds__(256) ptab_qslice_kernel(PtabRef t, const doubl
 // = w cos(theta) (F_N - F_S) as leg_analys_tile builds it (zero below the
 // polar threshold), column exponents g_c over the kept latitudes, then per
 // latitude tile a stack of NS x 32 rows x 128 latitudes, K-major (16-latitude
-// groups at B_GRP).  Thread item: (field-component fl of the tile, 16
-// latitudes): its four columns (even re, im; odd re, im).
+// groups at B_GRP).  Pass 1 (column maxima) and the value staging of pass 2
+// run with consecutive threads on consecutive latitudes of one
+// field-component (coalesced rows of F); pass 2 stages a tile's 32 x 128
+// values in shared memory and packs the digits of (column, 16 latitudes)
+// per thread.
+__device__ __forceinline__ void gvalues(const PtabRef& t, const LegParams& p, int im, int fc, int row, double wfac, int m,
+                                        double (&g)[4])
+{
+	g[0] = g[1] = g[2] = g[3] = 0.0;
+	if (fc >= p.nfc || row < p.mt.tm[im] || row >= p.nlat_2) return;
+	const int e = t.yexp[(long) im * p.nlat_2 + row];
+	if (e <= -1000) return;
+	double w = p.adjoint ? p.nphi * (m > 0 ? 2.0 : 1.0) : p.w[row] * wfac;
+	if (p.ctype[fc / p.nf] != 0) {
+		double s = p.sinv[row];
+		if (p.robert) s *= s;
+		w *= s;
+	}
+	w = ldexp(w, e + 2);
+	const double wo = w * p.x[row];
+	const int rn = p.south_first ? p.nlat - 1 - row : row;
+	const int rs = p.nlat - 1 - rn;
+	const double2* Ff = p.F + (long) fc * p.fstride + (long) im * p.nlat;
+	const double2 fn = __ldg(Ff + rn), fs = __ldg(Ff + rs);
+	g[0] = w * (fn.x + fs.x); g[1] = w * (fn.y + fs.y);
+	g[2] = wo * (fn.x - fs.x); g[3] = wo * (fn.y - fs.y);
+}
+
 template <int NS>
 __global__ void __launch_bounds__(256) ptab_gslice_kernel(PtabRef t, LegParams p, int nct, uint8_t* __restrict__ bs,
                                                           int* __restrict__ bexp)
 {
 	using L = PtLayout<NS>;
-	__shared__ double red[32][8][4];
-	__shared__ double colsc[8][4];
+	__shared__ double vals[PT_NC][PB_T + 2];               // one tile: [column][latitude]
+	__shared__ double red[8][8][4];
+	__shared__ double colsc[PT_NC];
 	const int ct = blockIdx.x, im = blockIdx.y;
 	const int m = im * p.mres;
 	const int t0 = t.t0[im];
-	const int tmm = p.mt.tm[im];
-	const int ngrp = (t.ntb - t0) * (PB_T / 16);          // 16-latitude groups kept
+	const int ntt = t.ntb - t0;
 	const double wfac = (m > 0) ? p.mpos_inv : 1.0;
-	const int tid = threadIdx.x, fl = tid & 7;
-	const int fc = ct * 8 + fl;
-	const bool fc_ok = fc < p.nfc;
-	const bool vec = fc_ok && p.ctype[fc / p.nf] != 0;
-	const double2* Ff = p.F + (long)(fc_ok ? fc : 0) * p.fstride + (long)im * p.nlat;
-	auto value = [&](int row, double (&g)[4]) {
-		g[0] = g[1] = g[2] = g[3] = 0.0;
-		if (!fc_ok || row < tmm || row >= p.nlat_2) return;
-		const int e = t.yexp[(long)im * p.nlat_2 + row];
-		if (e <= -1000) return;
-		double w = p.adjoint ? p.nphi * (m > 0 ? 2.0 : 1.0) : p.w[row] * wfac;
-		if (vec) {
-			double s = p.sinv[row];
-			if (p.robert) s *= s;
-			w *= s;
-		}
-		w = ldexp(w, e + 2);
-		const double wo = w * p.x[row];
-		const int rn = p.south_first ? p.nlat - 1 - row : row;
-		const int rs = p.nlat - 1 - rn;
-		const double2 fn = __ldg(Ff + rn), fs = __ldg(Ff + rs);
-		g[0] = w * (fn.x + fs.x); g[1] = w * (fn.y + fs.y);
-		g[2] = wo * (fn.x - fs.x); g[3] = wo * (fn.y - fs.y);
-	};
-	// pass 1: column maxima
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	// pass 1: column maxima; warp w takes field-component w of the tile,
+	// lanes consecutive latitudes
 	{
+		const int fc = ct * 8 + warp;
 		double mx[4] = {0.0, 0.0, 0.0, 0.0};
-		for (int gi = tid >> 3; gi < ngrp; gi += 32)
-			for (int e16 = 0; e16 < 16; e16++) {
-				double g[4];
-				value((t0 * (PB_T / 16) + gi) * 16 + e16, g);
-				#pragma unroll
-				for (int q = 0; q < 4; q++) mx[q] = fmax(mx[q], fabs(g[q]));
-			}
+		for (int row = t0 * PB_T + lane; row < t.ntb * PB_T; row += 32) {
+			double g[4];
+			gvalues(t, p, im, fc, row, wfac, m, g);
+			#pragma unroll
+			for (int q = 0; q < 4; q++) mx[q] = fmax(mx[q], fabs(g[q]));
+		}
 		#pragma unroll
-		for (int q = 0; q < 4; q++) red[tid >> 3][fl][q] = mx[q];
+		for (int q = 0; q < 4; q++)
+			#pragma unroll
+			for (int o = 16; o; o >>= 1) mx[q] = fmax(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], o));
+		if (lane == 0) {
+			#pragma unroll
+			for (int q = 0; q < 4; q++) red[0][warp][q] = mx[q];
+		}
 	}
 	__syncthreads();
 	if (tid < 32) {
 		const int f = tid >> 2, q = tid & 3;
-		double mx = 0.0;
-		for (int r = 0; r < 32; r++) mx = fmax(mx, red[r][f][q]);
+		const double mx = red[0][f][q];
 		int e = 0;
 		if (mx > 0.0) frexp(mx, &e);
-		colsc[f][q] = (mx > 0.0) ? ldexp(1.0, -(e + 2)) : 0.0;
 		// column of (field-component f, even/odd q >> 1, re/im q & 1) within the tile
 		const int cl = 16 * (f >> 2) + 2 * (f & 3) + (q & 1) + 8 * (q >> 1);
-		bexp[(long)im * (nct * PT_NC) + ct * PT_NC + cl] = (mx > 0.0) ? e : -2000;
+		colsc[cl] = (mx > 0.0) ? ldexp(1.0, -(e + 2)) : 0.0;
+		bexp[(long) im * (nct * PT_NC) + ct * PT_NC + cl] = (mx > 0.0) ? e : -2000;
 	}
 	__syncthreads();
-	// pass 2: digits, one column at a time (the F rows are re-read from L1)
-	for (int gi = tid >> 3; gi < ngrp; gi += 32) {
-		const int tt = gi / (PB_T / 16), g = gi % (PB_T / 16);
-		uint8_t* blk = bs + ((t.voff[im] + tt) * nct + ct) * (long) L::B_BYTES + (long) g * L::B_GRP;
-		#pragma unroll 1
-		for (int q = 0; q < 4; q++) {
+	// pass 2, per kept tile
+	for (int tt = 0; tt < ntt; tt++) {
+		const int row0 = (t0 + tt) * PB_T;
+		for (int e = tid; e < 8 * PB_T; e += 256) {
+			const int fl = e / PB_T, rr = e - fl * PB_T;
+			double g[4];
+			gvalues(t, p, im, ct * 8 + fl, row0 + rr, wfac, m, g);
+			#pragma unroll
+			for (int q = 0; q < 4; q++) {
+				const int cl = 16 * (fl >> 2) + 2 * (fl & 3) + (q & 1) + 8 * (q >> 1);
+				vals[cl][rr] = g[q] * colsc[cl];
+			}
+		}
+		__syncthreads();
+		{
+			const int cl = tid & 31, g = tid >> 5;            // column, 16-latitude group
 			double v[16];
 			#pragma unroll
-			for (int e16 = 0; e16 < 16; e16++) {
-				double gq[4];
-				value((t0 * (PB_T / 16) + gi) * 16 + e16, gq);
-				v[e16] = (q == 0 ? gq[0] : q == 1 ? gq[1] : q == 2 ? gq[2] : gq[3]) * colsc[fl][q];
-			}
+			for (int e16 = 0; e16 < 16; e16++) v[e16] = vals[cl][16 * g + e16];
 			uint4 w[NS];
 			pack16<NS>(v, w);
-			const int cl = 16 * (fl >> 2) + 2 * (fl & 3) + (q & 1) + 8 * (q >> 1);
+			uint8_t* blk = bs + ((t.voff[im] + tt) * nct + ct) * (long) L::B_BYTES + (long) g * L::B_GRP;
 			#pragma unroll
 			for (int j = 0; j < NS; j++) {
 				const int n = PT_NC * j + cl;
 				*reinterpret_cast<uint4*>(blk + (n >> 3) * 128 + (n & 7) * 16) = w[j];
 			}
 		}
+		__syncthreads();
 	}
 }
 
 // ---------------------------------------------------------------------------
-// The contraction.  SYNTH: CTA = (latitude tile `tile`, order im), K loop over
-// the 128-step blocks from the tile's first nonzero block to nblk; otherwise
-// CTA = (128-step block `tile`, order im), K loop over the kept latitude
-// tiles whose first nonzero block is at or before it.  On return 1 the
-// epilogue threads (warps 2-5) hold, for their row, acc[c] = sum_s 2^(-8 s)
-// D_s[c], c < 32; 0: nothing to contract (the result is zero); -1: a wait
-// gave up (acc not valid).
+// The contraction, persistent: one CTA per SM walks the work items w =
+// blockIdx.x, blockIdx.x + gridDim.x, ... (consecutive items are the column
+// tiles of one (order, tile), so the digit-blocks they share are read from L2).
+//   SYNTH:  item = (order im, latitude tile tb, column tile ct), all tiles
+//           (those below the polar threshold are written as zeros); blocks =
+//           the 128-step blocks from the tile's first nonzero one to the
+//           call's last step.
+//   ANALYS: item = (order im, 128-step block kb, column tile ct) over the
+//           table's step blocks; blocks = the kept latitude tiles whose first
+//           nonzero block is at or before kb.
+// Roles: warp 0 copies, warp 1 issues the products into one of two tensor-
+// memory accumulator buffers (256 columns each), warps 2-5 read the buffer
+// of the previous item, combine it in FP64 and store, then release it.
+struct PtItem {
+	int im, tile, ct;        // order, latitude tile (SYNTH) or step block, column tile
+	int nb;                  // blocks to contract (0: nothing; the result is zero)
+	int first;               // SYNTH: first step block
+};
+
 template <int NS, bool SYNTH>
-__device__ __forceinline__ int ptab_contract(const PtabRef& t, const uint8_t* __restrict__ bs, int im, int tile,
-                                             int ct, int nct, int nblk, uint8_t* smem, double (&acc)[PT_NC],
-                                             int* err)
+__device__ __forceinline__ PtItem ptab_item(const PtabRef& t, const LegParams& p, long w, int nct)
+{
+	PtItem it;
+	it.ct = (int)(w % nct);
+	const long e = w / nct;
+	if (SYNTH) {
+		it.tile = (int)(e % t.ntb);
+		it.im = (int)(e / t.ntb);
+		const int m = it.im * p.mres;
+		const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
+		const int nblk = (nk + PB_K - 1) / PB_K;
+		const int t0 = t.t0[it.im];
+		it.first = (it.tile >= t0) ? t.kf[t.voff[it.im] + it.tile - t0] : nblk;
+		it.nb = (it.tile >= t0 && nk > 0) ? max(0, nblk - it.first) : 0;
+	} else {
+		// order of the global step block e: the last im with koff[im] <= e
+		int lo = 0, hi = p.mlim;
+		while (lo < hi) {
+			const int mid = (lo + hi + 1) >> 1;
+			if (t.koff[mid] <= e) lo = mid; else hi = mid - 1;
+		}
+		it.im = lo;
+		it.tile = (int)(e - t.koff[lo]);
+		it.first = 0;
+		const int m = it.im * p.mres;
+		const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
+		const int ntt = t.ntb - t.t0[it.im];
+		int n = 0;
+		if (it.tile * PB_K < nk)
+			for (int ttr = 0; ttr < ntt; ttr++) n += (t.kf[t.voff[it.im] + ttr] <= it.tile) ? 1 : 0;
+		it.nb = n;
+	}
+	return it;
+}
+
+// b-th block of an item: first digit-block of Y (global index, digit 0) and
+// the digit-stack block; ttr_scan carries the analysis scan position
+template <int NS, bool SYNTH>
+__device__ __forceinline__ void ptab_block(const PtabRef& t, const PtItem& it, int& ttr_scan, long& ablk, long& bblk)
+{
+	const long nbk = tab_kblocks(t, it.im);
+	const long toff = t.toff[it.im], voff = t.voff[it.im];
+	if (SYNTH) {
+		const int kb = ttr_scan++;               // starts at it.first
+		const int ttr = it.tile - t.t0[it.im];
+		ablk = toff + (long) ttr * NS * nbk + kb;
+		bblk = t.koff[it.im] + kb;
+	} else {
+		int ttr = ttr_scan;
+		while (t.kf[voff + ttr] > it.tile) ttr++;
+		ttr_scan = ttr + 1;
+		ablk = toff + (long) ttr * NS * nbk + it.tile;
+		bblk = voff + ttr;
+	}
+}
+
+template <int NS, bool SYNTH>
+__global__ void __launch_bounds__(PT_THREADS, 1) ptab_kernel(PtabRef t, LegParams p, const uint8_t* __restrict__ bs,
+                                                             const int* __restrict__ bexp, int nct, long nitems, int* err)
 {
 	using L = PtLayout<NS>;
+	extern __shared__ __align__(1024) uint8_t smem_raw[];
+	uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
 	uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
-	uint64_t* fullA = bars;                  // PT_RA
-	uint64_t* emptyA = bars + PT_RA;         // PT_RA
-	uint64_t* fullB = bars + 2 * PT_RA;      // 2
-	uint64_t* emptyB = bars + 2 * PT_RA + 2; // 2
-	uint64_t* done = bars + 2 * PT_RA + 4;
-	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L::BAR_OFF + 8 * (2 * PT_RA + 5));
-	volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L::BAR_OFF + 8 * (2 * PT_RA + 5) + 4);
-	int* nitems_s = reinterpret_cast<int*>(smem + L::BAR_OFF + 8 * (2 * PT_RA + 5) + 8);
-	int2* items = reinterpret_cast<int2*>(smem + L::ITEM_OFF);
+	uint64_t* fullA = bars;
+	uint64_t* emptyA = bars + PT_RA;
+	uint64_t* fullB = bars + 2 * PT_RA;
+	uint64_t* emptyB = fullB + 2;
+	uint64_t* tfull = emptyB + 2;
+	uint64_t* tempty = tfull + 2;
+	uint64_t* drain = tempty + 2;
+	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L::BAR_OFF + 8 * L::NBAR);
+	volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L::BAR_OFF + 8 * L::NBAR + 4);
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-	const long nbk = tab_kblocks(t, im);        // step blocks of the order in the table (mres = 1: m = im)
-	const int t0 = t.t0[im];
-	const long toff = t.toff[im], voff = t.voff[im];
-
-	// work items (first digit-block of Y relative to the order, digit stack block)
-	if (tid == 0) {
-		int n = 0;
-		if (SYNTH) {
-			const int ttr = tile - t0;
-			for (int kb = t.kf[voff + ttr]; kb < nblk && n < PT_MAXITEMS; kb++)
-				items[n++] = make_int2((int)((long) ttr * NS * nbk + kb), (int)(t.koff[im] + kb));
-		} else {
-			for (int ttr = 0; ttr < nblk && n < PT_MAXITEMS; ttr++)
-				if (t.kf[voff + ttr] <= tile) items[n++] = make_int2((int)((long) ttr * NS * nbk + tile), (int)(voff + ttr));
-		}
-		*nitems_s = n;
-	}
-	__syncthreads();
-	const int nit = *nitems_s;
-	if (nit == 0) return 0;
 
 	if (warp == 1) {
 		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-		             :: "r"(smem_u32(tmem_slot)), "r"((uint32_t) L::TMEM_COLS) : "memory");
+		             :: "r"(smem_u32(tmem_slot)), "r"(2u * L::ACC_COLS) : "memory");
 		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
 	}
 	if (tid == 0) {
-		for (int i = 0; i < 2 * PT_RA + 5; i++) mbar_init(&bars[i], 1);
+		// one arrival per phase, except tempty: one per epilogue warp
+		for (int i = 0; i < L::NBAR; i++) mbar_init(&bars[i], (&bars[i] == &tempty[0] || &bars[i] == &tempty[1]) ? 4 : 1);
 		*abort_flag = 0;
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
@@ -530,179 +604,194 @@ __device__ __forceinline__ int ptab_contract(const PtabRef& t, const uint8_t* __
 	const uint32_t tmem = *tmem_slot;
 	const uint32_t sA = smem_u32(smem + L::A_OFF), sB = smem_u32(smem + L::B_OFF);
 
-	bool ok = true;
-	if (warp == 0 && lane == 0) {
-		// producer: per item the digit stack, then the NS digit-blocks of Y
-		int issuedA[PT_RA], issuedB[2] = {0, 0};
-		#pragma unroll
-		for (int q = 0; q < PT_RA; q++) issuedA[q] = 0;
-		for (int b = 0; b < nit && ok; b++) {
-			const int bsl = b & 1;
-			const int2 it = items[b];
-			if (b >= 2) ok = mbar_wait(&emptyB[bsl], ((b - 2) >> 1) & 1, abort_flag);
-			if (!ok) break;
-			mbar_expect_tx(&fullB[bsl], L::B_BYTES);
-			bulk_g2s(sB + bsl * L::B_BYTES, bs + ((long) it.y * nct + ct) * (long) L::B_BYTES, L::B_BYTES, &fullB[bsl]);
-			issuedB[bsl]++;
-			for (int i = 0; i < NS && ok; i++) {
-				const int u = b * NS + i, slot = u % PT_RA;
-				if (u >= PT_RA) ok = mbar_wait(&emptyA[slot], ((u / PT_RA) - 1) & 1, abort_flag);
-				if (!ok) break;
-				const long blk = toff + it.x + (long) i * nbk;
-				mbar_expect_tx(&fullA[slot], PB_BYTES);
-				bulk_g2s(sA + slot * PB_BYTES, t.tab + blk * PB_BYTES, PB_BYTES, &fullA[slot]);
-				#pragma unroll
-				for (int q = 0; q < PT_RA; q++) if (q == slot) issuedA[q]++;
+	if (warp == 0) {
+		if (lane == 0) {
+			// producer
+			bool ok = true;
+			long ua = 0, ub = 0;
+			int issuedA[PT_RA], issuedB[2] = {0, 0};
+			#pragma unroll
+			for (int q = 0; q < PT_RA; q++) issuedA[q] = 0;
+			for (long w = blockIdx.x; w < nitems && ok; w += gridDim.x) {
+				const PtItem it = ptab_item<NS, SYNTH>(t, p, w, nct);
+				int scan = it.first;
+				for (int b = 0; b < it.nb && ok; b++) {
+					long ablk, bblk;
+					ptab_block<NS, SYNTH>(t, it, scan, ablk, bblk);
+					const int bsl = (int)(ub & 1);
+					if (ub >= 2) ok = mbar_wait(&emptyB[bsl], (uint32_t)(((ub >> 1) - 1) & 1), abort_flag);
+					if (!ok) break;
+					mbar_expect_tx(&fullB[bsl], L::B_BYTES);
+					bulk_g2s(sB + bsl * L::B_BYTES, bs + (bblk * nct + it.ct) * (long) L::B_BYTES, L::B_BYTES, &fullB[bsl]);
+					issuedB[bsl]++;
+					ub++;
+					const long nbk = tab_kblocks(t, it.im);
+					for (int i = 0; i < NS && ok; i++) {
+						const int slot = (int)(ua % PT_RA);
+						if (ua >= PT_RA) ok = mbar_wait(&emptyA[slot], (uint32_t)(((ua / PT_RA) - 1) & 1), abort_flag);
+						if (!ok) break;
+						mbar_expect_tx(&fullA[slot], PB_BYTES);
+						bulk_g2s(sA + slot * PB_BYTES, t.tab + (ablk + (long) i * nbk) * PB_BYTES, PB_BYTES, &fullA[slot]);
+						#pragma unroll
+						for (int q = 0; q < PT_RA; q++) if (q == slot) issuedA[q]++;
+						ua++;
+					}
+				}
 			}
+			// only the last copy into each slot can still be in flight: wait
+			// (bounded) for it so that no copy lands after the CTA has left
+			#pragma unroll
+			for (int q = 0; q < PT_RA; q++) if (issuedA[q]) mbar_wait_quiet(&fullA[q], (issuedA[q] - 1) & 1);
+			#pragma unroll
+			for (int q = 0; q < 2; q++) if (issuedB[q]) mbar_wait_quiet(&fullB[q], (issuedB[q] - 1) & 1);
 		}
-		// only the last copy into each slot can still be in flight: wait (bounded)
-		// for it so that no copy lands after the CTA has left
-		#pragma unroll
-		for (int q = 0; q < PT_RA; q++) if (issuedA[q]) mbar_wait_quiet(&fullA[q], (issuedA[q] - 1) & 1);
-		#pragma unroll
-		for (int q = 0; q < 2; q++) if (issuedB[q]) mbar_wait_quiet(&fullB[q], (issuedB[q] - 1) & 1);
-	} else if (warp == 1 && lane == 0) {
-		// tensor-core issue
-		bool any = false;
-		for (int b = 0; b < nit && ok; b++) {
-			const int bsl = b & 1;
-			ok = mbar_wait(&fullB[bsl], (b >> 1) & 1, abort_flag);
-			for (int i = 0; i < NS && ok; i++) {
-				const int u = b * NS + i, slot = u % PT_RA;
-				ok = mbar_wait(&fullA[slot], (u / PT_RA) & 1, abort_flag);
+	} else if (warp == 1) {
+		if (lane == 0) {
+			// tensor-core issue
+			bool ok = true, any = false;
+			long ua = 0, ub = 0, ni = 0;
+			for (long w = blockIdx.x; w < nitems && ok; w += gridDim.x) {
+				const PtItem it = ptab_item<NS, SYNTH>(t, p, w, nct);
+				if (it.nb == 0) continue;
+				const int buf = (int)(ni & 1);
+				if (ni >= 2) ok = mbar_wait(&tempty[buf], (uint32_t)(((ni >> 1) - 1) & 1), abort_flag);
 				if (!ok) break;
 				tc_fence_after();
-				const uint32_t idesc = idesc_i8(128, PT_NC * (NS - i), SYNTH ? 0 : 1, 0);
-				#pragma unroll
-				for (int kk = 0; kk < 4; kk++) {
-					uint64_t ad;
-					if (SYNTH) {
-						// A K-major: M = latitudes (8-row groups 128 B apart), K = steps (16-step core matrices 2048 B apart)
-						ad = sdesc(sA + slot * PB_BYTES + kk * 2 * 2048, 2048, 128);
-					} else {
-						// A MN-major: M = steps (16-byte chunks 2048 B apart), K = latitudes (8-row groups 128 B apart)
-						ad = sdesc(sA + slot * PB_BYTES + kk * 4 * 128, 128, 2048);
+				const uint32_t dbase = tmem + buf * L::ACC_COLS;
+				bool first = true;
+				for (int b = 0; b < it.nb && ok; b++) {
+					const int bsl = (int)(ub & 1);
+					ok = mbar_wait(&fullB[bsl], (uint32_t)((ub >> 1) & 1), abort_flag);
+					for (int i = 0; i < NS && ok; i++) {
+						const int slot = (int)(ua % PT_RA);
+						ok = mbar_wait(&fullA[slot], (uint32_t)((ua / PT_RA) & 1), abort_flag);
+						if (!ok) break;
+						tc_fence_after();
+						const uint32_t idesc = idesc_i8(128, PT_NC * (NS - i), SYNTH ? 0 : 1, 0);
+						#pragma unroll
+						for (int kk = 0; kk < 4; kk++) {
+							uint64_t ad;
+							if (SYNTH) {
+								// A K-major: M = latitudes (8-row groups 128 B apart), K = steps (16-step core matrices 2048 B apart)
+								ad = sdesc(sA + slot * PB_BYTES + kk * 2 * 2048, 2048, 128);
+							} else {
+								// A MN-major: M = steps (16-byte chunks 2048 B apart), K = latitudes (8-row groups 128 B apart)
+								ad = sdesc(sA + slot * PB_BYTES + kk * 4 * 128, 128, 2048);
+							}
+							// B K-major: N = stacked digit rows (8-row groups 128 B apart), K in 16-byte core matrices B_GRP apart
+							const uint64_t bd = sdesc(sB + bsl * L::B_BYTES + kk * 2 * L::B_GRP, L::B_GRP, 128);
+							mma_i8(dbase + PT_NC * i, ad, bd, idesc, first ? 0u : 1u);
+							first = false;
+						}
+						any = true;
+						mma_commit(&emptyA[slot]);
+						ua++;
 					}
-					// B K-major: N = stacked digit rows (8-row groups 128 B apart), K in 16-byte core matrices B_GRP apart
-					const uint64_t bd = sdesc(sB + bsl * L::B_BYTES + kk * 2 * L::B_GRP, L::B_GRP, 128);
-					mma_i8(tmem + PT_NC * i, ad, bd, idesc, (b | i | kk) ? 1u : 0u);
+					if (ok) { mma_commit(&emptyB[bsl]); ub++; }
 				}
-				any = true;
-				mma_commit(&emptyA[slot]);
+				if (ok) { mma_commit(&tfull[buf]); ni++; }
 			}
-			if (ok) mma_commit(&emptyB[bsl]);
+			if (any) {
+				// products still in flight finish before the memory is released
+				mma_commit(drain);
+				mbar_wait_quiet(drain, 0);
+			}
 		}
-		if (any) {
-			mma_commit(done);
-			if (!ok) mbar_wait_quiet(done, 0);      // products in flight finish before the memory is freed
-		}
-	}
-	// epilogue threads wait for the last products
-	if (warp >= 2) ok = mbar_wait(done, 0, abort_flag);
-	__syncwarp();
-	ok = __all_sync(0xffffffffu, ok) && (*abort_flag == 0);
-	if (warp >= 2 && ok) {
-		tc_fence_after();
-		const uint32_t trow = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
-		#pragma unroll
-		for (int c = 0; c < PT_NC; c++) acc[c] = 0.0;
-		#pragma unroll
-		for (int s = NS - 1; s >= 0; s--) {
-			int v[16];
-			#pragma unroll
-			for (int h = 0; h < 2; h++) {
-				tmem_ld16(trow + PT_NC * s + 16 * h, v);
+	} else {
+		// epilogue: warps 2-5, TMEM lanes 32 (warp % 4) ..
+		const int q = warp & 3;
+		long ni = 0;
+		for (long w = blockIdx.x; w < nitems; w += gridDim.x) {
+			const PtItem it = ptab_item<NS, SYNTH>(t, p, w, nct);
+			const int m = it.im * p.mres;
+			const int r = 32 * q + lane;
+			double acc[PT_NC];
+			bool val = false;
+			if (it.nb > 0) {
+				const int buf = (int)(ni & 1);
+				bool ok = mbar_wait(&tfull[buf], (uint32_t)((ni >> 1) & 1), abort_flag);
+				ok = __all_sync(0xffffffffu, ok);
+				if (!ok) break;
+				tc_fence_after();
+				const uint32_t trow = tmem + buf * L::ACC_COLS + ((uint32_t)(32 * q) << 16);
 				#pragma unroll
-				for (int c = 0; c < 16; c++) acc[16 * h + c] = fma(acc[16 * h + c], 0.00390625, (double) v[c]);
+				for (int c = 0; c < PT_NC; c++) acc[c] = 0.0;
+				#pragma unroll
+				for (int s = NS - 1; s >= 0; s--) {
+					int v[16];
+					#pragma unroll
+					for (int h = 0; h < 2; h++) {
+						tmem_ld16(trow + PT_NC * s + 16 * h, v);
+						#pragma unroll
+						for (int c = 0; c < 16; c++) acc[16 * h + c] = fma(acc[16 * h + c], 0.00390625, (double) v[c]);
+					}
+				}
+				tc_fence_before();
+				__syncwarp();
+				if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(&tempty[buf])) : "memory");
+				ni++;
+				val = true;
+			}
+			// column exponents of the item, staged per warp
+			int* be = reinterpret_cast<int*>(smem + L::BE_OFF) + q * PT_NC;
+			__syncwarp();
+			be[lane] = __ldg(bexp + (long) it.im * (nct * PT_NC) + it.ct * PT_NC + lane);
+			__syncwarp();
+			if (SYNTH) {
+				const int row = it.tile * PB_T + r;
+				if (row < p.nlat_2) {
+					const int e = t.yexp[(long) it.im * p.nlat_2 + row];
+					const bool v = val && row >= p.mt.tm[it.im] && e > -1000;
+					const double cx = p.x[row];
+					#pragma unroll
+					for (int fl = 0; fl < 8; fl++) {
+						const int fc = it.ct * 8 + fl;
+						if (fc >= p.nfc) break;
+						const int c0 = 16 * (fl >> 2) + 2 * (fl & 3);          // even re; +1 im; +8 odd
+						auto col = [&](int cl) {
+							const int bc = be[cl];
+							return (v && bc > -1000) ? acc[cl] * pow2(e + bc + 4 - 16) : 0.0;
+						};
+						const double er = col(c0), ei = col(c0 + 1), orr = col(c0 + 8), oi = col(c0 + 9);
+						double nr = fma(cx, orr, er), ni2 = fma(cx, oi, ei);
+						double sr = fma(-cx, orr, er), si = fma(-cx, oi, ei);
+						const bool vec = (p.ctype[fc / p.nf] != 0) && !p.robert;
+						if (vec) { const double sv = p.sinv[row]; nr *= sv; ni2 *= sv; sr *= sv; si *= sv; }
+						if (p.adjoint) {
+							const double sa = p.w[row] * (m > 0 ? p.mpos_inv : 1.0) / (p.nphi * (m > 0 ? 2.0 : 1.0));
+							nr *= sa; ni2 *= sa; sr *= sa; si *= sa;
+						}
+						double2* Ff = p.F + (long) fc * p.fstride + (long) it.im * p.nlat;
+						const int rn = p.south_first ? p.nlat - 1 - row : row;
+						const int rs = p.nlat - 1 - rn;
+						Ff[rn] = make_double2(nr, ni2);
+						Ff[rs] = make_double2(sr, si);
+					}
+				}
+			} else {
+				const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
+				const int k = it.tile * PB_K + r;
+				if (k < nk) {
+					double* qrow = p.qq + ((long) p.mt.koff[it.im] + k) * p.ncol + it.ct * PT_NC;
+					#pragma unroll
+					for (int c = 0; c < PT_NC; c += 2) {
+						if (it.ct * PT_NC + c >= p.ncol) break;
+						const int b0 = be[c], b1 = be[c + 1];
+						const double a = (val && b0 > -1000) ? acc[c] * pow2(b0 + 2 - 16) : 0.0;
+						const double b = (val && b1 > -1000) ? acc[c + 1] * pow2(b1 + 2 - 16) : 0.0;
+						*reinterpret_cast<double2*>(qrow + c) = make_double2(a, b);
+					}
+				}
 			}
 		}
 	}
 	tc_fence_before();
 	__syncthreads();
-	const bool aborted = (*abort_flag != 0);
-	if (aborted && tid == 0 && err) atomicExch(err, 1);
+	if (tid == 0 && *abort_flag && err) atomicExch(err, 1);
 	if (warp == 1) {
 		tc_fence_after();
 		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
-		             :: "r"(tmem), "r"((uint32_t) L::TMEM_COLS) : "memory");
-	}
-	return aborted ? -1 : 1;
-}
-
-template <int NS>
-__global__ void __launch_bounds__(PT_THREADS, 2) ptab_synth_kernel(PtabRef t, LegParams p, const uint8_t* __restrict__ bs,
-                                                                   const int* __restrict__ bexp, int nct, int* err)
-{
-	extern __shared__ __align__(1024) uint8_t smem_raw[];
-	uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-	const int tb = blockIdx.x % t.ntb, ct = blockIdx.x / t.ntb;
-	const int im = blockIdx.y;
-	const int m = im * p.mres;
-	const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
-	const int nblk = (nk + PB_K - 1) / PB_K;
-	const bool live = tb >= t.t0[im] && nk > 0;
-	double acc[PT_NC];
-	int res = 0;
-	if (live) res = ptab_contract<NS, true>(t, bs, im, tb, ct, nct, nblk, smem, acc, err);
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	if (warp < 2) return;
-	const int row = tb * PB_T + 32 * (warp & 3) + lane;
-	if (row >= p.nlat_2) return;
-	const int tmm = p.mt.tm[im];
-	const int e = t.yexp[(long)im * p.nlat_2 + row];
-	const bool val = res == 1 && row >= tmm && e > -1000;
-	const double cx = p.x[row];
-	const int* be = bexp + (long)im * (nct * PT_NC) + ct * PT_NC;
-	#pragma unroll
-	for (int fl = 0; fl < 8; fl++) {
-		const int fc = ct * 8 + fl;
-		if (fc >= p.nfc) break;
-		const int c0 = 16 * (fl >> 2) + 2 * (fl & 3);          // even re; +1 im; +8 odd
-		auto col = [&](int cl) { return (val && be[cl] > -1000) ? acc[cl] * ldexp(1.0, e + be[cl] + 4 - 16) : 0.0; };
-		const double er = col(c0), ei = col(c0 + 1), orr = col(c0 + 8), oi = col(c0 + 9);
-		double nr = fma(cx, orr, er), ni = fma(cx, oi, ei);
-		double sr = fma(-cx, orr, er), si = fma(-cx, oi, ei);
-		const bool vec = (p.ctype[fc / p.nf] != 0) && !p.robert;
-		if (vec) { const double s = p.sinv[row]; nr *= s; ni *= s; sr *= s; si *= s; }
-		if (p.adjoint) {
-			const double s = p.w[row] * (m > 0 ? p.mpos_inv : 1.0) / (p.nphi * (m > 0 ? 2.0 : 1.0));
-			nr *= s; ni *= s; sr *= s; si *= s;
-		}
-		double2* Ff = p.F + (long)fc * p.fstride + (long)im * p.nlat;
-		const int rn = p.south_first ? p.nlat - 1 - row : row;
-		const int rs = p.nlat - 1 - rn;
-		Ff[rn] = make_double2(nr, ni);
-		Ff[rs] = make_double2(sr, si);
-	}
-}
-
-template <int NS>
-__global__ void __launch_bounds__(PT_THREADS, 2) ptab_analys_kernel(PtabRef t, LegParams p, const uint8_t* __restrict__ bs,
-                                                                    const int* __restrict__ bexp, int nct, int nkb, int* err)
-{
-	extern __shared__ __align__(1024) uint8_t smem_raw[];
-	uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-	const int kb = blockIdx.x % nkb, ct = blockIdx.x / nkb;
-	const int im = blockIdx.y;
-	const int m = im * p.mres;
-	const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
-	if (kb * PB_K >= nk) return;
-	const int ntt = t.ntb - t.t0[im];
-	double acc[PT_NC];
-	int res = 0;
-	if (ntt > 0) res = ptab_contract<NS, false>(t, bs, im, kb, ct, nct, ntt, smem, acc, err);
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	if (warp < 2) return;
-	const int k = kb * PB_K + 32 * (warp & 3) + lane;
-	if (k >= nk) return;
-	const int* be = bexp + (long)im * (nct * PT_NC) + ct * PT_NC;
-	double* qrow = p.qq + ((long)p.mt.koff[im] + k) * p.ncol + ct * PT_NC;
-	#pragma unroll
-	for (int c = 0; c < PT_NC; c += 2) {
-		if (ct * PT_NC + c >= p.ncol) break;
-		const double a = (res == 1 && be[c] > -1000) ? acc[c] * ldexp(1.0, be[c] + 2 - 16) : 0.0;
-		const double b = (res == 1 && be[c + 1] > -1000) ? acc[c + 1] * ldexp(1.0, be[c + 1] + 2 - 16) : 0.0;
-		*reinterpret_cast<double2*>(qrow + c) = make_double2(a, b);
+		             :: "r"(tmem), "r"(2u * L::ACC_COLS) : "memory");
 	}
 }
 
@@ -763,10 +852,6 @@ bool ptab_ensure(shtns_cfg o, int ns, cudaStream_t st)
 	}
 	// exactness of the INT32 accumulators: ns products of at most 2^14 per step or latitude
 	const long kmax_all = std::max<long>(o->kmax_h[0], (long) ntb * PB_T);
-	if ((o->kmax_h[0] + PB_K - 1) / PB_K > PT_MAXITEMS || ntb > PT_MAXITEMS) {
-		shtb_set_error(1, "split-precision table: more than 128 step blocks or latitude tiles");
-		return false;
-	}
 	if ((double) kmax_all * ns * 16384.0 >= 2147483647.0) {
 		shtb_set_error(1, "split-precision table: grid too large for exact accumulation");
 		return false;
@@ -789,6 +874,7 @@ bool ptab_ensure(shtns_cfg o, int ns, cudaStream_t st)
 	cudaMemcpy(o->d_pkoff, koff.data(), sizeof(long) * nm, cudaMemcpyHostToDevice);
 	cudaMemcpy(o->d_pvoff, voff.data(), sizeof(long) * nm, cudaMemcpyHostToDevice);
 	cudaMemcpy(o->d_pt0, t0.data(), sizeof(int) * nm, cudaMemcpyHostToDevice);
+	o->koff_blocks_h = koff;
 	o->ptab_bytes = bytes; o->ptab_ns = ns;
 	o->ptab_kblocks = kb; o->ptab_ttiles = tv;
 	if (!split_row_exponents(o, st)) { free_ptab(o); shtb_set_error(3, "out of device memory for row exponents"); return false; }
@@ -819,43 +905,53 @@ bool split_err_flag(shtns_cfg s, cudaStream_t st)
 	return true;
 }
 
-template <int NS>
-void synth_ns(shtns_cfg s, shtns_cfg o, const LegParams& p, int nct, cudaStream_t st)
+int num_sms()
+{
+	static int n = 0;
+	if (!n) {
+		int dev = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+		if (n <= 0) n = 148;
+	}
+	return n;
+}
+
+template <int NS, bool SYNTH>
+void launch_contract(const PtabRef& t, const LegParams& p, shtns_cfg s, int nct, long nitems, cudaStream_t st)
 {
 	using L = PtLayout<NS>;
-	const PtabRef t = ptab_ref(o);
 	const size_t smem = L::TOTAL + 1024;
 	static bool attr = false;
 	if (!attr) {
-		cudaFuncSetAttribute(ptab_synth_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+		cudaFuncSetAttribute(ptab_kernel<NS, SYNTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
 		attr = true;
 	}
+	const int grid = (int) std::max<long>(1, std::min<long>(nitems, num_sms()));
+	ptab_kernel<NS, SYNTH><<<grid, PT_THREADS, smem, st>>>(t, p, static_cast<const uint8_t*>(s->d_pbs), s->d_pexp, nct,
+	                                                       nitems, s->d_split_err);
+	shtb_count_launch();
+}
+
+template <int NS>
+void synth_ns(shtns_cfg s, shtns_cfg o, const LegParams& p, int nct, cudaStream_t st)
+{
+	const PtabRef t = ptab_ref(o);
 	ptab_qslice_kernel<NS><<<dim3(nct, p.mlim + 1), 256, 0, st>>>(t, p.qq, p.ncol, p.mt, p.llim, p.vec_extra, p.mres, nct,
 	                                                             static_cast<uint8_t*>(s->d_pbs), s->d_pexp);
 	shtb_count_launch();
-	ptab_synth_kernel<NS><<<dim3(t.ntb * nct, p.mlim + 1), PT_THREADS, smem, st>>>(
-		t, p, static_cast<const uint8_t*>(s->d_pbs), s->d_pexp, nct, s->d_split_err);
-	shtb_count_launch();
+	launch_contract<NS, true>(t, p, s, nct, (long)(p.mlim + 1) * t.ntb * nct, st);
 }
 
 template <int NS>
 void analys_ns(shtns_cfg s, shtns_cfg o, const LegParams& p, int nct, cudaStream_t st)
 {
-	using L = PtLayout<NS>;
 	const PtabRef t = ptab_ref(o);
-	const size_t smem = L::TOTAL + 1024;
-	static bool attr = false;
-	if (!attr) {
-		cudaFuncSetAttribute(ptab_analys_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-		attr = true;
-	}
 	ptab_gslice_kernel<NS><<<dim3(nct, p.mlim + 1), 256, 0, st>>>(t, p, nct, static_cast<uint8_t*>(s->d_pbs), s->d_pexp);
 	shtb_count_launch();
-	const int nk0 = (p.llim + p.vec_extra) / 2 + 1;             // steps of order 0, the largest
-	const int nkb = (nk0 + PB_K - 1) / PB_K;
-	ptab_analys_kernel<NS><<<dim3(nkb * nct, p.mlim + 1), PT_THREADS, smem, st>>>(
-		t, p, static_cast<const uint8_t*>(s->d_pbs), s->d_pexp, nct, nkb, s->d_split_err);
-	shtb_count_launch();
+	// step blocks of the orders 0 .. mlim in the table
+	const long nkb = (p.mlim < o->mmax) ? o->koff_blocks_h[p.mlim + 1] : o->ptab_kblocks;
+	launch_contract<NS, false>(t, p, s, nct, nkb * nct, st);
 }
 
 bool ptab_check(const LegParams& p)
@@ -909,6 +1005,7 @@ void free_ptab(shtns_cfg s)
 	s->d_ptab = nullptr; s->ptab_bytes = 0; s->ptab_ns = 0;
 	s->d_ptoff = s->d_pkoff = s->d_pvoff = nullptr; s->d_pt0 = nullptr; s->d_pkf = nullptr;
 	s->ptab_kblocks = 0; s->ptab_ttiles = 0;
+	s->koff_blocks_h.clear();
 	if (s->d_pbs) cudaFree(s->d_pbs);
 	if (s->d_pexp) cudaFree(s->d_pexp);
 	s->d_pbs = nullptr; s->pbs_cap = 0; s->d_pexp = nullptr; s->pexp_cap = 0;
