@@ -232,6 +232,91 @@ def fp64_gemm_peak(torch, dev):
     return best
 
 
+def host_array_pair(torch, dev, lib, sh, qn, sn, tn, nf, steps, world, dist):
+    """The drop-in host API end to end: SHqst_to_spat then spat_to_SHqst of the
+    nf fields with HOST spectral and spatial arrays (page-locked, from
+    shtns_malloc, as the reference's users allocate them), wall clock around
+    the synchronous calls (max over ranks), beside the link's ceiling for the
+    same copies: per call its host->device and device->host bytes moved at
+    once on two streams without the transforms."""
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+    bufs = []
+
+    def pinned(shape, dtype):
+        n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        ptr = lib.shtns_malloc(n)
+        if not ptr:
+            raise MemoryError("shtns_malloc")
+        bufs.append(ptr)
+        return np.frombuffer((C.c_char * n).from_address(ptr), dtype=dtype).reshape(shape)
+
+    try:
+        spec = [pinned((nf, sh.nlm), np.complex128) for _ in range(3)]
+        for a, src in zip(spec, (qn, sn, tn)):
+            a[...] = src
+        spat = [pinned((nf,) + sh.spat_shape, np.float64) for _ in range(3)]
+        back = [pinned((nf, sh.nlm), np.complex128) for _ in range(3)]
+        lib.shtns_set_batch(sh._cfg, nf, sh.nlm, sh.nspat)
+        lib.cushtns_set_streams(sh._cfg, C.c_void_p(torch.cuda.current_stream().cuda_stream), None)
+
+        def pair():
+            lib.SHqst_to_spat(sh._cfg, *(P(a) for a in spec), *(P(a) for a in spat))
+            lib.spat_to_SHqst(sh._cfg, *(P(a) for a in spat), *(P(a) for a in back))
+
+        pair()
+        err = max(float(np.abs(a - b).max() / np.abs(a).max()) for a, b in zip(spec, back))
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            pair()
+        dt = (time.perf_counter() - t0) / steps
+        # the link's ceiling: the same bytes per call, both directions at once
+        nspec, nspat = 3 * nf * sh.nlm * 16, 3 * nf * sh.nspat * 8
+        d_spec = torch.empty(nspec, dtype=torch.uint8, device=dev)
+        d_spat = torch.empty(nspat, dtype=torch.uint8, device=dev)
+        h_spec = torch.from_numpy(np.concatenate([a.reshape(-1).view(np.uint8) for a in spec]))
+        h_spat = torch.from_numpy(np.concatenate([a.reshape(-1).view(np.uint8) for a in spat])).pin_memory()
+        h_spec = h_spec.pin_memory()
+        s1, s2 = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+
+        def copies():
+            with torch.cuda.stream(s1):
+                d_spec.copy_(h_spec, non_blocking=True)      # synthesis: spectra in
+            with torch.cuda.stream(s2):
+                h_spat.copy_(d_spat, non_blocking=True)      # synthesis: grids out
+            torch.cuda.synchronize()
+            with torch.cuda.stream(s1):
+                d_spat.copy_(h_spat, non_blocking=True)      # analysis: grids in
+            with torch.cuda.stream(s2):
+                h_spec.copy_(d_spec, non_blocking=True)      # analysis: spectra out
+            torch.cuda.synchronize()
+
+        copies()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            copies()
+        dl = (time.perf_counter() - t0) / steps
+        del d_spec, d_spat, h_spec, h_spat
+        if world > 1:
+            t = torch.tensor([dt, dl], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt, dl = float(t[0]), float(t[1])
+        return {"value": world * nf / dt, "unit": UNIT, "ms_per_step": 1e3 * dt,
+                "h2d_bytes_per_step": nspec + nspat, "d2h_bytes_per_step": nspec + nspat,
+                "roundtrip_relerr": err,
+                "link_ceiling": {"value": world * nf / dl, "ms_per_step": 1e3 * dl,
+                                 "note": "the same host<->device bytes per call, both directions at once on two "
+                                         "streams, without the transforms, timed in this run"},
+                "frac_of_link_ceiling": dl / dt,
+                "form": "SHqst_to_spat + spat_to_SHqst with page-locked host arrays (shtns_malloc): the library "
+                        "pipelines the fields in chunks over a transfer stream, the compute stream and a second copy "
+                        "stream; wall clock around the synchronous calls"}
+    finally:
+        for ptr in bufs:
+            lib.shtns_free(C.c_void_p(ptr))
+
+
 def cufft_reference_times(torch, dev, spat, nf, reps=5):
     """cuFFT with the reference's theta-contiguous plan (sht_gpu.cu:186-190:
     Z2Z of length nphi over the nlat/2 latitude pairs of one field, one
@@ -469,6 +554,7 @@ def run_gpu(args):
     bytes_io = 3 * nf * sh.nlm * 16
 
     cufft_times = cufft_reference_times(torch, dev, spat, nf) if rank == 0 else None
+    host_api = host_array_pair(torch, dev, lib, sh, qn, sn, tn, nf, max(2, min(args.steps, 5)), world, dist)
 
     if rank == 0:
         ms_step = ms_total / args.steps
@@ -528,6 +614,7 @@ def run_gpu(args):
                              ((3 * nf * sh.nlm * 16 * 2 + 3 * nf * NLAT * NPHI * 8) / 1e9)},
             "roofline": roof,
             "stages": stages,
+            "e2e_host_arrays": host_api,
             "split_precision": dict(split, speedup_vs_fp64=split["value"] / value) if split else None,
             "cufft_reference": dict(cufft_times, **{
                 "ours_fft_synthesis_ms": float(per_launch[2]), "ours_fft_analysis_ms": float(per_launch[3]),

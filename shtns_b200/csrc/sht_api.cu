@@ -237,8 +237,59 @@ bool stage_alloc(shtns_cfg s, int nspec, int nspatial, Stage& st)
 	return true;
 }
 
-size_t spec_bytes(shtns_cfg s) { return sizeof(double2) * ((size_t)(s->batch - 1) * s->spec_dist + s->nlm); }
-size_t spat_bytes(shtns_cfg s) { return sizeof(double) * ((size_t)(s->batch - 1) * s->spat_dist + s->nspat); }
+
+// Host-pointer transforms, pipelined over chunks of fields (up to 8 chunks):
+// host->device copies of chunk c+1 on the transfer stream and device->host
+// copies of chunk c on a second copy stream overlap the transforms of chunk c
+// (c+1) on the compute stream; events order each chunk's copies and
+// transforms.  Page-locked host arrays (shtns_malloc, cudaHostAlloc,
+// cudaHostRegister) are copied fully asynchronously, both directions at once;
+// pageable arrays go through the driver's staging, and the next chunk's
+// transforms are enqueued before a chunk's device->host copy (which returns
+// only when done), so the GPU keeps working while the host copies.
+// (The reference offloads sht_gpu.cu:584-1489 overlap per-component copies
+// with the transforms of the next component in the same way.)
+struct HostChunks {
+	int B, fpc, nch;
+};
+
+HostChunks host_chunks(shtns_cfg s)
+{
+	HostChunks h;
+	h.B = s->batch;
+	const int want = std::min(h.B, 8);
+	h.fpc = (h.B + want - 1) / want;
+	h.nch = (h.B + h.fpc - 1) / h.fpc;
+	return h;
+}
+
+bool copy_resources(shtns_cfg s, int nev)
+{
+	if (!s->d2h_stream && cudaStreamCreateWithFlags(&s->d2h_stream, cudaStreamNonBlocking) != cudaSuccess) {
+		cudaGetLastError();
+		s->d2h_stream = nullptr;
+		shtb_set_error(2, "could not create the copy stream");
+		return false;
+	}
+	if (!s->xfer_stream) {
+		if (cudaStreamCreateWithFlags(&s->xfer_stream, cudaStreamNonBlocking) != cudaSuccess) {
+			cudaGetLastError();
+			shtb_set_error(2, "could not create the transfer stream");
+			return false;
+		}
+		s->own_xfer = 1;
+	}
+	while ((int) s->xev.size() < nev) {
+		cudaEvent_t e;
+		if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+			cudaGetLastError();
+			shtb_set_error(2, "could not create copy events");
+			return false;
+		}
+		s->xev.push_back(e);
+	}
+	return true;
+}
 
 void h_synth(shtns_cfg s, int ncomp, const int* types, const cplx* Q, const cplx* S, const cplx* T,
              double* o0, double* o1, double* o2, int ltr)
@@ -247,16 +298,48 @@ void h_synth(shtns_cfg s, int ncomp, const int* types, const cplx* Q, const cplx
 	const int nin = (Q ? 1 : 0) + (S ? 1 : 0) + (T ? 1 : 0);
 	Stage st;
 	if (!stage_alloc(s, nin, ncomp, st)) return;
-	int k = 0;
-	const double2* dQ = nullptr; const double2* dS = nullptr; const double2* dT = nullptr;
-	cudaStream_t cs = s->comp_stream;
-	if (Q) { cudaMemcpyAsync(st.spec[k], Q, spec_bytes(s), cudaMemcpyHostToDevice, cs); dQ = st.spec[k++]; }
-	if (S) { cudaMemcpyAsync(st.spec[k], S, spec_bytes(s), cudaMemcpyHostToDevice, cs); dS = st.spec[k++]; }
-	if (T) { cudaMemcpyAsync(st.spec[k], T, spec_bytes(s), cudaMemcpyHostToDevice, cs); dT = st.spec[k++]; }
-	run_synth(s, ncomp, types, (const cplx*) dQ, (const cplx*) dS, (const cplx*) dT, st.spat[0], st.spat[1], st.spat[2], ltr);
-	double* outs[3] = {o0, o1, o2};
-	for (int c = 0; c < ncomp; c++) cudaMemcpyAsync(outs[c], st.spat[c], spat_bytes(s), cudaMemcpyDeviceToHost, cs);
-	shtb_cuda_ok(cudaStreamSynchronize(cs), "synthesis");
+	const HostChunks h = host_chunks(s);
+	if (!copy_resources(s, 2 * h.nch)) return;
+	cudaStream_t cs = s->comp_stream, xh = s->xfer_stream, xd = s->d2h_stream;
+	const cplx* hin[3] = {Q, S, T};
+	double* hout[3] = {o0, o1, o2};
+	double2* din[3] = {nullptr, nullptr, nullptr};
+	{
+		int k = 0;
+		for (int i = 0; i < 3; i++) if (hin[i]) din[i] = st.spec[k++];
+	}
+	const long sd = s->spec_dist, pd = s->spat_dist;
+	auto h2d = [&](int c) {
+		const int f0 = c * h.fpc, nf = std::min(h.fpc, h.B - f0);
+		const size_t b = sizeof(double2) * ((size_t)(nf - 1) * sd + s->nlm);
+		for (int i = 0; i < 3; i++)
+			if (hin[i]) cudaMemcpyAsync(din[i] + f0 * sd, reinterpret_cast<const double2*>(hin[i]) + f0 * sd, b,
+			                            cudaMemcpyHostToDevice, xh);
+		cudaEventRecord(s->xev[2 * c], xh);
+	};
+	auto compute = [&](int c) {
+		const int f0 = c * h.fpc, nf = std::min(h.fpc, h.B - f0);
+		cudaStreamWaitEvent(cs, s->xev[2 * c], 0);
+		s->batch = nf;
+		auto in = [&](int i) { return din[i] ? reinterpret_cast<const cplx*>(din[i] + f0 * sd) : (const cplx*) nullptr; };
+		run_synth(s, ncomp, types, in(0), in(1), in(2), st.spat[0] ? st.spat[0] + f0 * pd : nullptr,
+		          st.spat[1] ? st.spat[1] + f0 * pd : nullptr, st.spat[2] ? st.spat[2] + f0 * pd : nullptr, ltr);
+		s->batch = h.B;
+		cudaEventRecord(s->xev[2 * c + 1], cs);
+	};
+	auto d2h = [&](int c) {
+		const int f0 = c * h.fpc, nf = std::min(h.fpc, h.B - f0);
+		const size_t b = sizeof(double) * ((size_t)(nf - 1) * pd + s->nspat);
+		cudaStreamWaitEvent(xd, s->xev[2 * c + 1], 0);
+		for (int i = 0; i < ncomp; i++) cudaMemcpyAsync(hout[i] + f0 * pd, st.spat[i] + f0 * pd, b, cudaMemcpyDeviceToHost, xd);
+	};
+	h2d(0);
+	compute(0);
+	for (int c = 0; c < h.nch; c++) {
+		if (c + 1 < h.nch) { h2d(c + 1); compute(c + 1); }
+		d2h(c);
+	}
+	shtb_cuda_ok(cudaStreamSynchronize(xd), "synthesis");
 }
 
 void h_analys(shtns_cfg s, int ncomp, const int* types, const double* i0, const double* i1, const double* i2,
@@ -265,20 +348,48 @@ void h_analys(shtns_cfg s, int ncomp, const int* types, const double* i0, const 
 	if (!s || !s->grid_set) { shtb_set_error(1, "transform on a plan without grid"); return; }
 	Stage st;
 	if (!stage_alloc(s, ncomp, ncomp, st)) return;
-	cudaStream_t cs = s->comp_stream;
-	const double* ins[3] = {i0, i1, i2};
-	for (int c = 0; c < ncomp; c++) cudaMemcpyAsync(st.spat[c], ins[c], spat_bytes(s), cudaMemcpyHostToDevice, cs);
-	double2* outs_d[3] = {nullptr, nullptr, nullptr};
-	cplx* outs_h[3] = {nullptr, nullptr, nullptr};
-	int k = 0;
-	if (Qo) { outs_d[0] = st.spec[k++]; outs_h[0] = Qo; }
-	if (So) { outs_d[1] = st.spec[k++]; outs_h[1] = So; }
-	if (To) { outs_d[2] = st.spec[k++]; outs_h[2] = To; }
-	run_analys(s, ncomp, types, st.spat[0], st.spat[1], st.spat[2],
-	           (cplx*) outs_d[0], (cplx*) outs_d[1], (cplx*) outs_d[2], ltr);
-	for (int c = 0; c < 3; c++)
-		if (outs_h[c]) cudaMemcpyAsync(outs_h[c], outs_d[c], spec_bytes(s), cudaMemcpyDeviceToHost, cs);
-	shtb_cuda_ok(cudaStreamSynchronize(cs), "analysis");
+	const HostChunks h = host_chunks(s);
+	if (!copy_resources(s, 2 * h.nch)) return;
+	cudaStream_t cs = s->comp_stream, xh = s->xfer_stream, xd = s->d2h_stream;
+	const double* hin[3] = {i0, i1, i2};
+	cplx* hout[3] = {Qo, So, To};
+	double2* dout[3] = {nullptr, nullptr, nullptr};
+	{
+		int k = 0;
+		for (int i = 0; i < 3; i++) if (hout[i]) dout[i] = st.spec[k++];
+	}
+	const long sd = s->spec_dist, pd = s->spat_dist;
+	auto h2d = [&](int c) {
+		const int f0 = c * h.fpc, nf = std::min(h.fpc, h.B - f0);
+		const size_t b = sizeof(double) * ((size_t)(nf - 1) * pd + s->nspat);
+		for (int i = 0; i < ncomp; i++) cudaMemcpyAsync(st.spat[i] + f0 * pd, hin[i] + f0 * pd, b, cudaMemcpyHostToDevice, xh);
+		cudaEventRecord(s->xev[2 * c], xh);
+	};
+	auto compute = [&](int c) {
+		const int f0 = c * h.fpc, nf = std::min(h.fpc, h.B - f0);
+		cudaStreamWaitEvent(cs, s->xev[2 * c], 0);
+		s->batch = nf;
+		auto out = [&](int i) { return dout[i] ? reinterpret_cast<cplx*>(dout[i] + f0 * sd) : (cplx*) nullptr; };
+		run_analys(s, ncomp, types, st.spat[0] + f0 * pd, st.spat[1] ? st.spat[1] + f0 * pd : nullptr,
+		           st.spat[2] ? st.spat[2] + f0 * pd : nullptr, out(0), out(1), out(2), ltr);
+		s->batch = h.B;
+		cudaEventRecord(s->xev[2 * c + 1], cs);
+	};
+	auto d2h = [&](int c) {
+		const int f0 = c * h.fpc, nf = std::min(h.fpc, h.B - f0);
+		const size_t b = sizeof(double2) * ((size_t)(nf - 1) * sd + s->nlm);
+		cudaStreamWaitEvent(xd, s->xev[2 * c + 1], 0);
+		for (int i = 0; i < 3; i++)
+			if (hout[i]) cudaMemcpyAsync(reinterpret_cast<double2*>(hout[i]) + f0 * sd, dout[i] + f0 * sd, b,
+			                             cudaMemcpyDeviceToHost, xd);
+	};
+	h2d(0);
+	compute(0);
+	for (int c = 0; c < h.nch; c++) {
+		if (c + 1 < h.nch) { h2d(c + 1); compute(c + 1); }
+		d2h(c);
+	}
+	shtb_cuda_ok(cudaStreamSynchronize(xd), "analysis");
 }
 
 } // namespace

@@ -127,6 +127,8 @@ struct shtns_info {
 	double *d_alm; long *d_almoff;
 	void *d_loc; size_t loc_cap;
 	cudaStream_t comp_stream, xfer_stream;
+	cudaStream_t d2h_stream;             // host-pointer transforms: device->host copies (created on first use)
+	std::vector<cudaEvent_t> xev;        // host-pointer transforms: chunk events (created on first use)
 	int own_xfer;
 	int is_clone;
 	shtns_cfg base;                      // plan whose tables a clone shares (NULL for originals)

@@ -341,6 +341,9 @@ static void free_device(shtns_cfg s)
 	if (s->d_F) cudaFree(s->d_F);
 	if (s->d_stage) cudaFree(s->d_stage);
 	if (s->own_xfer && s->xfer_stream) cudaStreamDestroy(s->xfer_stream);
+	if (s->d2h_stream) cudaStreamDestroy(s->d2h_stream);
+	for (cudaEvent_t e : s->xev) cudaEventDestroy(e);
+	s->d2h_stream = nullptr; s->xev.clear();
 	s->d_x = s->d_x2 = s->d_s = s->d_sinv = s->d_w = nullptr;
 	s->d_c = s->d_xs = s->d_xa = nullptr;
 	s->d_stdt_lo = s->d_stdt_hi = s->d_van_lo = s->d_van_hi = s->d_l2 = nullptr;
@@ -673,6 +676,7 @@ extern "C" shtns_cfg cushtns_clone(shtns_cfg b, cudaStream_t compute_stream, cud
 	s->d_pvoff = nullptr; s->d_pt0 = nullptr; s->d_pkf = nullptr; s->ptab_kblocks = 0; s->ptab_ttiles = 0;
 	s->d_pbs = nullptr; s->pbs_cap = 0; s->d_pexp = nullptr; s->pexp_cap = 0;
 	s->xfer_stream = nullptr; s->own_xfer = 0;
+	s->d2h_stream = nullptr; s->xev.clear();
 	s->ev.clear(); s->ev_stage.clear(); s->ev_used = 0; s->timing = 0;
 	cushtns_set_streams(s, compute_stream, transfer_stream);
 	std::lock_guard<std::mutex> lk(g_plans_mu);
