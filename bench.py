@@ -767,9 +767,13 @@ def run_highdeg(args):
     from tests.common import rand_spec
     lib = capi.load()
     nf = args.fields if args.fields != NFIELDS else HD_NF
-    sh = shtns_b200.sht(HD_L)
-    sh.set_grid(HD_NLAT, HD_NPHI, flags=shtns_b200.sht_quick_init | shtns_b200.SHT_THETA_CONTIGUOUS, polar_opt=EPS)
-    q = torch.from_numpy(rand_spec(HD_L, HD_L, 1, 400, power=1.0, nfields=nf)).to(dev)
+    L = args.hd_lmax
+    nlat = HD_NLAT if L == HD_L else 3 * (L + 1) // 2 + (3 * (L + 1) // 2) % 2
+    nphi = 2 * nlat
+    digits = [int(x) for x in args.hd_digits.split(",")]
+    sh = shtns_b200.sht(L)
+    sh.set_grid(nlat, nphi, flags=shtns_b200.sht_quick_init | shtns_b200.SHT_THETA_CONTIGUOUS, polar_opt=EPS)
+    q = torch.from_numpy(rand_spec(L, L, 1, 400, power=1.0, nfields=nf)).to(dev)
     v = torch.empty((nf,) + sh.spat_shape, dtype=torch.float64, device=dev)
     r = torch.empty_like(q)
     ref = {}
@@ -826,7 +830,7 @@ def run_highdeg(args):
     forms = {"fp64": {"pair_ms": ms_pair, "synth_ms": ms_syn, "analys_ms": ms_ana,
                       "legendre_synth_ms": st[1], "legendre_analys_ms": st[4],
                       "pairs_per_s": nf / (ms_pair * 1e-3)}}
-    for ns in (5, 6, 7):
+    for ns in digits:
         sh.set_split(ns, form=0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -855,29 +859,30 @@ def run_highdeg(args):
                                "synth_rms_rel_err": es[1], "kernel_errors": int(sh.kernel_errors())}
     sh.set_split(0)
     clk = clocks.stop()
-    tm = np.zeros(HD_L + 1, dtype=np.int32)
+    tm = np.zeros(L + 1, dtype=np.int32)
     lib.shtns_b200_polar_rows(sh._cfg, tm.ctypes.data_as(C.c_void_p))
-    rows = HD_NLAT // 2 - tm
-    ks = (HD_L - np.arange(HD_L + 1)) // 2 + 1
+    rows = nlat // 2 - tm
+    ks = (L - np.arange(L + 1)) // 2 + 1
     flops = 8.0 * float((rows * ks).sum()) * nf
     peak = fp64_gemm_peak(torch, dev)
     hbm = measured_peaks().get("hbm_gbs", 6650.0)
-    t7 = forms["table7"]
+    t7 = forms["table%d" % max(digits)]
     # the table kernels stream the digit table once per launch (plus the
     # digit stacks of the other operand, mostly from L2, and the outputs)
     ach_s = t7["table_bytes"] / (t7["legendre_synth_ms"] * 1e-3) / 1e9
     ach_a = t7["table_bytes"] / (t7["legendre_analys_ms"] * 1e-3) / 1e9
     line = {
-        "metric": METRIC, "value": nf / (t7["pair_ms"] * 1e-3), "unit": HD_UNIT, "n_gpus": 1, "steps": steps,
+        "metric": METRIC, "value": nf / (t7["pair_ms"] * 1e-3),
+        "unit": "field-pairs/s (SH_to_spat+spat_to_SH, lmax=%d, %dx%d)" % (L, nlat, nphi), "n_gpus": 1, "steps": steps,
         "warmup": args.warmup, "ms_per_step": t7["pair_ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8 digits x7, exact int32 sums, f64 combine",
         "data": "synthetic (seeded N(0,1)/(l+1))",
-        "config": {"workload": "lmax4095_8fields", "lmax": HD_L, "nlat": HD_NLAT, "nphi": HD_NPHI, "fields": nf,
+        "config": {"workload": "lmax%d_%dfields" % (L, nf), "lmax": L, "nlat": nlat, "nphi": nphi, "fields": nf,
                    "polar_eps": EPS, "layout": "theta-contiguous",
-                   "form": "split precision: 7-digit INT8 table, synthesis + analysis"},
+                   "form": "split precision: %d-digit INT8 table, synthesis + analysis" % max(digits)},
         "split_speedup_vs_fp64": t7["speedup_vs_fp64"],
         "forms": forms,
-        "roofline": {"kernel": "ptab_synth_kernel / ptab_analys_kernel (7 digits)", "bound": "hbm",
+        "roofline": {"kernel": "ptab_kernel (synthesis / analysis, %d digits)" % max(digits), "bound": "hbm",
                      "achieved": ach_s, "achieved_analysis": ach_a, "peak": hbm, "unit": "GB/s",
                      "frac": ach_s / hbm, "frac_analysis": ach_a / hbm, "traffic": None,
                      "work_per_launch": f"{t7['table_bytes']:.4e} bytes of digit table",
@@ -1134,6 +1139,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision form of the qst step")
     ap.add_argument("--split-digits", type=int, default=7)
+    ap.add_argument("--hd-lmax", type=int, default=HD_L, help="highdeg workload: lmax (grid 3(lmax+1)/2 x 3(lmax+1))")
+    ap.add_argument("--hd-digits", default="5,6,7", help="highdeg workload: digit counts of the table form")
     ap.add_argument("--e2e-chunks", type=int, default=E2E_CHUNKS,
                     help="field chunks (streams) of the end-to-end step")
     ap.add_argument("--exchange", default="nccl", choices=["nccl", "fused"],

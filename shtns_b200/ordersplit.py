@@ -358,6 +358,11 @@ class FusedOrderSplit(OrderSplit):
         barrier, Legendre stage into / from the buffers, barrier, FFT stage
     (synthesis), or FFT, barrier, Legendre, barrier (analysis): the barriers
     order the writes of one rank's kernels before the reads of another's.
+    Each barrier first waits on the host for the rank's own work on torch's
+    current stream (the stream the stages are enqueued on), then meets the
+    other ranks: a rank's kernels, and so its peer stores, have completed
+    before any other rank passes the barrier and launches kernels that read
+    them, whatever the backend's barrier does with streams.
     Buffers are allocated and mapped by prepare(nfc), a collective call."""
 
     def __init__(self, plan, group=None, rank=None, world=None, costs=None, barrier=None):
@@ -369,6 +374,9 @@ class FusedOrderSplit(OrderSplit):
         self._barrier = barrier
 
     def barrier(self):
+        import torch
+        if torch.cuda.is_available():
+            torch.cuda.current_stream().synchronize()
         if self._barrier is not None:
             self._barrier()
         elif self.world > 1:
