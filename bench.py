@@ -705,14 +705,32 @@ def run_uneven(args):
     lib = capi.load()
     ms_field = timed(ub.pair_per_field, max(3, args.steps // 20))
     ms_bucket = timed(ub.pair_per_bucket, args.steps)
+    ub.group.set_option(4, 0)          # every launch of the group on one stream
+    ms_group1 = timed(ub.pair, args.steps)
+    ub.group.set_option(4, 1)          # per-plan launches concurrently on side streams (default)
     ms_group = timed(ub.pair, args.steps)
     ub.capture()
     torch.cuda.synchronize()
     clocks = ClockSampler(0)
     clocks.start()
     time.sleep(0.3)
-    ms_graph = timed(ub.replay, args.steps)
+    ms_graph_persistent = timed(ub.replay, args.steps)
+    ub.release_graph()
+    # each bucket's own kernels, the buckets concurrently on the group's side
+    # streams, captured as parallel branches of one graph
+    ub.group.set_option(5, 1)
+    ms_group_pp = timed(ub.pair, args.steps)
+    ub.capture()
+    torch.cuda.synchronize()
+    ms_graph_pp = timed(ub.replay, args.steps)
     clk = clocks.stop()
+    per_plan = ms_graph_pp < ms_graph_persistent
+    ms_graph = min(ms_graph_pp, ms_graph_persistent)
+    if not per_plan:
+        ub.release_graph()
+        ub.group.set_option(5, 0)
+        ub.capture()
+        torch.cuda.synchronize()
     n0 = lib.shtns_b200_launch_count()
     ub.pair()
     torch.cuda.synchronize()
@@ -728,10 +746,17 @@ def run_uneven(args):
         "config": {"workload": "uneven_lmax_256fields", "fields": nf,
                    "fields_per_lmax": dict(zip(map(str, ub.buckets), ub.count)),
                    "grids": {str(l): list(B.grid_for(l)) for l in ub.buckets}, "polar_eps": EPS,
-                   "layout": "theta-contiguous", "form": "plan group replayed from a CUDA graph"},
+                   "layout": "theta-contiguous",
+                   "form": "plan group replayed from a CUDA graph (%s)" % (
+                       "per-bucket kernels on concurrent graph branches" if per_plan else
+                       "one persistent Legendre launch")},
         "forms_fields_per_s": {"per_field_launches": nf / (ms_field * 1e-3),
                                "per_bucket_batched": nf / (ms_bucket * 1e-3),
+                               "group_eager_one_stream": nf / (ms_group1 * 1e-3),
                                "group_eager": nf / (ms_group * 1e-3),
+                               "group_cuda_graph_persistent_legendre": nf / (ms_graph_persistent * 1e-3),
+                               "group_eager_per_bucket_kernels_concurrent": nf / (ms_group_pp * 1e-3),
+                               "group_cuda_graph_per_bucket_kernels_concurrent": nf / (ms_graph_pp * 1e-3),
                                "group_cuda_graph": nf / (ms_graph * 1e-3)},
         "speedup_vs_per_field": ms_field / ms_graph,
         "autotune": tune["options"],

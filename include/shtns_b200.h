@@ -135,7 +135,14 @@ shtns_group shtns_b200_group_create(int nplans, shtns_cfg* plans);
 void shtns_b200_group_destroy(shtns_group);
 /* option 1: work order, 0 by decreasing cost (default), 1 plan/order/tile;
  * option 2: CTAs of the persistent launch per SM, 1-3 (0: 3);
- * option 3: checkpoint spacing of all plans, 8, 16 or 32.  Return 0 or -1. */
+ * option 3: checkpoint spacing of all plans, 8, 16 or 32;
+ * option 4: 1 (default) the per-plan prologue, FFT and epilogue launches run
+ * concurrently on side streams of the group (forked from and joined back
+ * into the first plan's stream by events), 0 all on the first plan's stream;
+ * option 5: Legendre stage, 0 (default) one persistent launch over all plans,
+ * 1 each plan's own launch (its tile shape or SIMT kernels), chained with
+ * the plan's prologue and FFT on its side stream (with option 4 = 1 the
+ * plans run concurrently).  Return 0 or -1. */
 int shtns_b200_group_set_option(shtns_group, int option, int value);
 void shtns_b200_group_synth(shtns_group, cplx **Qlm, double **Vr, const int *nfields, int ltr);
 void shtns_b200_group_analys(shtns_group, double **Vr, cplx **Qlm, const int *nfields, int ltr);

@@ -515,9 +515,12 @@ extern "C" void spat_to_SHqst_l(shtns_cfg s, double* Vr, double* Vt, double* Vp,
 // ---------------------------------------------------------------------------
 // Plan groups: scalar transforms of several plans (fields of different lmax,
 // each on its own grid) where the Legendre stage of all plans is one
-// persistent launch.  The per-plan prologue, FFT and epilogue launches and
-// the persistent launch all go to the stream of the first plan, so the whole
-// group is one stream sequence that a CUDA graph can capture.
+// persistent launch.  The per-plan prologue, FFT and epilogue launches fork
+// from the stream of the first plan onto side streams of the group (one per
+// plan) and join back before the persistent launch and at the end, all by
+// events, so the small kernels of different plans run concurrently and the
+// whole group stays one dependency graph rooted in the first plan's stream,
+// which a CUDA graph captures as parallel branches.
 // Work list of one direction (synthesis or analysis): per-plan parameters and
 // (plan, order, tile, column tile) items, in pinned host memory and on the
 // device.  The host copies are rewritten only after the stream has drained,
@@ -546,7 +549,11 @@ struct shtns_b200_group {
 	int order;                       // 0: work items by decreasing cost, 1: plan/order/tile order
 	int nsm;
 	int ctas_per_sm;                 // CTAs of the persistent launch per SM (1-3)
+	int concurrent;                  // 1: per-plan launches on side streams (default), 0: all on the first plan's stream
+	int leg_per_plan;                // 1: Legendre stage as each plan's own launch (concurrent); 0: one persistent launch
 	GroupWork dir[2];                // [0] analysis, [1] synthesis
+	std::vector<cudaStream_t> side;  // one per plan
+	std::vector<cudaEvent_t> ev;     // fork + one join event per plan
 };
 
 namespace {
@@ -555,6 +562,27 @@ bool group_ok(shtns_group g)
 {
 	if (!g || g->plans.empty()) { shtb_set_error(1, "empty plan group"); return false; }
 	return true;
+}
+
+// Runs launch(i, stream) for every plan i with fields: forked onto the
+// group's side streams after the work already on st, joined back into st.
+template <class F>
+void group_fork(shtns_group g, cudaStream_t st, const int* nfields, F launch)
+{
+	const int np = (int) g->plans.size();
+	if (!g->concurrent || (int) g->side.size() < np) {
+		for (int i = 0; i < np; i++) if (nfields[i] > 0) launch(i, st);
+		return;
+	}
+	cudaEventRecord(g->ev[0], st);
+	for (int i = 0; i < np; i++) {
+		if (nfields[i] <= 0) continue;
+		cudaStreamWaitEvent(g->side[i], g->ev[0], 0);
+		launch(i, g->side[i]);
+		cudaEventRecord(g->ev[1 + i], g->side[i]);
+	}
+	for (int i = 0; i < np; i++)
+		if (nfields[i] > 0) cudaStreamWaitEvent(st, g->ev[1 + i], 0);
 }
 
 // A list must change: refuse under stream capture (the host buffers would be
@@ -674,7 +702,21 @@ extern "C" shtns_group shtns_b200_group_create(int nplans, shtns_cfg* plans)
 	g->ckseg = seg;
 	g->order = 0;
 	g->ctas_per_sm = 3;
+	g->concurrent = 1;
 	cudaDeviceGetAttribute(&g->nsm, cudaDevAttrMultiProcessorCount, plans[0]->dev);
+	g->side.assign(nplans, nullptr);
+	g->ev.assign(nplans + 1, nullptr);
+	bool ok = true;
+	for (int i = 0; i < nplans && ok; i++) ok = cudaStreamCreateWithFlags(&g->side[i], cudaStreamNonBlocking) == cudaSuccess;
+	for (int i = 0; i <= nplans && ok; i++) ok = cudaEventCreateWithFlags(&g->ev[i], cudaEventDisableTiming) == cudaSuccess;
+	if (!ok) {
+		// fall back to the single stream
+		cudaGetLastError();
+		for (cudaStream_t x : g->side) if (x) cudaStreamDestroy(x);
+		for (cudaEvent_t e : g->ev) if (e) cudaEventDestroy(e);
+		g->side.clear(); g->ev.clear();
+		g->concurrent = 0;
+	}
 	return g;
 }
 
@@ -684,6 +726,8 @@ extern "C" void shtns_b200_group_destroy(shtns_group g)
 	if (!g->plans.empty()) cudaStreamSynchronize(g->plans[0]->comp_stream);
 	g->dir[0].release();
 	g->dir[1].release();
+	for (cudaStream_t x : g->side) if (x) cudaStreamDestroy(x);
+	for (cudaEvent_t e : g->ev) if (e) cudaEventDestroy(e);
 	delete g;
 }
 
@@ -692,6 +736,12 @@ extern "C" int shtns_b200_group_set_option(shtns_group g, int option, int value)
 	if (!g) return -1;
 	if (option == 1 && (value == 0 || value == 1)) { g->order = value; return 0; }
 	if (option == 2 && value >= 0 && value <= 3) { g->ctas_per_sm = value ? value : 3; return 0; }
+	if (option == 5 && (value == 0 || value == 1)) { g->leg_per_plan = value; return 0; }
+	if (option == 4 && (value == 0 || value == 1)) {
+		if (value && g->side.empty()) return -1;     // no side streams: single-stream form only
+		g->concurrent = value;
+		return 0;
+	}
 	if (option == 3 && (value == 8 || value == 16 || value == 32)) {
 		for (shtns_cfg s : g->plans)
 			if (s->ckseg != value && shtns_b200_set_option(s, 2, value) != 0) return -1;
@@ -714,22 +764,36 @@ extern "C" void shtns_b200_group_synth(shtns_group g, cplx** Qlm, double** Vr, c
 		if (!setup_job(s, jobs[i], 1, T_SCAL, std::min<int>(ltr, s->lmax))) return;
 		lp[i] = leg_params(s, jobs[i]);
 	}
+	if (g->leg_per_plan) {
+		// each plan's own Legendre launch (its tile shape or SIMT kernels):
+		// prologue, Legendre and FFT chained per plan on its side stream
+		group_fork(g, st, nfields, [&](int i, cudaStream_t x) {
+			PrepParams pp = prep_params(g->plans[i], jobs[i]);
+			pp.Q = reinterpret_cast<const double2*>(Qlm[i]);
+			launch_prep_synth(pp, x);
+			launch_leg_synth(lp[i], x);
+			FftParams fp = fft_params(g->plans[i], jobs[i]);
+			fp.spat[0] = Vr[i];
+			fp.vec2 = aligned16(Vr[i], Vr[i], Vr[i], g->plans[i]->spat_dist);
+			launch_fft_synth(fp, jobs[i].nfc, x);
+		});
+		check_launch("group synthesis launch");
+		return;
+	}
 	if (!group_work(g, lp, nfields, true)) return;
-	for (int i = 0; i < np; i++) {
-		if (nfields[i] <= 0) continue;
+	group_fork(g, st, nfields, [&](int i, cudaStream_t x) {
 		PrepParams pp = prep_params(g->plans[i], jobs[i]);
 		pp.Q = reinterpret_cast<const double2*>(Qlm[i]);
-		launch_prep_synth(pp, st);
-	}
+		launch_prep_synth(pp, x);
+	});
 	const GroupWork& W = g->dir[1];
 	launch_leg_multi(W.d_plist, W.d_work, W.nwork, W.d_counter, g->ckseg, true, g->nsm * g->ctas_per_sm, st);
-	for (int i = 0; i < np; i++) {
-		if (nfields[i] <= 0) continue;
+	group_fork(g, st, nfields, [&](int i, cudaStream_t x) {
 		FftParams fp = fft_params(g->plans[i], jobs[i]);
 		fp.spat[0] = Vr[i];
 		fp.vec2 = aligned16(Vr[i], Vr[i], Vr[i], g->plans[i]->spat_dist);
-		launch_fft_synth(fp, jobs[i].nfc, st);
-	}
+		launch_fft_synth(fp, jobs[i].nfc, x);
+	});
 	check_launch("group synthesis launch");
 }
 
@@ -746,22 +810,38 @@ extern "C" void shtns_b200_group_analys(shtns_group g, double** Vr, cplx** Qlm, 
 		if (!setup_job(s, jobs[i], 1, T_SCAL, std::min<int>(ltr, s->lmax))) return;
 		lp[i] = leg_params(s, jobs[i]);
 	}
+	if (g->leg_per_plan) {
+		group_fork(g, st, nfields, [&](int i, cudaStream_t x) {
+			shtns_cfg s = g->plans[i];
+			FftParams fp = fft_params(s, jobs[i]);
+			fp.spat_in[0] = Vr[i];
+			fp.vec2 = aligned16(Vr[i], Vr[i], Vr[i], s->spat_dist);
+			launch_fft_analys(fp, jobs[i].nfc, x);
+			int kmax_all = 0;
+			for (int im = 0; im <= jobs[i].mlim; im++)
+				kmax_all = std::max(kmax_all, (jobs[i].llim + jobs[i].vec_extra - im * s->mres) / 2 + 1);
+			launch_leg_analys(lp[i], kmax_all, x);
+			PrepParams pp = prep_params(s, jobs[i]);
+			pp.Qo = reinterpret_cast<double2*>(Qlm[i]);
+			launch_post_analys_m(pp, s->mmax, x);
+		});
+		check_launch("group analysis launch");
+		return;
+	}
 	if (!group_work(g, lp, nfields, false)) return;
-	for (int i = 0; i < np; i++) {
-		if (nfields[i] <= 0) continue;
+	group_fork(g, st, nfields, [&](int i, cudaStream_t x) {
 		FftParams fp = fft_params(g->plans[i], jobs[i]);
 		fp.spat_in[0] = Vr[i];
 		fp.vec2 = aligned16(Vr[i], Vr[i], Vr[i], g->plans[i]->spat_dist);
-		launch_fft_analys(fp, jobs[i].nfc, st);
-	}
+		launch_fft_analys(fp, jobs[i].nfc, x);
+	});
 	const GroupWork& W = g->dir[0];
 	launch_leg_multi(W.d_plist, W.d_work, W.nwork, W.d_counter, g->ckseg, false, g->nsm * g->ctas_per_sm, st);
-	for (int i = 0; i < np; i++) {
-		if (nfields[i] <= 0) continue;
+	group_fork(g, st, nfields, [&](int i, cudaStream_t x) {
 		PrepParams pp = prep_params(g->plans[i], jobs[i]);
 		pp.Qo = reinterpret_cast<double2*>(Qlm[i]);
-		launch_post_analys_m(pp, g->plans[i]->mmax, st);
-	}
+		launch_post_analys_m(pp, g->plans[i]->mmax, x);
+	});
 	check_launch("group analysis launch");
 }
 

@@ -108,6 +108,44 @@ def test_graph_replay(small):
     ub.release_graph()
 
 
+@pytest.mark.parametrize("concurrent", [0, 1])
+def test_group_per_plan_legendre_form(small, concurrent):
+    """Group option 5 = 1 (each bucket's own Legendre kernels, chained with its
+    prologue and FFT) with the side streams on or off (option 4): the same
+    results as the persistent form, eagerly and replayed from a CUDA graph."""
+    ub = small
+    ub.group.set_option(5, 0)
+    ub.pair()
+    torch.cuda.synchronize()
+    V, R = [v.clone() for v in ub.V], [r.clone() for r in ub.R]
+    ub.group.set_option(4, concurrent)
+    ub.group.set_option(5, 1)
+    try:
+        for v in ub.V:
+            v.zero_()
+        ub.pair()
+        torch.cuda.synchronize()
+        for a, b in zip(V, ub.V):
+            assert float((a - b).abs().max() / a.abs().max()) < 1e-14
+        for a, b in zip(R, ub.R):
+            assert float((a - b).abs().max() / a.abs().max()) < 1e-14
+        for v in ub.V:
+            v.zero_()
+        for r in ub.R:
+            r.zero_()
+        ub.capture()
+        ub.replay()
+        torch.cuda.synchronize()
+        for a, b in zip(V, ub.V):
+            assert float((a - b).abs().max() / a.abs().max()) < 1e-14
+        for a, b in zip(R, ub.R):
+            assert float((a - b).abs().max() / a.abs().max()) < 1e-14
+        ub.release_graph()
+    finally:
+        ub.group.set_option(5, 0)
+        ub.group.set_option(4, 1)
+
+
 def test_autotune_options_agree(small, tmp_path):
     from shtns_b200 import batch as B
     ub = small
