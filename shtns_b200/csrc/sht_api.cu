@@ -131,6 +131,9 @@ FftParams fft_params(shtns_cfg s, const Job& j, int nrows)
 	// generic kernels need two buffers
 	p.generic = (s->fft_generic == 1) ? (fft_smem_bytes(s->nphi, 1) <= 227 * 1024 ? 1 : 0) : s->fft_generic;
 	p.extra_tx = s->fft_extra_tx;
+	p.tw1 = s->d_tw4;
+	p.tw2 = s->d_tw4 ? s->d_tw4 + 96 : nullptr;
+	p.scratch = nullptr;
 	return p;
 }
 
@@ -190,6 +193,18 @@ void run_analys(shtns_cfg s, int ncomp, const int* types, const double* i0, cons
 	FftParams fp = fft_params(s, j);
 	fp.spat_in[0] = i0; fp.spat_in[1] = i1; fp.spat_in[2] = i2;
 	fp.vec2 = aligned16(i0, i1, i2, s->spat_dist);
+	if (s->d_tw4 && !s->phi_contiguous && fp.vec2 && s->fft_generic == 0) {
+		// the four-step FFT analysis of nphi = 12288 needs a grid per field-component of scratch
+		// (without room for it the direct kernels run instead)
+		const size_t b = sizeof(double) * (size_t) j.nfc * s->nphi * s->nlat;
+		if (s->fscr_cap < b) {
+			if (s->d_fscr) cudaFree(s->d_fscr);
+			s->d_fscr = nullptr; s->fscr_cap = 0;
+			if (cudaMalloc(reinterpret_cast<void**>(&s->d_fscr), b) == cudaSuccess) s->fscr_cap = b;
+			else { cudaGetLastError(); s->d_fscr = nullptr; }
+		}
+		fp.scratch = s->d_fscr;
+	}
 	shtb_stage_begin(s, 3);
 	launch_fft_analys(fp, j.nfc, s->comp_stream);
 	shtb_stage_end(s);

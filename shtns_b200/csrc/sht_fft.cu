@@ -211,7 +211,7 @@ __device__ __forceinline__ double2* fft_run(double2* X, double2* Y, int N, int S
 __device__ __forceinline__ int seq_len(int N, int S)
 {
 	const int a = N + (N >> 3);
-	return a + (((8 / S) - a) & 7);
+	return a + (((S >= 8 ? 1 : 8 / S) - a) & 7);
 }
 
 // Synthesis: F[fc][m][theta] (m <= mlim) -> spatial field-component fc.
@@ -366,11 +366,16 @@ template <> struct NphiPlan<1536> { using L = RadixList<8, 8, 8, 3>; };
 template <> struct NphiPlan<3072> { using L = RadixList<8, 8, 4, 4, 3>; };
 template <> struct NphiPlan<6144> { using L = RadixList<8, 8, 8, 4, 3>; };
 template <> struct NphiPlan<12288> { using L = RadixList<8, 8, 8, 8, 3>; };
+template <> struct NphiPlan<96>  { using L = RadixList<8, 4, 3>; };
+template <> struct NphiPlan<128> { using L = RadixList<8, 4, 4>; };
 
 template <int N, int S>
 struct Geo {
 	static constexpr int A = N + (N >> 3);
-	static constexpr int SEQ = A + (((8 / S) - A) & 7);
+	// sequence stride 8/S mod 8 (16-byte units) for S <= 8, 1 mod 8 beyond, so
+	// that the 8 lanes of a 16-byte access phase, on consecutive sequences,
+	// hit distinct banks
+	static constexpr int SEQ = A + (((S >= 8 ? 1 : 8 / S) - A) & 7);
 	// one radix-8 butterfly per thread, at most 768 threads (two or more per thread beyond)
 	static constexpr int T = (S * N / 8 <= 768) ? S * N / 8 : 768;
 	static __device__ __forceinline__ int at(int s, int i) { return s * SEQ + i + (i >> 3); }
@@ -610,6 +615,143 @@ __global__ void __launch_bounds__(Geo<N, S>::T) fft3_analys_kernel(FftParams p)
 		else { o[0] = fa; o[1] = fb; }
 	};
 	fused_fft<N, S, 3>(smem, p.tw, -1, ld, st, NoHook{}, threadIdx.x, typename NphiPlan<N>::L{});
+}
+
+// ---------------------------------------------------------------------------
+// Four-step FFT for nphi = N1 N2 = 96 x 128 = 12288 (theta-contiguous grids).
+// With j = j1 + N1 j2 and k = k2 + N2 k1,
+//   exp(s 2 pi i j k / N) = w_N^(j1 k2) w_N1^(j1 k1) w_N2^(j2 k2),
+// so a length-N transform is N2 transforms of length N1 (over k1), a twiddle
+// w_N^(j1 k2), and N1 transforms of length N2 (over k2).  Each CTA runs the
+// short transforms of FS_S latitude pairs (one 256-byte run of a grid row per
+// element), so its loads and stores are coalesced rows and many CTAs share an
+// SM, where the one-pass kernel of this length holds one latitude pair per SM.
+// The intermediate lives in grid row j = N1 k2 + j1: the synthesis works in
+// place in its output grid (the second step reads and rewrites exactly the
+// rows j1 + N1 k2 of its j1), the analysis writes it to a scratch grid.
+// The analysis' second step takes k2 and N2 - k2 in one CTA, so that each
+// order's pair (z_m, z_{N-m}) is at hand to separate the two real spectra.
+constexpr int FS_S = 16;      // latitude pairs per CTA
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(Geo<N1, FS_S>::T) fft_fs_synth1_kernel(FftParams p)
+{
+	extern __shared__ double2 smem[];
+	constexpr int N = N1 * N2;
+	const int fc = blockIdx.z, k2 = blockIdx.y;
+	const int lat0 = blockIdx.x * 2 * FS_S;
+	const double2* __restrict__ Ff = p.F + (long)fc * p.fstride;
+	const int ml = p.mlim, nlat = p.nlat;
+	auto ld = [&](int s, int k1) -> double2 {
+		const int ra = lat0 + 2 * s;
+		const int j = k2 + N2 * k1;                 // frequency index
+		const int k = (j <= ml) ? j : ((j >= N - ml) ? N - j : -1);
+		if (k < 0 || ra >= nlat) return make_double2(0.0, 0.0);
+		double2 a = __ldg(Ff + (long)k * nlat + ra), b = __ldg(Ff + (long)k * nlat + ra + 1);
+		if (k == 0) { a.y = 0.0; b.y = 0.0; }
+		return (j <= ml) ? make_double2(a.x - b.y, a.y + b.x) : make_double2(a.x + b.y, b.x - a.y);
+	};
+	const int c = fc / p.nf;
+	double* out = (c == 0 ? p.spat[0] : c == 1 ? p.spat[1] : p.spat[2]) + (long)(fc - c * p.nf) * p.spat_dist;
+	auto st = [&](int s, int j1, double2 z) {
+		const int row = lat0 + 2 * s;
+		if (row >= nlat) return;
+		z = cmul(z, __ldg(p.tw + (j1 * k2) % N));
+		*reinterpret_cast<double2*>(out + (long)(N1 * k2 + j1) * nlat + row) = z;
+	};
+	fused_fft<N1, FS_S, 1>(smem, p.tw1, +1, ld, st, NoHook{}, threadIdx.x, typename NphiPlan<N1>::L{});
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(Geo<N2, FS_S>::T) fft_fs_synth2_kernel(FftParams p)
+{
+	extern __shared__ double2 smem[];
+	const int fc = blockIdx.z, j1 = blockIdx.y;
+	const int lat0 = blockIdx.x * 2 * FS_S;
+	const int nlat = p.nlat;
+	const int c = fc / p.nf;
+	double* out = (c == 0 ? p.spat[0] : c == 1 ? p.spat[1] : p.spat[2]) + (long)(fc - c * p.nf) * p.spat_dist;
+	auto ld = [&](int s, int k2) -> double2 {
+		const int row = lat0 + 2 * s;
+		if (row >= nlat) return make_double2(0.0, 0.0);
+		return *reinterpret_cast<const double2*>(out + (long)(N1 * k2 + j1) * nlat + row);
+	};
+	auto st = [&](int s, int j2, double2 z) {
+		const int row = lat0 + 2 * s;
+		if (row >= nlat) return;
+		*reinterpret_cast<double2*>(out + (long)(j1 + N1 * j2) * nlat + row) = z;
+	};
+	fused_fft<N2, FS_S, 1>(smem, p.tw2, +1, ld, st, NoHook{}, threadIdx.x, typename NphiPlan<N2>::L{});
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(Geo<N2, FS_S>::T) fft_fs_analys1_kernel(FftParams p)
+{
+	extern __shared__ double2 smem[];
+	constexpr int N = N1 * N2;
+	const int fc = blockIdx.z, j1 = blockIdx.y;
+	const int lat0 = blockIdx.x * 2 * FS_S;
+	const int nlat = p.nlat;
+	const int c = fc / p.nf;
+	const double* in = (c == 0 ? p.spat_in[0] : c == 1 ? p.spat_in[1] : p.spat_in[2]) + (long)(fc - c * p.nf) * p.spat_dist;
+	double* scr = p.scratch + (long)fc * N * nlat;
+	auto ld = [&](int s, int j2) -> double2 {
+		const int row = lat0 + 2 * s;
+		if (row >= nlat) return make_double2(0.0, 0.0);
+		return __ldg(reinterpret_cast<const double2*>(in + (long)(j1 + N1 * j2) * nlat + row));
+	};
+	auto st = [&](int s, int k2, double2 z) {
+		const int row = lat0 + 2 * s;
+		if (row >= nlat) return;
+		double2 w = __ldg(p.tw + (j1 * k2) % N);
+		w.y = -w.y;
+		*reinterpret_cast<double2*>(scr + (long)(N1 * k2 + j1) * nlat + row) = cmul(z, w);
+	};
+	fused_fft<N2, FS_S, 1>(smem, p.tw2, -1, ld, st, NoHook{}, threadIdx.x, typename NphiPlan<N2>::L{});
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(Geo<N1, 2 * FS_S>::T) fft_fs_analys2_kernel(FftParams p)
+{
+	extern __shared__ double2 smem[];
+	using G = Geo<N1, 2 * FS_S>;
+	constexpr int N = N1 * N2;
+	const int fc = blockIdx.z, ka = blockIdx.y;          // ka = 0 .. N2/2
+	const int kb = (N2 - ka) % N2;                        // partner k2 (ka for 0 and N2/2)
+	const int lat0 = blockIdx.x * 2 * FS_S;
+	const int nlat = p.nlat, ml = p.mlim;
+	const double* scr = p.scratch + (long)fc * N * nlat;
+	// sequences s < FS_S: k2 = ka, latitude pair s; s >= FS_S: k2 = kb, pair s - FS_S
+	auto ld = [&](int s, int j1) -> double2 {
+		const int pr = s % FS_S, k2 = (s < FS_S) ? ka : kb;
+		const int row = lat0 + 2 * pr;
+		if (row >= nlat) return make_double2(0.0, 0.0);
+		return *reinterpret_cast<const double2*>(scr + (long)(N1 * k2 + j1) * nlat + row);
+	};
+	NoHook no;
+	fused_fft<N1, 2 * FS_S, 0>(smem, p.tw1, -1, ld, no, NoHook{}, threadIdx.x, typename NphiPlan<N1>::L{});
+	// X[at(s, k1)] = z_k, k = k2(s) + N2 k1.  Partner z_{N-k}: for k2 = 0 at
+	// (same sequence, (N1 - k1) % N1), else at (other k2, N1 - 1 - k1).
+	double2* Ff = p.F + (long)fc * p.fstride;
+	const double sc = 0.5 / N;
+	const bool self = (ka == kb);
+	const int nseq = self ? FS_S : 2 * FS_S;
+	for (int e = threadIdx.x; e < nseq * N1; e += G::T) {
+		const int s = e / N1, k1 = e - s * N1;
+		const int pr = s % FS_S, k2 = (s < FS_S) ? ka : kb;
+		const int k = k2 + N2 * k1;
+		const int ra = lat0 + 2 * pr;
+		if (k > ml || ra >= nlat) continue;
+		int sp, kp;
+		if (k2 == 0) { sp = s; kp = (N1 - k1) % N1; }
+		else { sp = self ? s : (s < FS_S ? s + FS_S : s - FS_S); kp = N1 - 1 - k1; }
+		const double2 z = smem[G::at(s, k1)], w = smem[G::at(sp, kp)];
+		const double2 fa = make_double2(sc * (z.x + w.x), sc * (z.y - w.y));
+		const double2 fb = make_double2(sc * (z.y + w.y), -sc * (z.x - w.x));
+		double2* o = Ff + (long)k * nlat + ra;
+		asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};"
+		             :: "l"(o), "d"(fa.x), "d"(fa.y), "d"(fb.x), "d"(fb.y) : "memory");
+	}
 }
 
 // ---------------------------------------------------------------------------
@@ -1018,8 +1160,38 @@ bool launch_fft4_n(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 	}
 }
 
+// four-step path: nphi = 12288 on theta-contiguous grids with 16-byte
+// aligned latitude pairs and (analysis) a scratch grid; false otherwise
+bool launch_fourstep(const FftParams& p, int nfc, cudaStream_t st, bool synth)
+{
+	constexpr int N1 = 96, N2 = 128;
+	if (p.N != N1 * N2 || p.phi_contiguous || !p.vec2 || !p.tw1 || p.generic != 0 || (!synth && !p.scratch)) return false;
+	if (p.nlat % 2 || ((uintptr_t) p.F & 31)) return false;
+	using G1 = Geo<N1, FS_S>;
+	using G2 = Geo<N2, FS_S>;
+	using G3 = Geo<N1, 2 * FS_S>;
+	const size_t s1 = sizeof(double2) * (size_t) FS_S * G1::SEQ, s2 = sizeof(double2) * (size_t) FS_S * G2::SEQ;
+	const size_t s3 = sizeof(double2) * (size_t)(2 * FS_S) * G3::SEQ;
+	static bool attr = false;
+	if (!attr) {
+		cudaFuncSetAttribute(fft_fs_analys2_kernel<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) s3);
+		attr = true;
+	}
+	const int nlb = (p.nlat + 2 * FS_S - 1) / (2 * FS_S);
+	if (synth) {
+		fft_fs_synth1_kernel<N1, N2><<<dim3(nlb, N2, nfc), G1::T, s1, st>>>(p);
+		fft_fs_synth2_kernel<N1, N2><<<dim3(nlb, N1, nfc), G2::T, s2, st>>>(p);
+	} else {
+		fft_fs_analys1_kernel<N1, N2><<<dim3(nlb, N1, nfc), G2::T, s2, st>>>(p);
+		fft_fs_analys2_kernel<N1, N2><<<dim3(nlb, N2 / 2 + 1, nfc), G3::T, s3, st>>>(p);
+	}
+	shtb_count_launch();         // the second of the two launches is counted by the caller
+	return true;
+}
+
 bool launch_fused(const FftParams& p, int nfc, cudaStream_t st, bool synth)
 {
+	if (launch_fourstep(p, nfc, st, synth)) return true;
 	if (p.generic == 0 || p.generic == 3) {
 		bool done = false;
 		switch (p.N) {
@@ -1085,7 +1257,7 @@ void set_fused_limits()
 static int seq_len_host(int N, int S)
 {
 	const int a = N + (N >> 3);
-	return a + (((8 / S) - a) & 7);
+	return a + (((S >= 8 ? 1 : 8 / S) - a) & 7);
 }
 
 int fft_threads(int N, int S, unsigned long long rcode, int nradix)

@@ -89,6 +89,8 @@ struct shtns_info {
 	double *d_stdt_lo, *d_stdt_hi, *d_van_lo, *d_van_hi, *d_l2;
 	double2 *d_ck;                      // checkpoints (Y_k, Y_k+1), [segment][north row]
 	double2 *d_tw;                       // exp(+2 pi i j / nphi), j < nphi
+	double2 *d_tw4;                      // nphi = 12288: four-step factor tables (96 + 128 entries)
+	double *d_fscr; size_t fscr_cap;     // four-step FFT analysis scratch (grow on demand)
 	MTables mt;
 	int *d_mint;                         // backing store of mt
 	size_t table_bytes;
@@ -216,6 +218,8 @@ struct FftParams {
 	int extra_tx;                        // test hook: extra bytes expected per prefetched tile (0)
 	int generic;                         // 0 automatic, 1 generic mixed-radix kernels, 2 fused kernels without prefetch,
 	                                     // 3 prefetched loads with per-thread stores
+	const double2 *tw1, *tw2;            // four-step FFT (nphi = 96 x 128): exp(+2 pi i j / 96), exp(+2 pi i j / 128)
+	double *scratch;                     // four-step analysis: a grid per field-component (null: other kernels)
 };
 
 // ---- one transform call: its shape and the kernels' parameter blocks (sht_api.cu) ----

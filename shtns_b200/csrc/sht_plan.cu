@@ -330,7 +330,7 @@ static void free_device(shtns_cfg s)
 	if (s->is_clone) {
 		// clones own only their work buffers and streams
 	} else {
-		void* ptrs[] = {s->d_x, s->d_c, s->d_ck, s->d_tw, s->d_mint};
+		void* ptrs[] = {s->d_x, s->d_c, s->d_ck, s->d_tw, s->d_mint, s->d_tw4};
 		for (void* p : ptrs) if (p) cudaFree(p);
 	}
 	free_split(s);
@@ -340,6 +340,8 @@ static void free_device(shtns_cfg s)
 	if (s->d_qq) cudaFree(s->d_qq);
 	if (s->d_F) cudaFree(s->d_F);
 	if (s->d_stage) cudaFree(s->d_stage);
+	if (s->d_fscr) cudaFree(s->d_fscr);
+	s->d_fscr = nullptr; s->fscr_cap = 0; s->d_tw4 = nullptr;
 	if (s->own_xfer && s->xfer_stream) cudaStreamDestroy(s->xfer_stream);
 	if (s->d2h_stream) cudaStreamDestroy(s->d2h_stream);
 	for (cudaEvent_t e : s->xev) cudaEventDestroy(e);
@@ -399,6 +401,20 @@ static int init_device(shtns_cfg s)
 	ok &= ok && shtb_cuda_ok(cudaMalloc(&s->d_mint, sizeof(int) * mi.size()), "order tables");
 	ok &= ok && shtb_cuda_ok(cudaMalloc(&s->d_tw, sizeof(double2) * tw.size()), "twiddles");
 	ok &= ok && shtb_cuda_ok(cudaMalloc(&s->d_ck, sizeof(double2) * ck_elems), "checkpoints");
+	if (ok && s->nphi == 12288) {
+		// factor tables of the four-step FFT, 12288 = 96 x 128
+		std::vector<double2> t4(96 + 128);
+		for (int j = 0; j < 96; j++) {
+			long double a = 2.0L * 3.14159265358979323846264338327950288L * j / 96.0L;
+			t4[j] = make_double2((double) std::cos(a), (double) std::sin(a));
+		}
+		for (int j = 0; j < 128; j++) {
+			long double a = 2.0L * 3.14159265358979323846264338327950288L * j / 128.0L;
+			t4[96 + j] = make_double2((double) std::cos(a), (double) std::sin(a));
+		}
+		ok &= shtb_cuda_ok(cudaMalloc(&s->d_tw4, sizeof(double2) * t4.size()), "FFT factor tables");
+		if (ok) cudaMemcpy(s->d_tw4, t4.data(), sizeof(double2) * t4.size(), cudaMemcpyHostToDevice);
+	}
 	if (!ok) { free_device(s); return -1; }
 	s->table_bytes = sizeof(double) * (g.size() + nc) + sizeof(int) * mi.size() + sizeof(double2) * (tw.size() + ck_elems);
 	cudaMemcpy(s->d_x, g.data(), sizeof(double) * g.size(), cudaMemcpyHostToDevice);
@@ -669,6 +685,7 @@ extern "C" shtns_cfg cushtns_clone(shtns_cfg b, cudaStream_t compute_stream, cud
 	s->base->nclones++;
 	s->d_qq = nullptr; s->qq_cap = 0; s->d_F = nullptr; s->F_cap = 0;
 	s->d_stage = nullptr; s->stage_cap = 0;
+	s->d_fscr = nullptr; s->fscr_cap = 0;
 	s->d_alm = nullptr; s->d_almoff = nullptr; s->d_loc = nullptr; s->loc_cap = 0;
 	s->d_yexp = nullptr; s->d_boff = nullptr; s->split_chunks = 0; s->split_kc = 0;
 	s->d_bsl = nullptr; s->bsl_cap = 0; s->d_bexp = nullptr; s->bexp_cap = 0; s->d_split_err = nullptr;
