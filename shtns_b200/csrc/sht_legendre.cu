@@ -18,6 +18,7 @@
 #include "sht_internal.h"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace {
 
@@ -433,20 +434,40 @@ __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int t
 			__syncthreads();
 			if (k0 + LG_BK < nk) load_b(k0 + LG_BK);
 			const int kv = nk - k0;                      // steps of this chunk below nk
-			#pragma unroll
-			for (int kk = 0; kk < LG_BK; kk += 4) {
-				if (kk >= kv) break;                      // rows of Bs beyond nk are zero
-				double a[4], b[2];
+			// P0, P1: row-fragment pairs (0, 1) and (2, 3) computed; NJ column
+			// fragments.  The choice is made once per warp with a branch: an MMA
+			// switched off by a predicate still occupies the tensor pipe.
+			auto mma_chunk = [&](auto P0, auto P1, auto NJ) {
 				#pragma unroll
-				for (int i = 0; i < 4; i++) a[i] = As[kk + (lane & 3)][wm * 32 + i * 8 + (lane >> 2)];
-				#pragma unroll
-				for (int j = 0; j < 2; j++) b[j] = Bs[kk + (lane & 3)][wn * 16 + j * 8 + (lane >> 2)];
-				// fragment pairs (i, i + 1): computed when either carries results
-				#pragma unroll
-				for (int j = 0; j < 2; j++)
+				for (int kk = 0; kk < LG_BK; kk += 4) {
+					if (kk >= kv) break;                  // rows of Bs beyond nk are zero
+					double a[4], b[2];
 					#pragma unroll
-					for (int i = 0; i < 4; i += 2)
-						if (i + 1 >= ri0 && i < ri1 && j < cj1) dmma16(acc[i][j], acc[i + 1][j], a[i], a[i + 1], b[j]);
+					for (int i = 0; i < 4; i++)
+						if ((i < 2 && P0.value) || (i >= 2 && P1.value)) a[i] = As[kk + (lane & 3)][wm * 32 + i * 8 + (lane >> 2)];
+					#pragma unroll
+					for (int j = 0; j < NJ.value; j++) b[j] = Bs[kk + (lane & 3)][wn * 16 + j * 8 + (lane >> 2)];
+					#pragma unroll
+					for (int j = 0; j < NJ.value; j++) {
+						if constexpr (P0.value) dmma16(acc[0][j], acc[1][j], a[0], a[1], b[j]);
+						if constexpr (P1.value) dmma16(acc[2][j], acc[3][j], a[2], a[3], b[j]);
+					}
+				}
+			};
+			// fragment pairs (i, i + 1) carry results when either row fragment does
+			const bool p0 = ri0 <= 1 && ri1 > 0, p1 = ri0 <= 3 && ri1 > 2;
+			using T = std::true_type;
+			using F = std::false_type;
+			using J1 = std::integral_constant<int, 1>;
+			using J2 = std::integral_constant<int, 2>;
+			if (cj1 == 2) {
+				if (p0 && p1) mma_chunk(T{}, T{}, J2{});
+				else if (p0) mma_chunk(T{}, F{}, J2{});
+				else if (p1) mma_chunk(F{}, T{}, J2{});
+			} else if (cj1 == 1) {
+				if (p0 && p1) mma_chunk(T{}, T{}, J1{});
+				else if (p0) mma_chunk(T{}, F{}, J1{});
+				else if (p1) mma_chunk(F{}, T{}, J1{});
 			}
 			__syncthreads();
 		}
@@ -628,18 +649,31 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 		}
 		__syncthreads();
 		if (tt0 + LG_BK < p.nlat_2) load_next(tt0 + LG_BK);
-		#pragma unroll
-		for (int kk = 0; kk < LG_BK; kk += 4) {
-			double a[4], b[2];
+		// NP row-fragment pairs and NJ column fragments, chosen once per warp
+		// with a branch (a predicated-off MMA still occupies the tensor pipe)
+		auto mma_chunk = [&](auto NP, auto NJ) {
 			#pragma unroll
-			for (int i = 0; i < 4; i++) a[i] = As[wm * 32 + i * 8 + (lane >> 2)][kk + (lane & 3)];
-			#pragma unroll
-			for (int j = 0; j < 2; j++) b[j] = Bs[kk + (lane & 3)][(wn * 16 + j * 8 + (lane >> 2)) ^ (2 * ((kk >> 2) & 3))];
-			#pragma unroll
-			for (int j = 0; j < 2; j++)
+			for (int kk = 0; kk < LG_BK; kk += 4) {
+				double a[4], b[2];
 				#pragma unroll
-				for (int i = 0; i < 4; i += 2)
-					if (i < ki1 && j < cj1) dmma16(acc[i][j], acc[i + 1][j], a[i], a[i + 1], b[j]);
+				for (int i = 0; i < 2 * NP.value; i++) a[i] = As[wm * 32 + i * 8 + (lane >> 2)][kk + (lane & 3)];
+				#pragma unroll
+				for (int j = 0; j < NJ.value; j++)
+					b[j] = Bs[kk + (lane & 3)][(wn * 16 + j * 8 + (lane >> 2)) ^ (2 * ((kk >> 2) & 3))];
+				#pragma unroll
+				for (int j = 0; j < NJ.value; j++)
+					#pragma unroll
+					for (int i = 0; i < 2 * NP.value; i += 2) dmma16(acc[i][j], acc[i + 1][j], a[i], a[i + 1], b[j]);
+			}
+		};
+		using N1 = std::integral_constant<int, 1>;
+		using N2 = std::integral_constant<int, 2>;
+		if (ki1 > 2) {
+			if (cj1 == 2) mma_chunk(N2{}, N2{});
+			else if (cj1 == 1) mma_chunk(N2{}, N1{});
+		} else if (ki1 > 0) {
+			if (cj1 == 2) mma_chunk(N1{}, N2{});
+			else if (cj1 == 1) mma_chunk(N1{}, N1{});
 		}
 		__syncthreads();
 	}
