@@ -33,6 +33,17 @@ __device__ __forceinline__ void dmma16(double (&c0)[2], double (&c1)[2], double 
 	             : "+d"(c0[0]), "+d"(c0[1]), "+d"(c1[0]), "+d"(c1[1]) : "d"(a0), "d"(a1), "d"(b));
 }
 
+// Read-only load that does not allocate in L1: the streamed operands (F rows,
+// coefficient rows, checkpoints) are read once per CTA, and keeping them out
+// of L1 leaves it to the small per-row tables that every chunk's staging reads
+// (recurrence coefficients, weights, cos and 1/sin of the latitudes).
+__device__ __forceinline__ double2 ldg_stream(const double2* q)
+{
+	double2 v;
+	asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(q));
+	return v;
+}
+
 
 
 // ---------------------------------------------------------------------------
@@ -395,14 +406,14 @@ __device__ __forceinline__ void leg_synth_tile(const LegParams& p, int im, int t
 				const int e = tid + u * LG_THREADS;
 				const int kk = e / (BN / 2), cc2 = (e - kk * (BN / 2)) * 2;
 				const int k = k0 + kk, col = c0 + cc2;
-				bn[u] = (k < nk && col < p.ncol) ? __ldg(reinterpret_cast<const double2*>(qrow + (long)k * p.ncol + col))
+				bn[u] = (k < nk && col < p.ncol) ? ldg_stream(reinterpret_cast<const double2*>(qrow + (long)k * p.ncol + col))
 				                                 : make_double2(0.0, 0.0);
 			}
 			#pragma unroll
 			for (int u = 0; u < SPT; u++) {
 				const int sg = gj + u * GPR;
 				const int ks = k0 + sg * SEG;
-				ckn[u] = (sg < NSEGC && gen && ks < nk) ? __ldg(ckm + (long)(ks / SEG) * p.nlat_2 + tg)
+				ckn[u] = (sg < NSEGC && gen && ks < nk) ? ldg_stream(ckm + (long)(ks / SEG) * p.nlat_2 + tg)
 				                                       : make_double2(0.0, 0.0);
 			}
 		};
@@ -572,11 +583,11 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 				const int rs = p.nlat - 1 - rn;
 				if constexpr (!RB) {
 					const double2* Ff = p.F + (long)fc * p.fstride + (long)im * p.nlat;
-					fnn[u] = __ldg(Ff + rn);
-					fsn[u] = __ldg(Ff + rs);
+					fnn[u] = ldg_stream(Ff + rn);
+					fsn[u] = ldg_stream(Ff + rs);
 				} else {
-					fnn[u] = __ldg(fourier_row(p, fc, im, rn));
-					fsn[u] = __ldg(fourier_row(p, fc, im, rs));
+					fnn[u] = ldg_stream(fourier_row(p, fc, im, rn));
+					fsn[u] = ldg_stream(fourier_row(p, fc, im, rs));
 				}
 			}
 		}
@@ -584,7 +595,7 @@ __device__ __forceinline__ void leg_analys_tile(const LegParams& p, int im, int 
 		#pragma unroll
 		for (int u = 0; u < SPT; u++) {
 			const int sg = gsg + u * GPT, gks = k0 + sg * SEG;
-			ckn[u] = (sg < NSG && t < p.nlat_2 && gks < nk) ? __ldg(ckm + (long)(gks / SEG) * p.nlat_2 + t)
+			ckn[u] = (sg < NSG && t < p.nlat_2 && gks < nk) ? ldg_stream(ckm + (long)(gks / SEG) * p.nlat_2 + t)
 			                                               : make_double2(0.0, 0.0);
 		}
 	};
