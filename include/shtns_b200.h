@@ -87,7 +87,14 @@ void cu_spat_to_SH_adjoint(shtns_cfg, cplx *Qg, double *Vg, int ltr);
  * path (shtns_b200_kernel_errors returns 1, no output is written).  Option 9
  * (test hook, set only, any plan): fills the static scratch array of
  * cu_SH_to_spat_noalloc on the current device with the byte value 0..255
- * (0xFF: NaN doubles) and waits for it.  Return 0 or -1.
+ * (0xFF: NaN doubles) and waits for it.  Option 10: FP64 Legendre values
+ * of the 64 x 64 tile synthesis, 0 (default) from a table of Y_k(theta)
+ * built on the device on first use when it takes at most a quarter of the
+ * free device memory and 8 GiB (about 0.2 GB at lmax 511 on 768 latitudes;
+ * otherwise, and inside a stream capture before the table exists, on the
+ * fly), 1 always on the fly, 2 always the table (an error when it does not
+ * fit).  Both forms give bit-identical results; clones use the table of
+ * their base plan.  Return 0 or -1.
  * No counterpart in SHTns 3.5.2. */
 int shtns_b200_set_option(shtns_cfg, int option, int value);
 int shtns_b200_get_option(shtns_cfg, int option);

@@ -12,7 +12,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libshtns_b200.so")
 OBJDIR = os.path.join(HERE, "_build")
 
-SOURCES = ["sht_plan.cu", "sht_gauss.cu", "sht_api.cu", "sht_legendre.cu", "sht_legendre_simt.cu", "sht_fft.cu", "sht_noalloc.cu", "sht_split.cu", "sht_ptab.cu", "sht_local.cu", "sht_rotation.cu"]
+SOURCES = ["sht_plan.cu", "sht_gauss.cu", "sht_api.cu", "sht_legendre.cu", "sht_legendre_simt.cu", "sht_fft.cu", "sht_noalloc.cu", "sht_split.cu", "sht_ptab.cu", "sht_ftab.cu", "sht_local.cu", "sht_rotation.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 

@@ -171,7 +171,7 @@ void run_synth(shtns_cfg s, int ncomp, const int* types, const cplx* Q, const cp
 	lp.adjoint = adjoint;
 	shtb_stage_begin(s, 1);
 	if (s->split_ns) launch_leg_synth_split(s, lp, s->comp_stream);
-	else launch_leg_synth(lp, s->comp_stream);
+	else if (!launch_ftab_synth(s, lp, s->comp_stream)) launch_leg_synth(lp, s->comp_stream);
 	shtb_stage_end(s);
 	FftParams fp = fft_params(s, j);
 	fp.spat[0] = o0; fp.spat[1] = o1; fp.spat[2] = o2;

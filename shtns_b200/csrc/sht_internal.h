@@ -124,6 +124,15 @@ struct shtns_info {
 	std::vector<long> koff_blocks_h;     // host copy of d_pkoff
 	void *d_pbs; size_t pbs_cap;         // per call: B-operand digit stacks
 	int *d_pexp; size_t pexp_cap;        // per call: column exponents [im][column]
+	// FP64 Legendre values from a precomputed table (option 10): Y_k(theta) of
+	// every order in 32 x 32 blocks, built on first use and owned by the
+	// original plan (clones use their base plan's table)
+	int ftab_mode;                       // 0 automatic (within a memory budget), 1 off, 2 on
+	double *d_ftab; size_t ftab_bytes;   // table blocks
+	long *d_ftoff;                       // per order: first block
+	int *d_ftb0;                         // per order: first 32-latitude block kept by the polar threshold
+	double *d_fzero;                     // one zero row of the B operand (steps beyond the call's last)
+	int ftab_failed;                     // the automatic mode could not allocate the table: do not retry
 	// local evaluation (points, latitudes, operators): classic-recurrence
 	// tables on the device, allocated on first use (no grid needed), and staging
 	double *d_alm; long *d_almoff;
@@ -249,6 +258,8 @@ bool split_row_exponents(shtns_cfg s, cudaStream_t st);
 void launch_ptab_synth(shtns_cfg s, const LegParams& p, cudaStream_t st);
 void launch_ptab_analys(shtns_cfg s, const LegParams& p, cudaStream_t st);
 void free_ptab(shtns_cfg s);
+bool launch_ftab_synth(shtns_cfg s, const LegParams& p, cudaStream_t st);
+void free_ftab(shtns_cfg s);
 bool leg_simt_selected(const LegParams& p, bool synth);
 void launch_leg_synth_simt(const LegParams& p, cudaStream_t st);
 void launch_leg_analys_simt(const LegParams& p, int kmax_all, cudaStream_t st);

@@ -334,6 +334,7 @@ static void free_device(shtns_cfg s)
 		for (void* p : ptrs) if (p) cudaFree(p);
 	}
 	free_split(s);
+	free_ftab(s);
 	if (s->d_alm) cudaFree(s->d_alm);
 	if (s->d_loc) cudaFree(s->d_loc);
 	s->d_alm = nullptr; s->d_almoff = nullptr; s->d_loc = nullptr; s->loc_cap = 0;
@@ -692,6 +693,8 @@ extern "C" shtns_cfg cushtns_clone(shtns_cfg b, cudaStream_t compute_stream, cud
 	s->d_ptab = nullptr; s->ptab_bytes = 0; s->ptab_ns = 0; s->d_ptoff = nullptr; s->d_pkoff = nullptr;
 	s->d_pvoff = nullptr; s->d_pt0 = nullptr; s->d_pkf = nullptr; s->ptab_kblocks = 0; s->ptab_ttiles = 0;
 	s->d_pbs = nullptr; s->pbs_cap = 0; s->d_pexp = nullptr; s->pexp_cap = 0;
+	s->d_ftab = nullptr; s->ftab_bytes = 0; s->d_ftoff = nullptr; s->d_ftb0 = nullptr; s->d_fzero = nullptr;
+	s->ftab_failed = 0;
 	s->xfer_stream = nullptr; s->own_xfer = 0;
 	s->d2h_stream = nullptr; s->xev.clear();
 	s->ev.clear(); s->ev_stage.clear(); s->ev_used = 0; s->timing = 0;
@@ -831,7 +834,8 @@ extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
 			}
 			cudaFree(old);
 			s->d_ck = nck;
-			free_split(s);          // split-precision tables derive from the checkpoints
+			free_split(s);          // split-precision and FP64 tables derive from the checkpoints
+			free_ftab(s);
 			const int nm = s->mmax + 1;
 			cudaMemcpy(s->d_mint + 4 * nm, s->ckoff_h.data(), sizeof(int) * nm, cudaMemcpyHostToDevice);
 			launch_checkpoints(s, 0);
@@ -854,6 +858,11 @@ extern "C" int shtns_b200_set_option(shtns_cfg s, int option, int value)
 		case 9:   // test hook: fill the no-allocation entry point's static scratch with this byte
 			if (value < 0 || value > 255) return -1;
 			return shtb_noalloc_fill(value);
+		case 10:  // FP64 Legendre values: 0 automatic (precomputed table within a memory budget), 1 on the fly, 2 table
+			if (value < 0 || value > 2) return -1;
+			s->ftab_mode = value;
+			s->ftab_failed = 0;
+			return 0;
 		default:
 			return -1;
 	}
@@ -871,6 +880,7 @@ extern "C" int shtns_b200_get_option(shtns_cfg s, int option)
 		case 6: return fft_last_path();   // FFT kernels of the last launch in this process
 		case 7: return s->fft_extra_tx;
 		case 8: return s->split_form;
+		case 10: return s->ftab_mode;
 		default: return -1;
 	}
 }
