@@ -91,52 +91,57 @@ extern "C" int shtns_use_gpu(int device_id)
 }
 
 // ---------------------------------------------------------------------------
-// Legendre tables.  alm layout per order (as sht_legendre.c:630-657): pair 0 =
-// (seed Y_mm prefactor, a_{m+1}); pair j >= 1 = (b_{m+j+1}, a_{m+j+1});
-// computed up to degree lmax+1.
+// Legendre tables of the classic recurrence in the degree at fixed order m,
+//   P_l = a_l x P_{l-1} + b_l P_{l-2},   P_{m+1} = a_{m+1} x P_m,
+//   P_m = c_m sin^m(theta),
+// for the two normalisations of the API (standard results, e.g. Abramowitz &
+// Stegun 8.5.3 rescaled):
+//   orthonormal:  a_l = sqrt((4 l^2 - 1) / (l^2 - m^2)),
+//                 b_l = -sqrt((2 l + 1) ((l-1)^2 - m^2) / ((2 l - 3) (l^2 - m^2))),
+//                 c_m = sqrt(prod_{j=1..m} (2 j + 1) / (2 j) / (4 pi));
+//   Schmidt:      a_l = (2 l - 1) / sqrt(l^2 - m^2),
+//                 b_l = -sqrt(((l-1)^2 - m^2) / (l^2 - m^2)),
+//                 c_m = sqrt(prod_{j=1..m} (2 j + 1) / (2 j) / (2 m + 1));
+//   4 pi-normalised: the orthonormal a_l, b_l and c_m times sqrt(4 pi),
+// times the order renormalisation for m > 0 and the Condon-Shortley sign
+// (-1)^m when asked for.  Storage per order (the pair layout the local
+// evaluation kernels read): pair 0 = (c_m, a_{m+1}), pair j >= 1 =
+// (b_{m+j+1}, a_{m+j+1}), up to degree lmax + 1; all in long double.
 static void legendre_tables(shtns_cfg s)
 {
 	const int lmax = s->lmax, mmax = s->mmax, mres = s->mres;
-	const long lmax1 = lmax + 1;
+	const bool schmidt = (s->base_norm == sht_schmidt);
 	s->alm_off.resize(mmax + 2);
 	long tot = 0;
-	for (int im = 0; im <= mmax; im++) { s->alm_off[im] = tot; tot += 2 * (lmax1 - im * mres + 1); }
+	for (int im = 0; im <= mmax; im++) { s->alm_off[im] = tot; tot += 2 * (lmax + 2 - im * mres); }
 	s->alm_off[mmax + 1] = tot;
 	s->alm.assign(tot + 2, 0.0);
-	// seeds: Y_00 * sqrt(prod_{k<=m} (2k+1)/(2k)) with optional (-1)^m, in long double
-	long double t1 = (s->base_norm == sht_orthonormal) ? 0.25L / 3.14159265358979323846264338327950288L : 1.0L;
-	s->alm[s->alm_off[0]] = (double) std::sqrt(t1);
-	t1 *= (long double) s->mpos_renorm;
-	for (int im = 1, m = 0; im <= mmax; im++) {
-		while (m < im * mres) { m++; t1 *= ((long double) m + 0.5L) / (long double) m; }
-		long double t2 = std::sqrt(t1);
-		if ((m & 1) && s->cs_phase) t2 = -t2;
-		s->alm[s->alm_off[im]] = (double) t2;
-	}
+	const long double four_pi = 4.0L * 3.14159265358979323846264338327950288L;
+	long double prod = 1.0L;              // prod_{j=1..m} (2j+1)/(2j), advanced with m
+	int mprod = 0;
 	for (int im = 0; im <= mmax; im++) {
 		const long m = (long) im * mres;
+		while (mprod < m) { mprod++; prod *= ((long double) mprod + 0.5L) / (long double) mprod; }
+		long double c2 = prod * ((s->base_norm == sht_orthonormal) ? 1.0L / four_pi : 1.0L);
+		if (m > 0) c2 *= (long double) s->mpos_renorm;
+		long double c = std::sqrt(c2);
+		if (schmidt) c /= std::sqrt((long double)(2 * m + 1));
+		if ((m & 1) && s->cs_phase) c = -c;
+		const auto a_l = [&](long l) -> long double {
+			const long double d = (long double)((l - m) * (l + m));
+			return schmidt ? (2 * l - 1) / std::sqrt(d) : std::sqrt((long double)((2 * l + 1) * (2 * l - 1)) / d);
+		};
+		const auto b_l = [&](long l) -> long double {
+			const long double d = (long double)((l - m) * (l + m)), d1 = (long double)((l - 1 - m) * (l - 1 + m));
+			return schmidt ? -std::sqrt(d1) / std::sqrt(d)
+			               : -std::sqrt(((2 * l + 1) * d1) / ((long double)(2 * l - 3) * d));
+		};
 		double* al = s->alm.data() + s->alm_off[im];
-		if (s->base_norm == sht_schmidt) {
-			long double t2 = std::sqrt((long double)(2 * m + 1));
-			al[0] = (double)(al[0] / t2);
-			al[1] = (double) t2;
-			long j = 2;
-			for (long l = m + 2; l <= lmax1; l++) {
-				long double tt = std::sqrt((long double)((l + m) * (l - m)));
-				al[j + 1] = (double)((2 * l - 1) / tt);
-				al[j] = (double)(-t2 / tt);
-				t2 = tt; j += 2;
-			}
-		} else {
-			long double t2 = 2 * m + 1;
-			al[1] = (double) std::sqrt((long double)(2 * m + 3));
-			long j = 2;
-			for (long l = m + 2; l <= lmax1; l++) {
-				long double tt = (long double)((l + m) * (l - m));
-				al[j + 1] = (double) std::sqrt(((2 * l + 1) * (2 * l - 1)) / tt);
-				al[j] = (double)(-std::sqrt(((2 * l + 1) * t2) / ((2 * l - 3) * tt)));
-				t2 = tt; j += 2;
-			}
+		al[0] = (double) c;
+		al[1] = (double) a_l(m + 1);
+		for (long l = m + 2, j = 2; l <= lmax + 1; l++, j += 2) {
+			al[j] = (double) b_l(l);
+			al[j + 1] = (double) a_l(l);
 		}
 	}
 }
@@ -176,16 +181,36 @@ static void ct_coefficients(shtns_cfg s, double* mx, int stdt)
 extern "C" void mul_ct_matrix(shtns_cfg s, double* mx) { if (s && mx) ct_coefficients(s, mx, 0); }
 extern "C" void st_dt_matrix(shtns_cfg s, double* mx) { if (s && mx) ct_coefficients(s, mx, 1); }
 
-// Ishioka recurrence (sht_legendre.c:673-734): per order, the two-term
-// coefficients c (2 per k) and the basis change x (3 per k), padded so that
-// kernels may read whole 32-step segments.
+// Ishioka's recurrence (J. Meteor. Soc. Japan 96, 241-249, 2018,
+// doi:10.2151/jmsj.2018-019), derived here for the orthonormal functions.
+// With eps_l = sqrt((l^2 - m^2) / (4 l^2 - 1)), x P_l = eps_{l+1} P_{l+1} +
+// eps_l P_{l-1}.  Writing the odd degrees as P_{m+2k+1} = x p0 d_k Y_k (p0 the
+// seed c_m, Y_0 = sin^m(theta)) and applying the three-term relation twice
+// gives a two-term recurrence in x^2 for Y_k; choosing
+//   d_0 = 1 / eps_{m+1},   d_{k+1} = (-1)^k / (d_k eps_{m+2k+2} eps_{m+2k+3})
+// makes the coefficient of Y_{k-1} equal to one:
+//   Y_{k+1} = (C_{2k+1} x^2 + C_{2k}) Y_k + Y_{k-1},
+//   C_{2k+1} = (-1)^k d_k^2,   C_{2k} = -C_{2k+1} (eps_{m+2k+1}^2 + eps_{m+2k+2}^2).
+// The even degrees follow from x P_{m+2k} = eps_{m+2k+1} P_{m+2k+1} +
+// eps_{m+2k} P_{m+2k-1}:
+//   P_{m+2k} = p0 (eps_{m+2k+1} d_k Y_k + eps_{m+2k} d_{k-1} Y_{k-1}),
+// so a field sum_l Q_l P_l = sum_k (X0_k Q_{m+2k} + X1_k Q_{m+2k+2}) Y_k +
+// x sum_k X2_k Q_{m+2k+1} Y_k with
+//   X0_k = p0 eps_{m+2k+1} d_k,  X1_k = p0 eps_{m+2k+2} d_k,  X2_k = p0 d_k.
+// Schmidt functions are the orthonormal ones times sqrt(4 pi / (2l + 1)) up to
+// the seed: the same Y_k, with the synthesis coefficient of degree l divided
+// by sqrt(2 l + 1) (and p0 the orthonormal seed) and the analysis one
+// multiplied by it.  Per order: C (2 per k, padded so that kernels may read
+// whole 32-step segments) and the basis change X (3 per k) for synthesis (xs)
+// and analysis (xa).  (The reference builds the same recurrence in
+// sht_legendre.c:673-734.)
 static void ishioka_tables(shtns_cfg s)
 {
 	const int lmax = s->lmax, mmax = s->mmax, mres = s->mres;
 	s->kmax_h.resize(mmax + 1);
 	s->koff_h.resize(mmax + 1); s->coff_h.resize(mmax + 1); s->xoff_h.resize(mmax + 1);
 	s->voff_h.resize(mmax + 1); s->ckoff_h.resize(mmax + 1);
-	long kt = 0, ct = 0, xt = 0, vt = 0, sg = 0;
+	long kt = 0, ct = 0, xt = 0, vt = 0;
 	for (int im = 0; im <= mmax; im++) {
 		const int m = im * mres;
 		const int kmax = (lmax + 1 - m) / 2 + 1;         // Y_k rows for degrees up to lmax+1
@@ -196,50 +221,39 @@ static void ishioka_tables(shtns_cfg s)
 		s->xoff_h[im] = (int) xt;  xt += 3 * (kmax + 1);
 		s->voff_h[im] = (int) vt;  vt += lmax + 3 - m;
 	}
-	s->ktot = kt; s->ctot = ct; s->xtot = xt; s->vtot = vt; s->segtot = sg;
-	(void) sg;
+	s->ktot = kt; s->ctot = ct; s->xtot = xt; s->vtot = vt; s->segtot = 0;
 	s->ish_c.assign(ct, 0.0);
 	s->ish_xs.assign(xt, 0.0);
 	s->ish_xa.assign(xt, 0.0);
+	const bool schmidt = (s->base_norm == sht_schmidt);
 	for (int im = 0; im <= mmax; im++) {
 		const long m = (long) im * mres;
-		const long ne = lmax + 4 - m;
-		std::vector<long double> elm(ne + 2, 0.0L), dlm((lmax - m + 1) / 2 + 2, 0.0L);
-		for (long l = m + 1; l <= lmax + 4; l++) {
-			long double num = (long double)((l - m) * (l + m));
-			long double den = (long double)((2 * l + 1) * (2 * l - 1));
-			elm[l - (m + 1)] = std::sqrt(num / den);
-		}
-		long double alpha = 1.0L / elm[0];
-		for (long i = 0; i <= (lmax - m + 1) / 2; i++) {
-			dlm[i] = alpha;
-			alpha = (1.0L * (1 - 2 * (i & 1))) / (alpha * elm[2 * i + 2] * elm[2 * i + 1]);
-		}
+		const auto eps = [&](long l) -> long double {
+			return std::sqrt((long double)((l - m) * (l + m)) / (long double)((2 * l + 1) * (2 * l - 1)));
+		};
+		// degree-l scale of the Schmidt basis change (1 for orthonormal functions)
+		const auto nrm = [&](long l) -> long double { return schmidt ? std::sqrt((long double)(2 * l + 1)) : 1.0L; };
+		long double p0 = s->alm[s->alm_off[im]];
+		if (schmidt) p0 *= std::sqrt((long double)(2 * m + 1));     // the orthonormal seed
+		const long nk = (lmax - m + 1) / 2;                            // C for k < nk, X for k <= nk
 		double* c = s->ish_c.data() + s->coff_h[im];
-		for (long i = 0; i < (lmax - m + 1) / 2; i++) {
-			long double a = dlm[i] * dlm[i] * (1 - 2 * (i & 1));
-			c[2 * i] = (double)(-a * (elm[2 * i] * elm[2 * i] + elm[2 * i + 1] * elm[2 * i + 1]));
-			c[2 * i + 1] = (double) a;
-		}
-		long double a0m = s->alm[s->alm_off[im]];
-		if (s->base_norm == sht_schmidt) a0m *= std::sqrt((long double)(2 * m + 1));
 		double* xs = s->ish_xs.data() + s->xoff_h[im];
 		double* xa = s->ish_xa.data() + s->xoff_h[im];
-		long l = m;
-		for (long i = 0; i <= (lmax - m + 1) / 2; i++) {
-			long double a = dlm[i] * a0m;
-			long double x0 = elm[2 * i] * a, x1 = elm[2 * i + 1] * a, x2 = a;
-			long double y0 = x0, y1 = x1, y2 = x2;
-			if (s->base_norm == sht_schmidt) {
-				long double sq = std::sqrt((long double)(2 * l + 1));
-				long double sq1 = std::sqrt((long double)(2 * (l + 1) + 1));
-				long double sq2 = std::sqrt((long double)(2 * (l + 2) + 1));
-				y0 = x0 * sq;  y1 = x1 * sq2;  y2 = x2 * sq1;
-				x0 /= sq;      x1 /= sq2;      x2 /= sq1;
-				l += 2;
+		long double d = 1.0L / eps(m + 1);
+		for (long k = 0; k <= nk; k++) {
+			const long l = m + 2 * k;
+			const long double x0 = p0 * eps(l + 1) * d, x1 = p0 * eps(l + 2) * d, x2 = p0 * d;
+			xs[3 * k] = (double)(x0 / nrm(l));     xa[3 * k] = (double)(x0 * nrm(l));
+			xs[3 * k + 1] = (double)(x1 / nrm(l + 2)); xa[3 * k + 1] = (double)(x1 * nrm(l + 2));
+			xs[3 * k + 2] = (double)(x2 / nrm(l + 1)); xa[3 * k + 2] = (double)(x2 * nrm(l + 1));
+			if (k < nk) {
+				const long double sgn = (k & 1) ? -1.0L : 1.0L;
+				const long double c1 = sgn * d * d;
+				const long double e1 = eps(l + 1), e2 = eps(l + 2);
+				c[2 * k + 1] = (double) c1;
+				c[2 * k] = (double)(-c1 * (e1 * e1 + e2 * e2));
 			}
-			xs[3 * i] = (double) x0; xs[3 * i + 1] = (double) x1; xs[3 * i + 2] = (double) x2;
-			xa[3 * i] = (double) y0; xa[3 * i + 1] = (double) y1; xa[3 * i + 2] = (double) y2;
+			d = ((k & 1) ? -1.0L : 1.0L) / (d * eps(l + 2) * eps(l + 3));
 		}
 	}
 }
