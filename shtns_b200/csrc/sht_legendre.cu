@@ -123,8 +123,9 @@ __global__ void ck_kernel(int nlat_2, int mres, int seg, const double* __restric
 
 __global__ void __launch_bounds__(256, 6) prep_synth_kernel(PrepParams p)
 {
-	constexpr int NE = 2 * PT_F * PT_W, NU = (NE + 255) / 256;
 	__shared__ double2 win[2][PT_F][PT_W];
+	__shared__ double cfs[2][PT_W];          // sin d/dtheta coupling (lo, hi) of the window's degrees
+	__shared__ double xk[3 * PT_K];          // basis change X of the CTA's k rows
 	__shared__ int s_comp[PT_F], s_f[PT_F];
 	const int im = p.im0 + blockIdx.z;
 	if (im > p.mlim) return;
@@ -138,42 +139,62 @@ __global__ void __launch_bounds__(256, 6) prep_synth_kernel(PrepParams p)
 	const int lrel_max = p.llim - m;
 	const long off = (long)im * (2 * p.lmax + 2 - (im + 1) * p.mres) / 2 + m;   // LM(m, m)
 	const int d0 = 2 * k0 - 1;
-	if (threadIdx.x < PT_F) {
-		const int fc = fc0 + threadIdx.x;
-		const int comp = fc / p.nf;
-		s_comp[threadIdx.x] = (fc < nfc) ? comp : -1;
-		s_f[threadIdx.x] = fc - comp * p.nf;
-	}
-	__syncthreads();
-	// all window loads of a thread are issued before the first is stored
-	double2 v[NU];
-	#pragma unroll
-	for (int u = 0; u < NU; u++) {
-		const int e = threadIdx.x + 256 * u;
-		const int a = e / (PT_F * PT_W), r = e - a * PT_F * PT_W;
-		const int fl = r / PT_W, i = r - fl * PT_W;
-		const int d = d0 + i;
-		v[u] = make_double2(0.0, 0.0);
-		const int comp = (e < NE) ? s_comp[fl] : -1;
-		if (comp >= 0 && d >= 0 && d <= lrel_max) {
-			const double2* base = (p.comp_type[comp] == 0) ? (a == 0 ? p.Q : nullptr) : (a == 0 ? p.S : p.T);
-			if (base) v[u] = base[off + (long)s_f[fl] * p.spec_dist + d];
-		}
-	}
-	#pragma unroll
-	for (int u = 0; u < NU; u++) {
-		const int e = threadIdx.x + 256 * u;
-		if (e < NE) {
-			const int a = e / (PT_F * PT_W), r = e - a * PT_F * PT_W;
-			const int fl = r / PT_W, i = r - fl * PT_W;
-			if (m0) v[u].y = 0.0;
-			win[a][fl][i] = v[u];
-		}
-	}
-	__syncthreads();
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	const int voff = p.mt.voff[im];
+	if (tid < PT_F) {
+		const int fc = fc0 + tid;
+		const int comp = fc / p.nf;
+		s_comp[tid] = (fc < nfc) ? comp : -1;
+		s_f[tid] = fc - comp * p.nf;
+	} else if (tid >= 32 && tid < 32 + PT_W) {
+		const int i = tid - 32, d = d0 + i;
+		cfs[0][i] = (d > 0 && d <= lrel_max + 1) ? p.stdt_lo[voff + d] : 0.0;
+		cfs[1][i] = (d >= 0 && d <= lrel_max + 1) ? p.stdt_hi[voff + d] : 0.0;
+	} else if (tid >= 128 && tid < 128 + 3 * PT_K) {
+		const int e = tid - 128;
+		xk[e] = (k0 + e / 3 <= kmax) ? p.xs[p.mt.xoff[im] + 3 * k0 + e] : 0.0;
+	}
+	// window of degrees d0 .. d0 + 68 of each (array, field-component): warp w
+	// stages pairs w, w + 8, w + 16, w + 24 (array = pair / 16), lanes along
+	// the degrees, two pairs at a time with all their loads issued before the
+	// first store
+	constexpr int NI = (PT_W + 31) / 32;
+	#pragma unroll
+	for (int h = 0; h < 2; h++) {
+		double2 v[2][NI];
+		#pragma unroll
+		for (int qi = 0; qi < 2; qi++) {
+			const int q = warp + 8 * (2 * h + qi), a = q / PT_F, fl = q % PT_F;
+			const int fc = fc0 + fl;
+			const double2* base = nullptr;
+			if (fc < nfc) {
+				const int comp = fc / p.nf, f = fc - comp * p.nf;
+				base = (p.comp_type[comp] == 0) ? (a == 0 ? p.Q : nullptr) : (a == 0 ? p.S : p.T);
+				if (base) base += off + (long)f * p.spec_dist;
+			}
+			#pragma unroll
+			for (int u = 0; u < NI; u++) {
+				const int d = d0 + lane + 32 * u;
+				v[qi][u] = (base && lane + 32 * u < PT_W && d >= 0 && d <= lrel_max) ? base[d] : make_double2(0.0, 0.0);
+			}
+		}
+		#pragma unroll
+		for (int qi = 0; qi < 2; qi++) {
+			const int q = warp + 8 * (2 * h + qi), a = q / PT_F, fl = q % PT_F;
+			#pragma unroll
+			for (int u = 0; u < NI; u++) {
+				const int i = lane + 32 * u;
+				if (i < PT_W) {
+					double2 x = v[qi][u];
+					if (m0) x.y = 0.0;
+					win[a][fl][i] = x;
+				}
+			}
+		}
+	}
+	__syncthreads();
 	const double em = (p.msign < 0) ? -(double) m : (double) m;   // signed m (negative orders of the _ml transforms)
-	for (int e = threadIdx.x; e < PT_K * PT_F; e += blockDim.x) {
+	for (int e = tid; e < PT_K * PT_F; e += blockDim.x) {
 		const int kl = e / PT_F, fl = e - kl * PT_F;
 		const int k = k0 + kl, fc = fc0 + fl;
 		if (k >= kmax || fc >= nfc) continue;
@@ -181,28 +202,28 @@ __global__ void __launch_bounds__(256, 6) prep_synth_kernel(PrepParams p)
 		// fields from neg_from on carry the order -m (complex-field transforms)
 		const int fld = s_f[fl];
 		const double emf = (p.neg_from > 0 && fld >= p.neg_from) ? -em : em;
+		const int i0 = 2 * kl + 1;                 // window index of degree 2k
 		double2 q3[3];
-		#pragma unroll
-		for (int r = 0; r < 3; r++) {
-			const int d = 2 * k + r;               // relative degree
-			const int i = d - d0;                  // window index of degree d
-			if (type == 0) {
-				q3[r] = win[0][fl][i];
-			} else if (d > lrel_max + 1) {
-				q3[r] = make_double2(0.0, 0.0);
-			} else {
-				const double lo = (d > 0) ? p.stdt_lo[voff + d] : 0.0;
-				const double hi = p.stdt_hi[voff + d];
-				const double2 sm = win[0][fl][i - 1], sp = win[0][fl][i + 1], s0 = win[0][fl][i];
-				const double2 tmn = win[1][fl][i - 1], tp = win[1][fl][i + 1], t0 = win[1][fl][i];
-				if (type == 1)   // V = stdt S + i m T
-					q3[r] = make_double2(lo * sm.x + hi * sp.x - emf * t0.y, lo * sm.y + hi * sp.y + emf * t0.x);
-				else             // W = -stdt T + i m S
-					q3[r] = make_double2(-(lo * tmn.x + hi * tp.x) - emf * s0.y, -(lo * tmn.y + hi * tp.y) + emf * s0.x);
+		if (type == 0) {
+			#pragma unroll
+			for (int r = 0; r < 3; r++) q3[r] = win[0][fl][i0 + r];
+		} else {
+			// V = stdt S + i m T (type 1), W = -stdt T + i m S (type 2): the
+			// coupled array at degrees d -/+ 1, the other one at d
+			const int ac = (type == 1) ? 0 : 1;
+			#pragma unroll
+			for (int r = 0; r < 3; r++) {
+				const int d = 2 * k + r;               // relative degree
+				if (d > lrel_max + 1) { q3[r] = make_double2(0.0, 0.0); continue; }
+				const double lo = cfs[0][i0 + r], hi = cfs[1][i0 + r];
+				const double2 cm = win[ac][fl][i0 - 1 + r], cp = win[ac][fl][i0 + 1 + r], o0 = win[1 - ac][fl][i0 + r];
+				if (type == 1)
+					q3[r] = make_double2(lo * cm.x + hi * cp.x - emf * o0.y, lo * cm.y + hi * cp.y + emf * o0.x);
+				else
+					q3[r] = make_double2(-(lo * cm.x + hi * cp.x) - emf * o0.y, -(lo * cm.y + hi * cp.y) + emf * o0.x);
 			}
 		}
-		const double* X = p.xs + p.mt.xoff[im] + 3 * k;
-		const double x0 = X[0], x1 = X[1], x2 = X[2];
+		const double x0 = xk[3 * kl], x1 = xk[3 * kl + 1], x2 = xk[3 * kl + 2];
 		double* row = p.qq + (long)(p.mt.koff[im] + k) * p.ncol;
 		const int ce = 16 * (fc >> 2) + 2 * (fc & 3);
 		*reinterpret_cast<double2*>(row + ce) = make_double2(fma(x0, q3[0].x, x1 * q3[2].x), fma(x0, q3[0].y, x1 * q3[2].y));
@@ -309,17 +330,33 @@ __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 			}
 		}
 	}
-	__syncthreads();
+	// vector coupling (lo, hi) of degrees j0 - 1 .. j0 + PE_J and 1 / (l (l + 1))
+	// of the tile's degrees, shared by its fields
+	__shared__ double vlo[PE_J + 2], vhi[PE_J + 2], vl2[PE_J];
 	const int voff = p.mt.voff[im];
+	if (!scalar_group) {
+		for (int e = threadIdx.x; e < PE_J + 2; e += blockDim.x) {
+			const int j = j0 - 1 + e;
+			vlo[e] = (j > 0 && j < nl) ? p.van_lo[voff + j] : 0.0;
+			vhi[e] = (j >= 0 && j < nl) ? p.van_hi[voff + j] : 0.0;
+			if (e < PE_J) vl2[e] = (j0 + e < nl) ? p.l2[m + j0 + e] : 0.0;
+		}
+	}
+	__syncthreads();
 	const double em = (p.msign < 0) ? -(double) m : (double) m;   // signed m (negative orders of the _ml transforms)
+	const int lane = threadIdx.x & 31;
+	// a warp covers 32 consecutive degrees of one field: each lane forms its
+	// own degree in the spectral basis and takes the neighbours (j -/+ 1) of
+	// the vector formulas from the adjacent lanes
 	for (int e = threadIdx.x; e < PE_J * PE_F; e += blockDim.x) {
 		const int fl = e / PE_J, jl = e - fl * PE_J;
 		const int j = j0 + jl, f = f0 + fl;
-		if (j >= nl || f >= p.nf) continue;
 		const int l = m + j;
+		const bool live = j < nl && f < p.nf;
 		const long o = off + (long)f * p.spec_dist + j;
 		const bool zero = zero_m || (l > p.llim);
 		if (scalar_group) {
+			if (!live) continue;
 			double2 q = make_double2(0.0, 0.0);
 			if (!zero) {
 				q = ish_inv_s(sv, xs, kb, fl, j);
@@ -328,13 +365,22 @@ __global__ void __launch_bounds__(256) post_analys_kernel(PrepParams p)
 			p.Qo[o] = q;
 			continue;
 		}
+		const bool fv = !zero_m && f < p.nf && j < nl + 1;   // rows staged: degrees up to nl
+		const double2 v0 = fv ? ish_inv_s(sv, xs, kb, fl, j) : make_double2(0.0, 0.0);
+		const double2 w0 = fv ? ish_inv_s(sw, xs, kb, fl, j) : make_double2(0.0, 0.0);
+		double2 vm, vp, wm, wp;
+		vm.x = __shfl_up_sync(0xffffffffu, v0.x, 1); vm.y = __shfl_up_sync(0xffffffffu, v0.y, 1);
+		wm.x = __shfl_up_sync(0xffffffffu, w0.x, 1); wm.y = __shfl_up_sync(0xffffffffu, w0.y, 1);
+		vp.x = __shfl_down_sync(0xffffffffu, v0.x, 1); vp.y = __shfl_down_sync(0xffffffffu, v0.y, 1);
+		wp.x = __shfl_down_sync(0xffffffffu, w0.x, 1); wp.y = __shfl_down_sync(0xffffffffu, w0.y, 1);
+		if (!live) continue;
 		double2 s = make_double2(0.0, 0.0), t = make_double2(0.0, 0.0);
 		if (!zero) {
-			const double2 vm = ish_inv_s(sv, xs, kb, fl, j - 1), v0 = ish_inv_s(sv, xs, kb, fl, j), vp = ish_inv_s(sv, xs, kb, fl, j + 1);
-			const double2 wm = ish_inv_s(sw, xs, kb, fl, j - 1), w0 = ish_inv_s(sw, xs, kb, fl, j), wp = ish_inv_s(sw, xs, kb, fl, j + 1);
-			const double lo = (j > 0) ? p.van_lo[voff + j] : 0.0;
-			const double hi = p.van_hi[voff + j];
-			const double l2 = p.l2[l];
+			if (lane == 0) { vm = ish_inv_s(sv, xs, kb, fl, j - 1); wm = ish_inv_s(sw, xs, kb, fl, j - 1); }
+			if (lane == 31) { vp = ish_inv_s(sv, xs, kb, fl, j + 1); wp = ish_inv_s(sw, xs, kb, fl, j + 1); }
+			const double lo = vlo[jl + 1];
+			const double hi = vhi[jl + 1];
+			const double l2 = vl2[jl];
 			const double mxv_r = lo * vm.x + hi * vp.x, mxv_i = lo * vm.y + hi * vp.y;
 			const double mxw_r = lo * wm.x + hi * wp.x, mxw_i = lo * wm.y + hi * wp.y;
 			const double emf = (p.neg_from > 0 && f >= p.neg_from) ? -em : em;   // order -m fields
