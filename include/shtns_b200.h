@@ -128,7 +128,8 @@ int shtns_b200_get_option(shtns_cfg, int option);
 int shtns_b200_kernel_errors(shtns_cfg);
 size_t shtns_b200_split_table_bytes(shtns_cfg);
 
-/* Plan groups: scalar transforms of fields of different lmax, each on the grid
+/* Plan groups: transforms of fields of different lmax (scalar, and the vector
+ * forms below), each on the grid
  * of its own plan, with the Legendre stage of all plans in one persistent
  * launch whose CTAs take work items (plan, order, tile) from a queue in
  * decreasing cost order.  Qlm[i] / Vr[i] hold nfields[i] contiguous fields of
@@ -153,6 +154,16 @@ void shtns_b200_group_destroy(shtns_group);
 int shtns_b200_group_set_option(shtns_group, int option, int value);
 void shtns_b200_group_synth(shtns_group, cplx **Qlm, double **Vr, const int *nfields, int ltr);
 void shtns_b200_group_analys(shtns_group, double **Vr, cplx **Qlm, const int *nfields, int ltr);
+/* Vector transforms of a group (the plans' SHsphtor / SHqst forms): per plan
+ * i, nfields[i] fields of each component, device pointers, as above. */
+void shtns_b200_group_SHsphtor_to_spat(shtns_group, cplx **Slm, cplx **Tlm, double **Vt, double **Vp,
+                                       const int *nfields, int ltr);
+void shtns_b200_group_spat_to_SHsphtor(shtns_group, double **Vt, double **Vp, cplx **Slm, cplx **Tlm,
+                                       const int *nfields, int ltr);
+void shtns_b200_group_SHqst_to_spat(shtns_group, cplx **Qlm, cplx **Slm, cplx **Tlm, double **Vr, double **Vt,
+                                    double **Vp, const int *nfields, int ltr);
+void shtns_b200_group_spat_to_SHqst(shtns_group, double **Vr, double **Vt, double **Vp, cplx **Qlm, cplx **Slm,
+                                    cplx **Tlm, const int *nfields, int ltr);
 
 /* Scalar synthesis (same result as cu_SH_to_spat on device pointers) that
  * allocates no device memory, for callers that cannot call cudaMalloc where

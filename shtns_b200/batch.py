@@ -87,6 +87,52 @@ class PlanGroup:
         self._lib.shtns_b200_group_analys(self._g, A, B, nf, int(1 << 30 if ltr is None else ltr))
         capi.check(self._lib)
 
+    @staticmethod
+    def _ptrs(lists, n):
+        """One C array of device pointers per component list (null entries and
+        missing lists give null pointers)."""
+        out = []
+        for lst in lists:
+            if lst is None:
+                out.append(None)
+            else:
+                out.append((C.c_void_p * n)(*[x.data_ptr() if x is not None else 0 for x in lst]))
+        return out
+
+    def vector_synth_into(self, spec, spat, ltr=None):
+        """Spheroidal/toroidal (spec = (S, T), spat = (Vt, Vp)) or qst
+        (spec = (Q, S, T), spat = (Vr, Vt, Vp)) synthesis of every plan: each
+        entry a per-plan list of CUDA tensors, complex128 (nf_i, nlm_i) and
+        float64 (nf_i, *spat_shape_i)."""
+        n = len(self.plans)
+        nf = (C.c_int * n)()
+        for i, (p, x) in enumerate(zip(self.plans, spec[-1])):
+            nf[i] = 0 if x is None else x.numel() // p.nlm
+        P = self._ptrs(list(spec) + list(spat), n)
+        self.plans[0]._stream()
+        lt = int(1 << 30 if ltr is None else ltr)
+        if len(spec) == 2:
+            self._lib.shtns_b200_group_SHsphtor_to_spat(self._g, *P, nf, lt)
+        else:
+            self._lib.shtns_b200_group_SHqst_to_spat(self._g, *P, nf, lt)
+        capi.check(self._lib)
+
+    def vector_analys_into(self, spat, spec, ltr=None):
+        """Analysis counterpart of vector_synth_into (spat = (Vt, Vp) or
+        (Vr, Vt, Vp), spec = (S, T) or (Q, S, T))."""
+        n = len(self.plans)
+        nf = (C.c_int * n)()
+        for i, (p, x) in enumerate(zip(self.plans, spat[-1])):
+            nf[i] = 0 if x is None else x.numel() // p.nspat
+        P = self._ptrs(list(spat) + list(spec), n)
+        self.plans[0]._stream()
+        lt = int(1 << 30 if ltr is None else ltr)
+        if len(spat) == 2:
+            self._lib.shtns_b200_group_spat_to_SHsphtor(self._g, *P, nf, lt)
+        else:
+            self._lib.shtns_b200_group_spat_to_SHqst(self._g, *P, nf, lt)
+        capi.check(self._lib)
+
     def close(self):
         if getattr(self, "_g", None):
             self._lib.shtns_b200_group_destroy(self._g)

@@ -139,6 +139,10 @@ PROTOTYPES = {
     "shtns_b200_group_set_option": (I, [P, I, I]),
     "shtns_b200_group_synth": (None, [P, P, P, P, I]),
     "shtns_b200_group_analys": (None, [P, P, P, P, I]),
+    "shtns_b200_group_SHsphtor_to_spat": (None, [P, P, P, P, P, P, I]),
+    "shtns_b200_group_spat_to_SHsphtor": (None, [P, P, P, P, P, P, I]),
+    "shtns_b200_group_SHqst_to_spat": (None, [P, P, P, P, P, P, P, P, I]),
+    "shtns_b200_group_spat_to_SHqst": (None, [P, P, P, P, P, P, P, P, I]),
     "SH_to_point": (D, [CFG, P, D, D]),
     "SH_to_point_cplx": (CPLX, [CFG, P, D, D]),
     "SH_to_grad_point": (None, [CFG, P, P, D, D, P, P, P]),

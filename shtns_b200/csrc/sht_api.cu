@@ -766,7 +766,13 @@ extern "C" int shtns_b200_group_set_option(shtns_group g, int option, int value)
 	return -1;
 }
 
-extern "C" void shtns_b200_group_synth(shtns_group g, cplx** Qlm, double** Vr, const int* nfields, int ltr)
+namespace {
+
+// Group transforms of ncomp components (types: T_SCAL, T_VEC or T_QST): the
+// spectral arrays spec[c][i] and the grids spat[c][i] of component c, plan i
+// (a null array list reads zeros / is not written, as for the plan calls).
+void group_synth_impl(shtns_group g, int ncomp, const int* types, cplx** const* spec, double** const* spat,
+                      const int* nfields, int ltr)
 {
 	if (!group_ok(g)) return;
 	const int np = (int) g->plans.size();
@@ -776,43 +782,45 @@ extern "C" void shtns_b200_group_synth(shtns_group g, cplx** Qlm, double** Vr, c
 	for (int i = 0; i < np; i++) {
 		shtns_cfg s = g->plans[i];
 		shtns_set_batch(s, std::max(1, nfields[i]), s->nlm, s->nspat);
-		if (!setup_job(s, jobs[i], 1, T_SCAL, std::min<int>(ltr, s->lmax))) return;
+		if (!setup_job(s, jobs[i], ncomp, types, std::min<int>(ltr, s->lmax))) return;
 		lp[i] = leg_params(s, jobs[i]);
 	}
+	auto prologue = [&](int i, cudaStream_t x) {
+		PrepParams pp = prep_params(g->plans[i], jobs[i]);
+		pp.Q = spec[0] ? reinterpret_cast<const double2*>(spec[0][i]) : nullptr;
+		pp.S = spec[1] ? reinterpret_cast<const double2*>(spec[1][i]) : nullptr;
+		pp.T = spec[2] ? reinterpret_cast<const double2*>(spec[2][i]) : nullptr;
+		launch_prep_synth(pp, x);
+	};
+	auto fft = [&](int i, cudaStream_t x) {
+		FftParams fp = fft_params(g->plans[i], jobs[i]);
+		double* o[3];
+		for (int c = 0; c < 3; c++) o[c] = (c < ncomp && spat[c]) ? spat[c][i] : nullptr;
+		for (int c = 0; c < 3; c++) fp.spat[c] = o[c];
+		fp.vec2 = aligned16(o[0], o[1] ? o[1] : o[0], o[2] ? o[2] : o[0], g->plans[i]->spat_dist);
+		launch_fft_synth(fp, jobs[i].nfc, x);
+	};
 	if (g->leg_per_plan) {
 		// each plan's own Legendre launch (its tile shape or SIMT kernels):
 		// prologue, Legendre and FFT chained per plan on its side stream
 		group_fork(g, st, nfields, [&](int i, cudaStream_t x) {
-			PrepParams pp = prep_params(g->plans[i], jobs[i]);
-			pp.Q = reinterpret_cast<const double2*>(Qlm[i]);
-			launch_prep_synth(pp, x);
+			prologue(i, x);
 			launch_leg_synth(lp[i], x);
-			FftParams fp = fft_params(g->plans[i], jobs[i]);
-			fp.spat[0] = Vr[i];
-			fp.vec2 = aligned16(Vr[i], Vr[i], Vr[i], g->plans[i]->spat_dist);
-			launch_fft_synth(fp, jobs[i].nfc, x);
+			fft(i, x);
 		});
 		check_launch("group synthesis launch");
 		return;
 	}
 	if (!group_work(g, lp, nfields, true)) return;
-	group_fork(g, st, nfields, [&](int i, cudaStream_t x) {
-		PrepParams pp = prep_params(g->plans[i], jobs[i]);
-		pp.Q = reinterpret_cast<const double2*>(Qlm[i]);
-		launch_prep_synth(pp, x);
-	});
+	group_fork(g, st, nfields, prologue);
 	const GroupWork& W = g->dir[1];
 	launch_leg_multi(W.d_plist, W.d_work, W.nwork, W.d_counter, g->ckseg, true, g->nsm * g->ctas_per_sm, st);
-	group_fork(g, st, nfields, [&](int i, cudaStream_t x) {
-		FftParams fp = fft_params(g->plans[i], jobs[i]);
-		fp.spat[0] = Vr[i];
-		fp.vec2 = aligned16(Vr[i], Vr[i], Vr[i], g->plans[i]->spat_dist);
-		launch_fft_synth(fp, jobs[i].nfc, x);
-	});
+	group_fork(g, st, nfields, fft);
 	check_launch("group synthesis launch");
 }
 
-extern "C" void shtns_b200_group_analys(shtns_group g, double** Vr, cplx** Qlm, const int* nfields, int ltr)
+void group_analys_impl(shtns_group g, int ncomp, const int* types, double** const* spat, cplx** const* spec,
+                       const int* nfields, int ltr)
 {
 	if (!group_ok(g)) return;
 	const int np = (int) g->plans.size();
@@ -822,42 +830,91 @@ extern "C" void shtns_b200_group_analys(shtns_group g, double** Vr, cplx** Qlm, 
 	for (int i = 0; i < np; i++) {
 		shtns_cfg s = g->plans[i];
 		shtns_set_batch(s, std::max(1, nfields[i]), s->nlm, s->nspat);
-		if (!setup_job(s, jobs[i], 1, T_SCAL, std::min<int>(ltr, s->lmax))) return;
+		if (!setup_job(s, jobs[i], ncomp, types, std::min<int>(ltr, s->lmax))) return;
 		lp[i] = leg_params(s, jobs[i]);
 	}
+	auto fft = [&](int i, cudaStream_t x) {
+		FftParams fp = fft_params(g->plans[i], jobs[i]);
+		const double* in[3];
+		for (int c = 0; c < 3; c++) in[c] = (c < ncomp && spat[c]) ? spat[c][i] : nullptr;
+		for (int c = 0; c < 3; c++) fp.spat_in[c] = in[c];
+		fp.vec2 = aligned16(in[0], in[1] ? in[1] : in[0], in[2] ? in[2] : in[0], g->plans[i]->spat_dist);
+		launch_fft_analys(fp, jobs[i].nfc, x);
+	};
+	auto epilogue = [&](int i, cudaStream_t x) {
+		PrepParams pp = prep_params(g->plans[i], jobs[i]);
+		pp.Qo = spec[0] ? reinterpret_cast<double2*>(spec[0][i]) : nullptr;
+		pp.So = spec[1] ? reinterpret_cast<double2*>(spec[1][i]) : nullptr;
+		pp.To = spec[2] ? reinterpret_cast<double2*>(spec[2][i]) : nullptr;
+		launch_post_analys_m(pp, g->plans[i]->mmax, x);
+	};
 	if (g->leg_per_plan) {
 		group_fork(g, st, nfields, [&](int i, cudaStream_t x) {
 			shtns_cfg s = g->plans[i];
-			FftParams fp = fft_params(s, jobs[i]);
-			fp.spat_in[0] = Vr[i];
-			fp.vec2 = aligned16(Vr[i], Vr[i], Vr[i], s->spat_dist);
-			launch_fft_analys(fp, jobs[i].nfc, x);
+			fft(i, x);
 			int kmax_all = 0;
 			for (int im = 0; im <= jobs[i].mlim; im++)
 				kmax_all = std::max(kmax_all, (jobs[i].llim + jobs[i].vec_extra - im * s->mres) / 2 + 1);
 			launch_leg_analys(lp[i], kmax_all, x);
-			PrepParams pp = prep_params(s, jobs[i]);
-			pp.Qo = reinterpret_cast<double2*>(Qlm[i]);
-			launch_post_analys_m(pp, s->mmax, x);
+			epilogue(i, x);
 		});
 		check_launch("group analysis launch");
 		return;
 	}
 	if (!group_work(g, lp, nfields, false)) return;
-	group_fork(g, st, nfields, [&](int i, cudaStream_t x) {
-		FftParams fp = fft_params(g->plans[i], jobs[i]);
-		fp.spat_in[0] = Vr[i];
-		fp.vec2 = aligned16(Vr[i], Vr[i], Vr[i], g->plans[i]->spat_dist);
-		launch_fft_analys(fp, jobs[i].nfc, x);
-	});
+	group_fork(g, st, nfields, fft);
 	const GroupWork& W = g->dir[0];
 	launch_leg_multi(W.d_plist, W.d_work, W.nwork, W.d_counter, g->ckseg, false, g->nsm * g->ctas_per_sm, st);
-	group_fork(g, st, nfields, [&](int i, cudaStream_t x) {
-		PrepParams pp = prep_params(g->plans[i], jobs[i]);
-		pp.Qo = reinterpret_cast<double2*>(Qlm[i]);
-		launch_post_analys_m(pp, g->plans[i]->mmax, x);
-	});
+	group_fork(g, st, nfields, epilogue);
 	check_launch("group analysis launch");
+}
+
+} // namespace
+
+extern "C" void shtns_b200_group_synth(shtns_group g, cplx** Qlm, double** Vr, const int* nfields, int ltr)
+{
+	cplx** const spec[3] = {Qlm, nullptr, nullptr};
+	double** const spat[3] = {Vr, nullptr, nullptr};
+	group_synth_impl(g, 1, T_SCAL, spec, spat, nfields, ltr);
+}
+
+extern "C" void shtns_b200_group_analys(shtns_group g, double** Vr, cplx** Qlm, const int* nfields, int ltr)
+{
+	double** const spat[3] = {Vr, nullptr, nullptr};
+	cplx** const spec[3] = {Qlm, nullptr, nullptr};
+	group_analys_impl(g, 1, T_SCAL, spat, spec, nfields, ltr);
+}
+
+extern "C" void shtns_b200_group_SHsphtor_to_spat(shtns_group g, cplx** Slm, cplx** Tlm, double** Vt, double** Vp,
+                                                  const int* nfields, int ltr)
+{
+	cplx** const spec[3] = {nullptr, Slm, Tlm};
+	double** const spat[3] = {Vt, Vp, nullptr};
+	group_synth_impl(g, 2, T_VEC, spec, spat, nfields, ltr);
+}
+
+extern "C" void shtns_b200_group_spat_to_SHsphtor(shtns_group g, double** Vt, double** Vp, cplx** Slm, cplx** Tlm,
+                                                  const int* nfields, int ltr)
+{
+	double** const spat[3] = {Vt, Vp, nullptr};
+	cplx** const spec[3] = {nullptr, Slm, Tlm};
+	group_analys_impl(g, 2, T_VEC, spat, spec, nfields, ltr);
+}
+
+extern "C" void shtns_b200_group_SHqst_to_spat(shtns_group g, cplx** Qlm, cplx** Slm, cplx** Tlm, double** Vr, double** Vt,
+                                               double** Vp, const int* nfields, int ltr)
+{
+	cplx** const spec[3] = {Qlm, Slm, Tlm};
+	double** const spat[3] = {Vr, Vt, Vp};
+	group_synth_impl(g, 3, T_QST, spec, spat, nfields, ltr);
+}
+
+extern "C" void shtns_b200_group_spat_to_SHqst(shtns_group g, double** Vr, double** Vt, double** Vp, cplx** Qlm, cplx** Slm,
+                                               cplx** Tlm, const int* nfields, int ltr)
+{
+	double** const spat[3] = {Vr, Vt, Vp};
+	cplx** const spec[3] = {Qlm, Slm, Tlm};
+	group_analys_impl(g, 3, T_QST, spat, spec, nfields, ltr);
 }
 
 // ---------------------------------------------------------------------------
