@@ -5,8 +5,9 @@ results agree bit for bit.  Cases: vector (qst) fields with a polar
 threshold, a truncated call (ltr < lmax: coefficient rows beyond the call's
 last step are zeros), a column tile that is not full, a grid whose half
 latitude count is not a multiple of 32, and the automatic mode (option 10 =
-0), which takes the table for these sizes.  The table is built once per plan
-and shared by its clones."""
+0), which takes the table for these sizes; an mres = 2 plan, the adjoint of
+the analysis (the same launch with row weights) and clones made before and
+after the table is built (they use the base plan's table)."""
 import numpy as np
 import pytest
 
@@ -74,3 +75,43 @@ def test_table_option_validation_and_round_trip():
     q = torch.from_numpy(rand_spec(L, L, 1, 35, power=1.0, nfields=24)).to(dev)
     back = sh.analys(sh.synth(q))
     assert float((back - q).abs().max() / q.abs().max()) < 1e-12
+
+
+def test_table_synthesis_mres2_adjoint_and_clones():
+    """mres = 2 plan; the adjoint of the analysis (a synthesis with quadrature
+    row weights, cu_spat_to_SH_adjoint); a clone built before the table
+    exists and one built after share the base plan's table: all bit-identical
+    to the on-the-fly kernels."""
+    import ctypes as C
+    import shtns_b200
+    from shtns_b200 import capi
+    lib = capi.load()
+    dev = torch.device("cuda:0")
+    L, M, mres = 255, 126, 2
+    sh = shtns_b200.sht(L, M, mres)
+    sh.set_grid(384, 768, flags=shtns_b200.sht_quick_init | shtns_b200.SHT_THETA_CONTIGUOUS, polar_opt=1e-10)
+    nf = 12
+    q = torch.from_numpy(rand_spec(L, M, mres, 51, power=1.0, nfields=nf)).to(dev)
+    early = sh.clone()                       # before the table is built
+    out = {}
+    for mode in (1, 2):
+        for p in (sh, early):
+            assert lib.shtns_b200_set_option(p._cfg, 10, mode) == 0
+        out[mode] = sh.synth(q)
+        out[mode, "early"] = early.synth(q)
+        # adjoint of the analysis on the same coefficients
+        adj = torch.empty((nf,) + sh.spat_shape, dtype=torch.float64, device=dev)
+        sh._batch(nf)
+        sh._stream()
+        lib.cu_spat_to_SH_adjoint(sh._cfg, C.c_void_p(q.data_ptr()), C.c_void_p(adj.data_ptr()), L)
+        capi.check(lib)
+        out[mode, "adj"] = adj
+        assert sh.kernel_errors() == 0 and early.kernel_errors() == 0
+    late = sh.clone()                        # after the table exists
+    assert lib.shtns_b200_set_option(late._cfg, 10, 2) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(out[2], out[1])
+    assert torch.equal(out[2, "early"], out[1])
+    assert torch.equal(out[2, "adj"], out[1, "adj"])
+    assert torch.equal(late.synth(q), out[1])
+    assert late.kernel_errors() == 0
