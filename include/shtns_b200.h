@@ -34,7 +34,9 @@ const char* shtns_b200_last_error(void);
  * the status is cleared by this call. */
 int shtns_b200_status(void);
 
-/* Device used by a plan and bytes of GPU memory it holds (tables + work). */
+/* Device used by a plan and bytes of GPU memory it holds: its tables (for a
+ * clone, none: they belong to the base plan), including the FP64 and INT8
+ * Legendre tables once built, and its work buffers. */
 int shtns_b200_device(shtns_cfg);
 size_t shtns_b200_device_bytes(shtns_cfg);
 

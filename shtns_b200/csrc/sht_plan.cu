@@ -681,7 +681,11 @@ extern "C" int shtns_b200_device(shtns_cfg s) { return s ? s->dev : -1; }
 extern "C" size_t shtns_b200_device_bytes(shtns_cfg s)
 {
 	if (!s) return 0;
-	return (s->is_clone ? 0 : s->table_bytes) + sizeof(double) * s->qq_cap + sizeof(double2) * s->F_cap + s->stage_cap;
+	// tables owned by the original plan (recurrence tables, FP64 and INT8
+	// Legendre tables), then the plan's own work buffers
+	const size_t tables = s->is_clone ? 0 : s->table_bytes + s->ftab_bytes + s->ptab_bytes;
+	return tables + sizeof(double) * s->qq_cap + sizeof(double2) * s->F_cap + s->stage_cap + s->fscr_cap + s->pbs_cap +
+	       s->pexp_cap + s->bsl_cap + s->bexp_cap;
 }
 
 // ---------------------------------------------------------------------------

@@ -71,9 +71,16 @@ def test_table_option_validation_and_round_trip():
     sh = _plan(L, 192, 384, 1e-10)
     assert lib.shtns_b200_set_option(sh._cfg, 10, 3) == -1
     assert lib.shtns_b200_set_option(sh._cfg, 10, -1) == -1
-    assert lib.shtns_b200_set_option(sh._cfg, 10, 2) == 0
     q = torch.from_numpy(rand_spec(L, L, 1, 35, power=1.0, nfields=24)).to(dev)
-    back = sh.analys(sh.synth(q))
+    assert lib.shtns_b200_set_option(sh._cfg, 10, 1) == 0
+    sh.synth(q)                               # work buffers, no table
+    b1 = lib.shtns_b200_device_bytes(sh._cfg)
+    assert lib.shtns_b200_set_option(sh._cfg, 10, 2) == 0
+    v = sh.synth(q)
+    # the table built by this call counts in the plan's device memory, not in a clone's
+    assert lib.shtns_b200_device_bytes(sh._cfg) > b1 + 1_000_000
+    assert lib.shtns_b200_device_bytes(sh.clone()._cfg) < b1
+    back = sh.analys(v)
     assert float((back - q).abs().max() / q.abs().max()) < 1e-12
 
 
