@@ -65,20 +65,27 @@ constexpr int PB_K = 128;                  // Ishioka steps per digit-block and 
 constexpr int PB_BYTES = PB_T * PB_K;      // one digit-block: 16 KB
 constexpr int PT_NC = 32;                  // GEMM columns per CTA
 constexpr int PT_THREADS = 192;
-constexpr int PT_RA = 8;                   // digit-block slots of the copy ring
-
-template <int NS>
+// CT: 32-column tiles per work item.  CT = 1: two accumulator buffers in
+// tensor memory (the epilogue of one item overlaps the products of the
+// next); CT = 2: each digit-block of the table is read once for two column
+// tiles, whose accumulators fill the one 512-column buffer (tile c at column
+// 256 c), so the epilogue does not overlap the products (the analysis at high
+// degrees, see contract()).
+template <int NS, int CT = 1>
 struct PtLayout {
+	static constexpr int RA = (CT == 1) ? 8 : 6;               // digit-block slots of the copy ring
 	static constexpr int B_BYTES = NS * PT_NC * 128;          // digit stack of one block: NS x 32 rows x 128 bytes
+	static constexpr int B_SLOT = CT * B_BYTES;               // stacks of the item's column tiles
 	static constexpr int B_GRP = NS * (PT_NC / 8) * 128;      // bytes between 16-step (or 16-latitude) groups of a stack
 	static constexpr int A_OFF = 0;
-	static constexpr int B_OFF = PT_RA * PB_BYTES;
-	static constexpr int BAR_OFF = B_OFF + 2 * B_BYTES;
-	static constexpr int NBAR = 2 * PT_RA + 2 + 2 + 2 + 2 + 1;   // fullA, emptyA, fullB, emptyB, tfull, tempty, drain
+	static constexpr int B_OFF = RA * PB_BYTES;
+	static constexpr int BAR_OFF = B_OFF + 2 * B_SLOT;
+	static constexpr int NBAR = 2 * RA + 2 + 2 + 2 + 2 + 1;    // fullA, emptyA, fullB, emptyB, tfull, tempty, drain
 	static constexpr int BE_OFF = BAR_OFF + 8 * NBAR + 16;     // column exponents of the current item, per epilogue warp
-	static constexpr int TOTAL = BE_OFF + 4 * PT_NC * 4;
-	static constexpr int ACC_COLS = 256;                        // one accumulator buffer (NS x 32 used)
+	static constexpr int TOTAL = BE_OFF + 4 * CT * PT_NC * 4;
+	static constexpr int ACC_COLS = 256;                        // one accumulator buffer / tile (NS x 32 used)
 	static_assert(PT_NC * NS <= ACC_COLS, "accumulators exceed a buffer");
+	static_assert(CT == 1 || CT == 2, "column tiles per item");
 	static_assert(TOTAL + 1024 <= 227 * 1024, "shared memory");
 };
 
@@ -445,17 +452,20 @@ __global__ void __launch_bounds__(256) ptab_gslice_kernel(PtabRef t, LegParams p
 // memory accumulator buffers (256 columns each), warps 2-5 read the buffer
 // of the previous item, combine it in FP64 and store, then release it.
 struct PtItem {
-	int im, tile, ct;        // order, latitude tile (SYNTH) or step block, column tile
+	int im, tile, ct;        // order, latitude tile (SYNTH) or step block, first column tile
+	int ntl;                 // column tiles of the item (1 .. CT)
 	int nb;                  // blocks to contract (0: nothing; the result is zero)
 	int first;               // SYNTH: first step block
 };
 
-template <int NS, bool SYNTH>
+template <int NS, bool SYNTH, int CT = 1>
 __device__ __forceinline__ PtItem ptab_item(const PtabRef& t, const LegParams& p, long w, int nct)
 {
 	PtItem it;
-	it.ct = (int)(w % nct);
-	const long e = w / nct;
+	const int nctp = (nct + CT - 1) / CT;
+	it.ct = (int)(w % nctp) * CT;
+	it.ntl = min(CT, nct - it.ct);
+	const long e = w / nctp;
 	if (SYNTH) {
 		it.tile = (int)(e % t.ntb);
 		it.im = (int)(e / t.ntb);
@@ -507,11 +517,12 @@ __device__ __forceinline__ void ptab_block(const PtabRef& t, const PtItem& it, i
 	}
 }
 
-template <int NS, bool SYNTH>
+template <int NS, bool SYNTH, int CT>
 __global__ void __launch_bounds__(PT_THREADS, 1) ptab_kernel(PtabRef t, LegParams p, const uint8_t* __restrict__ bs,
                                                              const int* __restrict__ bexp, int nct, long nitems, int* err)
 {
-	using L = PtLayout<NS>;
+	using L = PtLayout<NS, CT>;
+	constexpr int PT_RA = L::RA;
 	extern __shared__ __align__(1024) uint8_t smem_raw[];
 	uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
 	uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
@@ -552,7 +563,7 @@ __global__ void __launch_bounds__(PT_THREADS, 1) ptab_kernel(PtabRef t, LegParam
 			#pragma unroll
 			for (int q = 0; q < PT_RA; q++) issuedA[q] = 0;
 			for (long w = blockIdx.x; w < nitems && ok; w += gridDim.x) {
-				const PtItem it = ptab_item<NS, SYNTH>(t, p, w, nct);
+				const PtItem it = ptab_item<NS, SYNTH, CT>(t, p, w, nct);
 				int scan = it.first;
 				for (int b = 0; b < it.nb && ok; b++) {
 					long ablk, bblk;
@@ -560,8 +571,10 @@ __global__ void __launch_bounds__(PT_THREADS, 1) ptab_kernel(PtabRef t, LegParam
 					const int bsl = (int)(ub & 1);
 					if (ub >= 2) ok = mbar_wait(&emptyB[bsl], (uint32_t)(((ub >> 1) - 1) & 1), abort_flag);
 					if (!ok) break;
-					mbar_expect_tx(&fullB[bsl], L::B_BYTES);
-					bulk_g2s(sB + bsl * L::B_BYTES, bs + (bblk * nct + it.ct) * (long) L::B_BYTES, L::B_BYTES, &fullB[bsl]);
+					// the stacks of the item's column tiles are adjacent (column tile fastest)
+					mbar_expect_tx(&fullB[bsl], it.ntl * L::B_BYTES);
+					bulk_g2s(sB + bsl * L::B_SLOT, bs + (bblk * nct + it.ct) * (long) L::B_BYTES, it.ntl * L::B_BYTES,
+					         &fullB[bsl]);
 					issuedB[bsl]++;
 					ub++;
 					const long nbk = tab_kblocks(t, it.im);
@@ -590,10 +603,12 @@ __global__ void __launch_bounds__(PT_THREADS, 1) ptab_kernel(PtabRef t, LegParam
 			bool ok = true, any = false;
 			long ua = 0, ub = 0, ni = 0;
 			for (long w = blockIdx.x; w < nitems && ok; w += gridDim.x) {
-				const PtItem it = ptab_item<NS, SYNTH>(t, p, w, nct);
+				const PtItem it = ptab_item<NS, SYNTH, CT>(t, p, w, nct);
 				if (it.nb == 0) continue;
-				const int buf = (int)(ni & 1);
-				if (ni >= 2) ok = mbar_wait(&tempty[buf], (uint32_t)(((ni >> 1) - 1) & 1), abort_flag);
+				// CT = 1: alternate between the two buffers; CT = 2: the one buffer
+				const int buf = (CT == 1) ? (int)(ni & 1) : 0;
+				if (CT == 1 && ni >= 2) ok = mbar_wait(&tempty[buf], (uint32_t)(((ni >> 1) - 1) & 1), abort_flag);
+				if (CT == 2 && ni >= 1) ok = mbar_wait(&tempty[0], (uint32_t)((ni - 1) & 1), abort_flag);
 				if (!ok) break;
 				tc_fence_after();
 				const uint32_t dbase = tmem + buf * L::ACC_COLS;
@@ -618,8 +633,12 @@ __global__ void __launch_bounds__(PT_THREADS, 1) ptab_kernel(PtabRef t, LegParam
 								ad = sdesc(sA + slot * PB_BYTES + kk * 4 * 128, 128, 2048);
 							}
 							// B K-major: N = stacked digit rows (8-row groups 128 B apart), K in 16-byte core matrices B_GRP apart
-							const uint64_t bd = sdesc(sB + bsl * L::B_BYTES + kk * 2 * L::B_GRP, L::B_GRP, 128);
-							mma_i8(dbase + PT_NC * i, ad, bd, idesc, first ? 0u : 1u);
+							#pragma unroll
+							for (int c = 0; c < CT; c++) {
+								if (c >= it.ntl) break;
+								const uint64_t bd = sdesc(sB + bsl * L::B_SLOT + c * L::B_BYTES + kk * 2 * L::B_GRP, L::B_GRP, 128);
+								mma_i8(dbase + c * L::ACC_COLS + PT_NC * i, ad, bd, idesc, first ? 0u : 1u);
+							}
 							first = false;
 						}
 						any = true;
@@ -641,28 +660,33 @@ __global__ void __launch_bounds__(PT_THREADS, 1) ptab_kernel(PtabRef t, LegParam
 		const int q = warp & 3;
 		long ni = 0;
 		for (long w = blockIdx.x; w < nitems; w += gridDim.x) {
-			const PtItem it = ptab_item<NS, SYNTH>(t, p, w, nct);
+			const PtItem it = ptab_item<NS, SYNTH, CT>(t, p, w, nct);
 			const int m = it.im * p.mres;
 			const int r = 32 * q + lane;
-			double acc[PT_NC];
+			double accs[CT][PT_NC];
 			bool val = false;
 			if (it.nb > 0) {
-				const int buf = (int)(ni & 1);
-				bool ok = mbar_wait(&tfull[buf], (uint32_t)((ni >> 1) & 1), abort_flag);
+				const int buf = (CT == 1) ? (int)(ni & 1) : 0;
+				const uint32_t par = (CT == 1) ? (uint32_t)((ni >> 1) & 1) : (uint32_t)(ni & 1);
+				bool ok = mbar_wait(&tfull[buf], par, abort_flag);
 				ok = __all_sync(0xffffffffu, ok);
 				if (!ok) break;
 				tc_fence_after();
-				const uint32_t trow = tmem + buf * L::ACC_COLS + ((uint32_t)(32 * q) << 16);
 				#pragma unroll
-				for (int c = 0; c < PT_NC; c++) acc[c] = 0.0;
-				#pragma unroll
-				for (int s = NS - 1; s >= 0; s--) {
-					int v[16];
+				for (int ci = 0; ci < CT; ci++) {
+					if (ci >= it.ntl) break;
+					const uint32_t trow = tmem + buf * L::ACC_COLS + ci * L::ACC_COLS + ((uint32_t)(32 * q) << 16);
 					#pragma unroll
-					for (int h = 0; h < 2; h++) {
-						tmem_ld16(trow + PT_NC * s + 16 * h, v);
+					for (int c = 0; c < PT_NC; c++) accs[ci][c] = 0.0;
+					#pragma unroll
+					for (int s = NS - 1; s >= 0; s--) {
+						int v[16];
 						#pragma unroll
-						for (int c = 0; c < 16; c++) acc[16 * h + c] = fma(acc[16 * h + c], 0.00390625, (double) v[c]);
+						for (int h = 0; h < 2; h++) {
+							tmem_ld16(trow + PT_NC * s + 16 * h, v);
+							#pragma unroll
+							for (int c = 0; c < 16; c++) accs[ci][16 * h + c] = fma(accs[ci][16 * h + c], 0.00390625, (double) v[c]);
+						}
 					}
 				}
 				tc_fence_before();
@@ -671,10 +695,15 @@ __global__ void __launch_bounds__(PT_THREADS, 1) ptab_kernel(PtabRef t, LegParam
 				ni++;
 				val = true;
 			}
-			// column exponents of the item, staged per warp
-			int* be = reinterpret_cast<int*>(smem + L::BE_OFF) + q * PT_NC;
+			#pragma unroll
+			for (int ci = 0; ci < CT; ci++) {
+			if (ci >= it.ntl) break;
+			const int ct = it.ct + ci;
+			const double* acc = accs[ci];
+			// column exponents of the tile, staged per warp
+			int* be = reinterpret_cast<int*>(smem + L::BE_OFF) + (q * CT + ci) * PT_NC;
 			__syncwarp();
-			be[lane] = __ldg(bexp + (long) it.im * (nct * PT_NC) + it.ct * PT_NC + lane);
+			be[lane] = __ldg(bexp + (long) it.im * (nct * PT_NC) + ct * PT_NC + lane);
 			__syncwarp();
 			if (SYNTH) {
 				const int row = it.tile * PB_T + r;
@@ -684,7 +713,7 @@ __global__ void __launch_bounds__(PT_THREADS, 1) ptab_kernel(PtabRef t, LegParam
 					const double cx = p.x[row];
 					#pragma unroll
 					for (int fl = 0; fl < 8; fl++) {
-						const int fc = it.ct * 8 + fl;
+						const int fc = ct * 8 + fl;
 						if (fc >= p.nfc) break;
 						const int c0 = 16 * (fl >> 2) + 2 * (fl & 3);          // even re; +1 im; +8 odd
 						auto col = [&](int cl) {
@@ -711,16 +740,17 @@ __global__ void __launch_bounds__(PT_THREADS, 1) ptab_kernel(PtabRef t, LegParam
 				const int nk = (p.llim + p.vec_extra - m) / 2 + 1;
 				const int k = it.tile * PB_K + r;
 				if (k < nk) {
-					double* qrow = p.qq + ((long) p.mt.koff[it.im] + k) * p.ncol + it.ct * PT_NC;
+					double* qrow = p.qq + ((long) p.mt.koff[it.im] + k) * p.ncol + ct * PT_NC;
 					#pragma unroll
 					for (int c = 0; c < PT_NC; c += 2) {
-						if (it.ct * PT_NC + c >= p.ncol) break;
+						if (ct * PT_NC + c >= p.ncol) break;
 						const int b0 = be[c], b1 = be[c + 1];
 						const double a = (val && b0 > -1000) ? acc[c] * pow2(b0 + 2 - 16) : 0.0;
 						const double b = (val && b1 > -1000) ? acc[c + 1] * pow2(b1 + 2 - 16) : 0.0;
 						*reinterpret_cast<double2*>(qrow + c) = make_double2(a, b);
 					}
 				}
+			}
 			}
 		}
 	}
@@ -856,20 +886,40 @@ int num_sms()
 	return n;
 }
 
-template <int NS, bool SYNTH>
-void launch_contract(const PtabRef& t, const LegParams& p, shtns_cfg s, int nct, long nitems, cudaStream_t st)
+// nunits: work items per column tile (synthesis: order x latitude tile;
+// analysis: the table's step blocks of the call's orders)
+template <int NS, bool SYNTH, int CT>
+void launch_contract(const PtabRef& t, const LegParams& p, shtns_cfg s, int nct, long nunits, cudaStream_t st)
 {
-	using L = PtLayout<NS>;
+	using L = PtLayout<NS, CT>;
 	const size_t smem = L::TOTAL + 1024;
 	static bool attr = false;
 	if (!attr) {
-		cudaFuncSetAttribute(ptab_kernel<NS, SYNTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+		cudaFuncSetAttribute(ptab_kernel<NS, SYNTH, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
 		attr = true;
 	}
+	const long nitems = nunits * ((nct + CT - 1) / CT);
 	const int grid = (int) std::max<long>(1, std::min<long>(nitems, num_sms()));
-	ptab_kernel<NS, SYNTH><<<grid, PT_THREADS, smem, st>>>(t, p, static_cast<const uint8_t*>(s->d_pbs), s->d_pexp, nct,
-	                                                       nitems, s->d_split_err);
+	ptab_kernel<NS, SYNTH, CT><<<grid, PT_THREADS, smem, st>>>(t, p, static_cast<const uint8_t*>(s->d_pbs), s->d_pexp, nct,
+	                                                           nitems, s->d_split_err);
 	shtb_count_launch();
+}
+
+// Two column tiles per work item, for the analysis from this call degree on
+// (and at least two tiles): the items are then long enough that the
+// epilogue, which no longer overlaps the next item's products, costs less
+// than the second read of the table saves.  Measured at lmax 4095, 16 fields,
+// 7 digits: analysis 24.3 -> 22.7 ms; the synthesis did not gain (25.4 vs
+// 26.0 ms, within run-to-run noise), so it keeps one tile per item.
+constexpr int PT_CT2_LMIN = 2047;
+
+template <int NS, bool SYNTH>
+void contract(const PtabRef& t, const LegParams& p, shtns_cfg s, int nct, long nunits, cudaStream_t st)
+{
+	if constexpr (!SYNTH) {
+		if (nct >= 2 && p.llim >= PT_CT2_LMIN) { launch_contract<NS, SYNTH, 2>(t, p, s, nct, nunits, st); return; }
+	}
+	launch_contract<NS, SYNTH, 1>(t, p, s, nct, nunits, st);
 }
 
 template <int NS>
@@ -879,7 +929,7 @@ void synth_ns(shtns_cfg s, shtns_cfg o, const LegParams& p, int nct, cudaStream_
 	ptab_qslice_kernel<NS><<<dim3(nct, p.mlim + 1), 256, 0, st>>>(t, p.qq, p.ncol, p.mt, p.llim, p.vec_extra, p.mres, nct,
 	                                                             static_cast<uint8_t*>(s->d_pbs), s->d_pexp);
 	shtb_count_launch();
-	launch_contract<NS, true>(t, p, s, nct, (long)(p.mlim + 1) * t.ntb * nct, st);
+	contract<NS, true>(t, p, s, nct, (long)(p.mlim + 1) * t.ntb, st);
 }
 
 template <int NS>
@@ -890,7 +940,7 @@ void analys_ns(shtns_cfg s, shtns_cfg o, const LegParams& p, int nct, cudaStream
 	shtb_count_launch();
 	// step blocks of the orders 0 .. mlim in the table
 	const long nkb = (p.mlim < o->mmax) ? o->koff_blocks_h[p.mlim + 1] : o->ptab_kblocks;
-	launch_contract<NS, false>(t, p, s, nct, nkb * nct, st);
+	contract<NS, false>(t, p, s, nct, nkb, st);
 }
 
 bool ptab_check(const LegParams& p)

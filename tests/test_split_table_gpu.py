@@ -127,3 +127,29 @@ def test_table_high_degree_within_1e11():
     print("lmax 4095, 7 digits: synthesis", es, "analysis", ea)
     assert es < 1e-11, es
     assert ea < 1e-11, ea
+
+
+def test_table_two_column_tiles_per_item():
+    """From lmax 2047 on, each analysis work item reads the table once for two
+    32-column tiles (accumulators of both in tensor memory).  20 fields = 80
+    GEMM columns = 3 tiles: items hold a pair of tiles or the last single one.
+    Synthesis and analysis within 1e-11 of the FP64 stages, as in the 8-field
+    (one tile per item) case above."""
+    dev = torch.device("cuda:0")
+    L = 2047
+    sh = _plan(L, nlat=3072, eps=1e-10)
+    q = torch.from_numpy(rand_spec(L, L, 1, 16, power=1.0, nfields=20)).to(dev)
+    v64 = sh.synth(q)
+    q64 = sh.analys(v64)
+    sh.set_split(7)
+    v = sh.synth(q)
+    qa = sh.analys(v64)
+    assert sh.kernel_errors() == 0
+    es, ea = _rel(v, v64), _rel(qa, q64)
+    print("lmax 2047, 20 fields, 7 digits: synthesis", es, "analysis", ea)
+    assert es < 1e-11, es
+    assert ea < 1e-11, ea
+    # every field, not only the largest values: per-field errors against each field's maximum
+    for f in (0, 9, 19):
+        assert _rel(v[f], v64[f]) < 1e-11
+        assert _rel(qa[f], q64[f]) < 1e-11
