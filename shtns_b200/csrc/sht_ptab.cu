@@ -44,6 +44,10 @@
 //   warps 2-5: read the NS INT32 accumulators (tcgen05.ld), combine them in
 //     FP64 and store F (synthesis: folded hemispheres, as leg_synth_tile) or
 //     the Ishioka-basis coefficients (analysis).
+// The two 256-column accumulator buffers alternate between items, so the
+// epilogue of one item overlaps the products of the next; the analysis at
+// lmax >= 2047 instead gives each item two column tiles (one table read for
+// both, their accumulators in the two halves of tensor memory).
 // Every mbarrier wait is bounded (about one second by %globaltimer); a wait
 // that gives up records an error flag (shtns_b200_kernel_errors), the CTA
 // waits (bounded) for the copies and products it issued, frees its tensor
