@@ -45,9 +45,10 @@
 //     FP64 and store F (synthesis: folded hemispheres, as leg_synth_tile) or
 //     the Ishioka-basis coefficients (analysis).
 // The two 256-column accumulator buffers alternate between items, so the
-// epilogue of one item overlaps the products of the next; the analysis at
-// lmax >= 2047 instead gives each item two column tiles (one table read for
-// both, their accumulators in the two halves of tensor memory).
+// epilogue of one item overlaps the products of the next; the analysis (with
+// two or more column tiles) instead gives each item two column tiles (one
+// table read for both, their accumulators in the two halves of tensor
+// memory).
 // Every mbarrier wait is bounded (about one second by %globaltimer); a wait
 // that gives up records an error flag (shtns_b200_kernel_errors), the CTA
 // waits (bounded) for the copies and products it issued, frees its tensor
@@ -73,8 +74,8 @@ constexpr int PT_THREADS = 192;
 // tensor memory (the epilogue of one item overlaps the products of the
 // next); CT = 2: each digit-block of the table is read once for two column
 // tiles, whose accumulators fill the one 512-column buffer (tile c at column
-// 256 c), so the epilogue does not overlap the products (the analysis at high
-// degrees, see contract()).
+// 256 c), so the epilogue does not overlap the products (the analysis, see
+// contract()).
 template <int NS, int CT = 1>
 struct PtLayout {
 	static constexpr int RA = (CT == 1) ? 8 : 6;               // digit-block slots of the copy ring
@@ -909,19 +910,18 @@ void launch_contract(const PtabRef& t, const LegParams& p, shtns_cfg s, int nct,
 	shtb_count_launch();
 }
 
-// Two column tiles per work item, for the analysis from this call degree on
-// (and at least two tiles): the items are then long enough that the
-// epilogue, which no longer overlaps the next item's products, costs less
-// than the second read of the table saves.  Measured at lmax 4095, 16 fields,
-// 7 digits: analysis 24.3 -> 22.7 ms; the synthesis did not gain (25.4 vs
-// 26.0 ms, within run-to-run noise), so it keeps one tile per item.
-constexpr int PT_CT2_LMIN = 2047;
-
+// Two column tiles per work item for the analysis (with at least two
+// tiles): one read of each table block serves both, which saves more than
+// the epilogue, no longer overlapped with the next item's products, costs.
+// Measured with 7 digits: lmax 4095, 16 fields 24.3 -> 22.7 ms; lmax 511,
+// 64 fields qst (24 tiles) 1.748 -> 1.687 ms.  The synthesis did not gain
+// (lmax 4095, 16 fields: 25.4 vs 26.0 ms, within run-to-run noise), so it
+// keeps one tile per item.
 template <int NS, bool SYNTH>
 void contract(const PtabRef& t, const LegParams& p, shtns_cfg s, int nct, long nunits, cudaStream_t st)
 {
 	if constexpr (!SYNTH) {
-		if (nct >= 2 && p.llim >= PT_CT2_LMIN) { launch_contract<NS, SYNTH, 2>(t, p, s, nct, nunits, st); return; }
+		if (nct >= 2) { launch_contract<NS, SYNTH, 2>(t, p, s, nct, nunits, st); return; }
 	}
 	launch_contract<NS, SYNTH, 1>(t, p, s, nct, nunits, st);
 }

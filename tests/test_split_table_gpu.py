@@ -130,8 +130,8 @@ def test_table_high_degree_within_1e11():
 
 
 def test_table_two_column_tiles_per_item():
-    """From lmax 2047 on, each analysis work item reads the table once for two
-    32-column tiles (accumulators of both in tensor memory).  20 fields = 80
+    """Each analysis work item reads the table once for two 32-column tiles
+    (accumulators of both in tensor memory), here at lmax 2047.  20 fields = 80
     GEMM columns = 3 tiles: items hold a pair of tiles or the last single one.
     Synthesis and analysis within 1e-11 of the FP64 stages, as in the 8-field
     (one tile per item) case above."""
